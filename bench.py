@@ -1,0 +1,315 @@
+"""Benchmark of the spatial-operator hot path: DOF-updates/s per RK stage on one B200.
+
+Workload (default): the shocked Euler case with DG/FV blending -- Sedov-type blast on 32^3
+elements, N = 3 (2,097,152 nodes, 5 variables), gamma 1.4, ambient rho 1, p 1e-5, E0 = 1 in a
+Gaussian of width 0.05, modal-energy indicator with alpha in [0, 0.5], positivity repair, periodic
+box, LSRK 5-4 at CFL 0.5.  One "step" is one full time step (5 RK stages + the device CFL
+reduction); one DOF-update is one node with all 5 variables advanced through one stage.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload W]
+
+Multi-GPU (torchrun): every rank advances its own replica of the workload (independent runs; the
+element-partitioned halo exchange is not built), the timed region is bracketed by barriers and the
+max over ranks is reported; value is the whole-job DOF-updates/s.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+WORKLOADS = {
+    # name: (elements per direction, setup, indicator)
+    "sedov32": dict(nx=32, setup="sedov", indicator=1, positivity=1,
+                    desc="Sedov blast 32^3 elements N=3 (2.1M nodes), DG/FV blending, FP64"),
+    "wave16": dict(nx=16, setup="wave", indicator=0, positivity=0,
+                   desc="periodic density wave 16^3 elements N=3 (262k nodes), EC volume + HLLC, FP64"),
+}
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def make_state(wl):
+    from nemo_b200 import mesh, setups
+    w = WORKLOADS[wl]
+    if w["setup"] == "sedov":
+        m = mesh.brick(w["nx"], lo=(-0.5,) * 3, hi=(0.5,) * 3)
+        u = setups.sedov(m, sigma=0.05)
+    else:
+        m = mesh.brick(w["nx"])
+        u = setups.density_wave(m, seed=1234)
+    return m, u
+
+
+def make_cfg(wl):
+    from nemo_b200 import abi
+    w = WORKLOADS[wl]
+    return abi.default_cfg(indicator=w["indicator"], positivity=w["positivity"], cfl=0.5)
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.out = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            os.makedirs(os.path.dirname(self.out), exist_ok=True)
+            self.f = open(self.out, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}", "--format=csv",
+                                          "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.3)
+            self.proc.terminate()
+            self.proc.wait()
+            self.f.close()
+
+    def summary(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        rows = []
+        with open(self.out) as f:
+            for line in f.read().splitlines()[1:]:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1].split()[0]) for r in rows]
+        mx = float(rows[0][2].split()[0])
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower().startswith("active")})
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": reasons, "samples": len(rows)}
+
+
+def cpu_baseline(wl, u, m, nthreads=None, sample_stages=5):
+    """The oracle (C++ FP64 restatement, OpenMP) on the host cores, on a bounded sample of the same
+    workload: sample_stages RK stages of the full state."""
+    from oracle import oracle as orc
+    c = make_cfg(wl)
+    o = orc.Oracle(c, m.neighbors(), m.delta, nthreads=nthreads)
+    uu, reg = u.copy(), np.zeros_like(u)
+    dt, _ = o.timestep(uu)
+    o.stage(uu, reg, 0, dt)  # untimed warm-up stage (page-in)
+    uu, reg = u.copy(), np.zeros_like(u)
+    t0 = time.perf_counter()
+    for s in range(sample_stages):
+        o.stage(uu, reg, s % 5, dt)
+    el = time.perf_counter() - t0
+    dof = m.E * 64 * sample_stages
+    return {"value": dof / el, "unit": "DOF-updates/s", "cores": o.nthreads, "kind": "port",
+            "sample": f"{sample_stages} RK stages of the full {WORKLOADS[wl]['desc']} state, "
+                      f"{o.nthreads} OpenMP threads, {el:.2f} s"}
+
+
+def run_reference(args, rank, world):
+    """--impl reference: the reference's CPU implementation of the path.  The Fortran reference
+    cannot be built here (no Fortran compiler / MPI / p4est / HDF5), so this times the C++ FP64
+    restatement of it (oracle/) on all host cores; each step is one full time step (5 stages)."""
+    if rank != 0:
+        return
+    from oracle import oracle as orc
+    orc.build()
+    m, u = make_state(args.workload)
+    c = make_cfg(args.workload)
+    o = orc.Oracle(c, m.neighbors(), m.delta)
+    uu = u.copy()
+    for _ in range(args.warmup):
+        uu, _, _, _ = o.run(uu, nsteps=1)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        uu, _, _, _ = o.run(uu, nsteps=1)
+    el = time.perf_counter() - t0
+    val = m.E * 64 * 5 * args.steps / el
+    line = {
+        "impl": "reference", "metric": "DOF-updates/s per RK stage", "value": val, "unit": "DOF-updates/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOADS[args.workload]["desc"], "elements": m.E, "nodes": m.E * 64,
+                   "stages_per_step": 5},
+        "cpu_baseline": {"value": val, "unit": "DOF-updates/s", "cores": o.nthreads, "kind": "port",
+                         "sample": f"{args.steps} full time steps, {o.nthreads} OpenMP threads; the Fortran "
+                                   "reference is unbuildable here, this is its C++ FP64 restatement"},
+        "e2e": {"value": val, "unit": "DOF-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="sedov32", choices=sorted(WORKLOADS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    assert args.warmup >= 3 or args.impl == "reference" or os.environ.get("NEMO_BENCH_ALLOW_SHORT")
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    from nemo_b200 import abi
+    from nemo_b200.solver import Solver
+    import ctypes
+
+    m, u = make_state(args.workload)
+    c = make_cfg(args.workload)
+    s = Solver(c, m)
+    s.upload(u)
+    stream_ptr = ctypes.c_uint64()
+    abi.call("nemo_gpu_stream", ctypes.byref(stream_ptr))
+    stream = torch.cuda.ExternalStream(stream_ptr.value)
+
+    # warm-up (graphs are built here)
+    s.run(nsteps=args.warmup)
+
+    # ---- timed region: K steps, per-kernel CUDA events on the library stream
+    abi.call("nemo_gpu_set_timing", 1)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        t_sim, nst = s.run(nsteps=args.steps)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    ms = ev0.elapsed_time(ev1)
+    st_ms, st_n, tot_ms, tot_n = (ctypes.c_double(), ctypes.c_int64(), ctypes.c_double(), ctypes.c_int64())
+    abi.call("nemo_gpu_kernel_timing", ctypes.byref(st_ms), ctypes.byref(st_n), ctypes.byref(tot_ms),
+             ctypes.byref(tot_n))
+    abi.call("nemo_gpu_set_timing", 0)
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    dof_per_step = m.E * 64 * 5
+    value = world * dof_per_step * args.steps / (ms * 1e-3)
+
+    # ---- roofline of the stage kernel (HBM): algorithmic bytes per launch / avg launch time
+    V = 5
+    bytes_per_launch = sum(m.E * 64 * V * 8 * (3 if st == 0 else 4) for st in range(5)) / 5.0
+    avg_stage_s = st_ms.value * 1e-3 / max(st_n.value, 1)
+    peak, peak_kind = load_peaks()
+    achieved = bytes_per_launch / avg_stage_s / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "stage_traffic.json")
+    if os.path.exists(tpath):
+        with open(tpath) as f:
+            traffic = json.load(f).get(args.workload)
+
+    # ---- end to end through the C-ABI: pinned host state in, one step, state out (every step)
+    nbytes = u.nbytes
+    host_in = torch.empty(nbytes // 8, dtype=torch.float64, pin_memory=True)
+    host_out = torch.empty(nbytes // 8, dtype=torch.float64, pin_memory=True)
+    host_in.numpy()[:] = np.ascontiguousarray(u.transpose(1, 0, 2)).ravel()
+    row = V * 64 * 8
+    for _ in range(2):  # warm-up
+        s.upload_aos(host_in.data_ptr(), row)
+        s.run(nsteps=1)
+        abi.call("nemo_gpu_download_state", ctypes.c_void_p(host_out.data_ptr()), row)
+    e2e_steps = max(3, min(args.steps, 10))
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        s.upload_aos(host_in.data_ptr(), row)
+        s.run(nsteps=1)
+        abi.call("nemo_gpu_download_state", ctypes.c_void_p(host_out.data_ptr()), row)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    if dist:
+        t = torch.tensor([e2e_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_val = world * dof_per_step * e2e_steps / (e2e_ms * 1e-3)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(args.workload, u, m)
+
+    if rank == 0:
+        line = {
+            "metric": "DOF-updates/s per RK stage",
+            "value": value,
+            "unit": "DOF-updates/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": ms / args.steps,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": WORKLOADS[args.workload]["desc"], "elements": m.E, "nodes": m.E * 64,
+                       "stages_per_step": 5, "precision": "plain FP64",
+                       "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
+                       "l2": "working set (u in/out + register, 3 x 84 MB) larger than L2"},
+            "clocks": clk.summary(),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
+                         "kernel": "k_stage_euler64", "algorithmic_bytes_per_launch": bytes_per_launch,
+                         "avg_launch_ms": avg_stage_s * 1e3},
+            "e2e": {"value": e2e_val, "unit": "DOF-updates/s", "h2d_bytes_per_step": nbytes,
+                    "d2h_bytes_per_step": nbytes,
+                    "note": "per step: upload of the full state from pinned host memory, one time step, "
+                            "download of the full state"},
+            "gpu_launches": int(tot_n.value),
+            "sim": {"t": t_sim, "steps": nst},
+        }
+        if cpu:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line), flush=True)
+    s.finalize()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

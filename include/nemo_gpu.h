@@ -1,0 +1,173 @@
+/*
+ * nemo_gpu.h -- C-ABI of the B200 spatial operator for nemo (jmark/nemo).
+ *
+ * The reference drives its spatial operator through Fortran hook modules that the
+ * build registry wires together at compile time (scripts/nemo.py:245-305).  The GPU
+ * module replaces three of them:
+ *
+ *   hook_calc_timestep_200   source/kernel/mcfv/3d/kernel_timestep_mod.f90:17-58
+ *   hook_pre_rk_timestep_300 source/kernel/mcfv/3d/kernel_hooks_mod.f90:7-20
+ *   hook_mid_rk_timestep_500 source/timedisc/rungekutta/low-storage/4-5/timedisc_hooks_mod.f90:51-58
+ *
+ * and calls this library through iso_c_binding interfaces in the style of the p4wrap
+ * bindings (source/mesh/p4est/wrapper/p4wrap_interfaces_mod.f90).  Every entry point is
+ * plain C: pointers, sizes and scalars only, and returns an int status (0 = OK).  No C++
+ * exception crosses the boundary; on a non-zero status nemo_gpu_last_error() yields the
+ * message, and the Fortran shim forwards it to raise_error (source/utils/status_mod.f90:7-21).
+ *
+ * Data conventions (match the reference's):
+ *   - one element ("quad") holds N_NODES^3 Gauss-Lobatto nodes, Fortran order state(i,j,k,v),
+ *     i fastest (x), then j (y), k (z), then the variable; variables rho, rho*u, rho*v, rho*w, E
+ *     (source/equations/euler/equations_const_mod.f90:7-16) or the 9 GLM-MHD variables
+ *     (source/equations/mhd/equations_const_mod.f90:7-29);
+ *   - face ids NOR,SOU = x-/x+, WES,EAS = y-/y+, FRO,BAC = z-/z+ are 1..6 on the Fortran side
+ *     (source/utils/constants_mod.f90:33-40) and 0..5 in this header;
+ *   - du/dt = rhs, the time integrator is the 2N low-storage RK 5-4 of Kennedy-Carpenter
+ *     (source/timedisc/rungekutta/low-storage/4-5/timedisc_const_mod.f90:5-29).
+ *
+ * Threading: call from one host thread; the library owns one CUDA stream and all device
+ * memory.  The state on the device is authoritative between upload and download.
+ */
+#ifndef NEMO_GPU_H
+#define NEMO_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- configuration ------------------------------------------------------------------ */
+
+enum nemo_eqn        { NEMO_EQN_EULER = 0, NEMO_EQN_MHD = 1 };
+/* two-point volume fluxes: source/equations/euler/two_point/{chandrashekar,standard},
+   source/equations/mhd/two_point/ec */
+enum nemo_volflux    { NEMO_VOLFLUX_CHANDRASHEKAR = 0, NEMO_VOLFLUX_CENTRAL = 1, NEMO_VOLFLUX_EC_MHD = 2 };
+/* surface fluxes: source/equations/euler/riemann/{hllc,rusanov}, source/equations/mhd/riemann/{hlld,rusanov} */
+enum nemo_surfflux   { NEMO_SURFFLUX_HLLC = 0, NEMO_SURFFLUX_RUSANOV = 1, NEMO_SURFFLUX_HLLD = 2 };
+/* arithmetic of the flux bulk; conserved-variable RK registers are FP64 in every mode */
+enum nemo_precision  { NEMO_PREC_FP64 = 0, NEMO_PREC_FP32 = 1 };
+/* DG/FV blending coefficient alpha: none, modal-energy indicator, learned MLP (modal fallback) */
+enum nemo_indicator  { NEMO_IND_NONE = 0, NEMO_IND_MODAL = 1, NEMO_IND_LEARNED = 2 };
+
+enum nemo_face { NEMO_NOR = 0, NEMO_SOU = 1, NEMO_WES = 2, NEMO_EAS = 3, NEMO_FRO = 4, NEMO_BAC = 5 };
+
+enum nemo_status {
+    NEMO_OK = 0,
+    NEMO_ERR_ARG = 1,          /* bad argument (size, null pointer, unsupported option) */
+    NEMO_ERR_STATE = 2,        /* call out of order (no init / no mesh / no state) */
+    NEMO_ERR_CUDA = 3,         /* a CUDA runtime call failed */
+    NEMO_ERR_REPAIR = 4,       /* positivity repair failed on at least one element */
+    NEMO_ERR_NONFINITE = 5     /* non-finite time step or state */
+};
+
+typedef struct nemo_cfg {
+    int32_t n_nodes;          /* Gauss-Lobatto nodes per direction (N+1); 4 is compiled */
+    int32_t n_vars;           /* 5 (Euler) or 9 (GLM-MHD) */
+    int32_t eqn;              /* enum nemo_eqn */
+    int32_t volume_flux;      /* enum nemo_volflux */
+    int32_t surface_flux;     /* enum nemo_surfflux */
+    int32_t precision;        /* enum nemo_precision */
+    int32_t indicator;        /* enum nemo_indicator */
+    int32_t alpha_smoothing;  /* 1: alpha_e = max(alpha_e, 0.5 * max over face neighbours) */
+    int32_t positivity;       /* 1: element-tile squeeze repair after every stage
+                                 (source/kernel/mcfv/3d/kernel_validate_mod.f90:159-272) */
+    int32_t non_conservative; /* MHD: add the Powell/GLM non-conservative term */
+    double  kappa;            /* ratio of specific heats (setup_config_mod kappa) */
+    double  mu0;              /* magnetic permeability (MHD) */
+    double  cfl;              /* CFL number used by nemo_gpu_calc_timestep / run */
+    double  alpha_max;        /* upper clip of alpha (0.5) */
+    double  alpha_min;        /* alpha below this is set to 0 (0.001) */
+    double  repair_decr;      /* squeeze decrement of the repair (0.01, kernel_config_mod.f90:5) */
+    double  glm_ch;           /* GLM cleaning speed (MHD); updated by calc_timestep */
+    double  glm_alpha;        /* GLM damping (MHD); updated by calc_timestep */
+    double  reserved[4];
+} nemo_cfg;
+
+/* Fill *cfg with the defaults of the Euler DGSEM path (N=3, Chandrashekar, HLLC, FP64). */
+int nemo_gpu_default_cfg(nemo_cfg* cfg);
+
+/* hook_init_400 (source/kernel/dgsem/weakform/2d/kernel_hooks_mod.f90:7-13 ->
+   kernel_share_mod.f90:56-151): build the Gauss-Lobatto operators and select the device. */
+int nemo_gpu_init(const nemo_cfg* cfg);
+
+/* Operator matrices as kernel_share_mod exports them, computed on the host without a GPU:
+   nodes/weights on [-1,1] (n), D (n*n, row-major D[i*n+m] = l_m'(x_i)), the split-form
+   matrix S = 2D - W^-1 B (n*n), the modal transform inverse Vandermonde Vinv (n*n). */
+int nemo_gpu_operators(int32_t n, double* nodes, double* weights, double* dmat, double* smat,
+                       double* vinv);
+
+/* Mesh in the reference's side form (source/mesh/p4est/mesh_types_mod.f90:57-77):
+     delta[nelems*3], center[nelems*3]            element sizes and centres
+     side_quads[nsides*2*4]                        0-based element ids, [side][iside][iquad]
+     side_faceid[nsides*2]                         face id (0..5) of the side as seen by each element
+     side_nquads[nsides*2]                         1, or 4 on the fine side of a 2:1 mortar, 0 at a boundary
+     boundary[nsides]                              0 = interior, else 1 + face id of the domain face
+   The element order is the order of the state arrays.  Sides with nquads 4 on one side are
+   2:1 mortars; iquad runs over the fine elements in face-local (a,b) Morton order. */
+int nemo_gpu_set_mesh(int64_t nelems, const double* delta, const double* center, int64_t nsides,
+                      const int32_t* side_quads, const int8_t* side_faceid,
+                      const int8_t* side_nquads, const int32_t* boundary);
+
+/* Independent runs batched in one mesh (ensembles): group id per element, 0..ngroups-1.
+   Each group gets its own time step and simulation time.  Default: one group. */
+int nemo_gpu_set_groups(int32_t ngroups, const int32_t* group_of_elem);
+
+/* Copy the conserved state host->device.  host points at the first element's state(1,1,1,1);
+   consecutive elements are elem_stride_bytes apart (sizeof(quad_t) when the state sits in the
+   reference's quad_t array, n^3*V*8 for a packed [E][V][n^3] array).  Resets the RK register. */
+int nemo_gpu_upload_state(const double* host, int64_t elem_stride_bytes);
+int nemo_gpu_download_state(double* host, int64_t elem_stride_bytes);
+
+/* hook_calc_timestep_200: dt = 0.5^(D-1) * cfl / (2*N_NODES-1) * min_e min_d (delta_d / lambda_d),
+   lmax = max wave speed.  Device reduction in FP64.  dt_out/lmax_out are host pointers. */
+int nemo_gpu_calc_timestep(double cfl, double* dt_out, double* lmax_out);
+
+/* One RK stage (hook_pre_rk_timestep_300 + hook_mid_rk_timestep_500): rhs of the current
+   state, register update, state update, positivity repair.  stage is 1..5 as rt%rkstage.
+   nbad_out (may be NULL) receives the number of elements whose repair failed. */
+int nemo_gpu_stage(int32_t stage, double dt, double t_stage, int32_t* nbad_out);
+
+/* One full time step (5 stages) with the given dt, replayed from a captured CUDA graph. */
+int nemo_gpu_step(double dt);
+
+/* Run nsteps time steps, or until t_end if t_end > 0 (the last step is clamped), with dt
+   computed on the device before every step (hook_calc_timestep then hook_evolve).  The loop
+   is captured as CUDA graphs; the host syncs once.  t_out, steps_out may be NULL. */
+int nemo_gpu_run(int64_t nsteps, double t_end, double* t_out, int64_t* steps_out);
+
+/* kernel_calc_flux for every element: rhs (packed [E][V][n^3] host array) of the current
+   state, without updating it (source/kernel/mcfv/3d/kernel_flux_mod.f90:280-500). */
+int nemo_gpu_rhs(double* rhs_host);
+
+/* Blending coefficient alpha per element (host array [E]) of the current state. */
+int nemo_gpu_alpha(double* alpha_host);
+
+/* Conserved totals (sum of w_ijk * vol * u) per variable, out[10] (first n_vars used);
+   source/setups/euler/3d/_common_/setup_analyze_mod.f90:28-150. */
+int nemo_gpu_totals(double* out);
+
+/* Simulation time of group 0 and the accumulated repair-failure count. */
+int nemo_gpu_status(double* t_out, int64_t* nbad_total_out);
+
+int nemo_gpu_finalize(void);
+
+/* Copy the last error message (NUL terminated, truncated to len). */
+int nemo_gpu_last_error(char* buf, int32_t len);
+
+/* Timing mode: when on, nemo_gpu_run issues its kernels as plain launches with a CUDA event
+   between consecutive kernels on the library stream (instead of replaying CUDA graphs), and
+   nemo_gpu_kernel_timing reports, for the last run, the summed device time and launch count of
+   the stage kernels and of all kernels. */
+int nemo_gpu_set_timing(int32_t on);
+int nemo_gpu_kernel_timing(double* stage_ms, int64_t* stage_launches, double* total_ms, int64_t* total_launches);
+
+/* The library's CUDA stream (cudaStream_t as an integer), for callers that record their own
+   events on it. */
+int nemo_gpu_stream(uint64_t* stream_out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* NEMO_GPU_H */

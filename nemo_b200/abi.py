@@ -1,0 +1,127 @@
+"""ctypes binding of the C-ABI in include/nemo_gpu.h (libnemo_gpu.so, built in-tree).
+
+There is no CPU fallback: if the library is missing or fails to load, every call raises.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libnemo_gpu.so")
+
+EQN_EULER, EQN_MHD = 0, 1
+VOLFLUX_CHANDRASHEKAR, VOLFLUX_CENTRAL, VOLFLUX_EC_MHD = 0, 1, 2
+SURFFLUX_HLLC, SURFFLUX_RUSANOV, SURFFLUX_HLLD = 0, 1, 2
+PREC_FP64, PREC_FP32 = 0, 1
+IND_NONE, IND_MODAL, IND_LEARNED = 0, 1, 2
+
+STATUS = {0: "OK", 1: "ERR_ARG", 2: "ERR_STATE", 3: "ERR_CUDA", 4: "ERR_REPAIR", 5: "ERR_NONFINITE"}
+
+# Every entry point declared in include/nemo_gpu.h (checked by the CPU tests against the header).
+EXPORTS = [
+    "nemo_gpu_default_cfg", "nemo_gpu_init", "nemo_gpu_operators", "nemo_gpu_set_mesh",
+    "nemo_gpu_set_groups", "nemo_gpu_upload_state", "nemo_gpu_download_state",
+    "nemo_gpu_calc_timestep", "nemo_gpu_stage", "nemo_gpu_step", "nemo_gpu_run", "nemo_gpu_rhs",
+    "nemo_gpu_alpha", "nemo_gpu_totals", "nemo_gpu_status", "nemo_gpu_finalize",
+    "nemo_gpu_last_error", "nemo_gpu_set_timing", "nemo_gpu_kernel_timing", "nemo_gpu_stream",
+]
+
+
+class NemoError(RuntimeError):
+    def __init__(self, func, code, msg):
+        super().__init__(f"{func} -> {STATUS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class NemoCfg(ctypes.Structure):
+    _fields_ = [
+        ("n_nodes", ctypes.c_int32), ("n_vars", ctypes.c_int32), ("eqn", ctypes.c_int32),
+        ("volume_flux", ctypes.c_int32), ("surface_flux", ctypes.c_int32), ("precision", ctypes.c_int32),
+        ("indicator", ctypes.c_int32), ("alpha_smoothing", ctypes.c_int32), ("positivity", ctypes.c_int32),
+        ("non_conservative", ctypes.c_int32),
+        ("kappa", ctypes.c_double), ("mu0", ctypes.c_double), ("cfl", ctypes.c_double),
+        ("alpha_max", ctypes.c_double), ("alpha_min", ctypes.c_double), ("repair_decr", ctypes.c_double),
+        ("glm_ch", ctypes.c_double), ("glm_alpha", ctypes.c_double), ("reserved", ctypes.c_double * 4),
+    ]
+
+
+_LIB = None
+_dp = ctypes.POINTER(ctypes.c_double)
+
+
+def load(path=LIB_PATH):
+    """Load libnemo_gpu.so; raises if it is absent (build it with nemo_b200.build.build())."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(path):
+        raise RuntimeError(f"{path} not found: the CUDA library is required (no CPU fallback); "
+                           "build it with python -m nemo_b200.build")
+    L = ctypes.CDLL(path)
+    i32, i64, dbl = ctypes.c_int32, ctypes.c_int64, ctypes.c_double
+    vp = ctypes.c_void_p
+    sig = {
+        "nemo_gpu_default_cfg": [ctypes.POINTER(NemoCfg)],
+        "nemo_gpu_init": [ctypes.POINTER(NemoCfg)],
+        "nemo_gpu_operators": [i32, vp, vp, vp, vp, vp],
+        "nemo_gpu_set_mesh": [i64, vp, vp, i64, vp, vp, vp, vp],
+        "nemo_gpu_set_groups": [i32, vp],
+        "nemo_gpu_upload_state": [vp, i64],
+        "nemo_gpu_download_state": [vp, i64],
+        "nemo_gpu_calc_timestep": [dbl, ctypes.POINTER(dbl), ctypes.POINTER(dbl)],
+        "nemo_gpu_stage": [i32, dbl, dbl, ctypes.POINTER(i32)],
+        "nemo_gpu_step": [dbl],
+        "nemo_gpu_run": [i64, dbl, ctypes.POINTER(dbl), ctypes.POINTER(i64)],
+        "nemo_gpu_rhs": [vp],
+        "nemo_gpu_alpha": [vp],
+        "nemo_gpu_totals": [vp],
+        "nemo_gpu_status": [ctypes.POINTER(dbl), ctypes.POINTER(i64)],
+        "nemo_gpu_finalize": [],
+        "nemo_gpu_last_error": [ctypes.c_char_p, i32],
+        "nemo_gpu_set_timing": [i32],
+        "nemo_gpu_kernel_timing": [ctypes.POINTER(dbl), ctypes.POINTER(i64), ctypes.POINTER(dbl),
+                                   ctypes.POINTER(i64)],
+        "nemo_gpu_stream": [ctypes.POINTER(ctypes.c_uint64)],
+    }
+    for name, args in sig.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = ctypes.c_int
+    _LIB = L
+    return L
+
+
+def last_error():
+    buf = ctypes.create_string_buffer(1024)
+    load().nemo_gpu_last_error(buf, 1024)
+    return buf.value.decode(errors="replace")
+
+
+def call(name, *args):
+    rc = getattr(load(), name)(*args)
+    if rc != 0:
+        raise NemoError(name, rc, last_error())
+    return rc
+
+
+def default_cfg(**kw):
+    c = NemoCfg()
+    call("nemo_gpu_default_cfg", ctypes.byref(c))
+    for k, v in kw.items():
+        if not hasattr(c, k):
+            raise AttributeError(k)
+        setattr(c, k, v)
+    return c
+
+
+def operators():
+    n = 4
+    x, w = np.zeros(n), np.zeros(n)
+    D, S, Vi = np.zeros((n, n)), np.zeros((n, n)), np.zeros((n, n))
+    call("nemo_gpu_operators", n, x.ctypes.data, w.ctypes.data, D.ctypes.data, S.ctypes.data, Vi.ctypes.data)
+    return x, w, D, S, Vi
+
+
+def ptr(a):
+    return ctypes.c_void_p(a.ctypes.data)

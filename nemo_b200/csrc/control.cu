@@ -1,0 +1,101 @@
+// control.cu -- small kernels that manage the device-side run control and the state layout.
+#include "kernels.h"
+
+namespace nemo {
+
+namespace {
+
+constexpr unsigned long long POS_INF_BITS = 0x7FF0000000000000ull;
+
+__global__ void k_ctrl_reset(Control* c) {
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g < c->ngroups) {
+        c->dtmin_bits[g] = POS_INF_BITS;
+        c->lmax_bits[g] = 0ull;
+    }
+}
+
+__global__ void k_ctrl_set_dt(Control* c, double dt) {
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g < c->ngroups) c->dt[g] = dt;
+    if (g == 0) c->done = 0;
+}
+
+// hook_calc_timestep for the next step, from the CFL bounds accumulated by the previous
+// step's last stage (or by a prepare launch): dt = factor * min(delta/lambda), clamped to t_end.
+__global__ void k_ctrl_step(Control* c) {
+    __shared__ int s_live;
+    if (threadIdx.x == 0) s_live = 0;
+    __syncthreads();
+    for (int g = threadIdx.x; g < c->ngroups; g += blockDim.x) {
+        const double dtmin = __longlong_as_double((long long)c->dtmin_bits[g]);
+        double dt = c->dt_factor * dtmin;
+        const double t = c->t[g];
+        if (c->t_end > 0.0) {
+            if (t >= c->t_end) dt = 0.0;
+            else {
+                if (t + dt > c->t_end) dt = c->t_end - t;
+                atomicOr(&s_live, 1);
+            }
+        } else {
+            atomicOr(&s_live, 1);
+        }
+        if (!(dt >= 0.0) || isinf(dt)) {
+            atomicOr(&c->error, 2);
+            dt = 0.0;
+        }
+        c->dt[g] = dt;
+        c->dtmin_bits[g] = POS_INF_BITS;
+        c->lmax_bits[g] = 0ull;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) c->done = (s_live == 0 || c->error) ? 1 : 0;
+}
+
+// aos[e][v][n] <-> soa[v][e][n]
+__global__ void k_aos_to_soa(const double* __restrict__ aos, double* __restrict__ soa, int64_t E, int nv) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t total = E * nv * NP;
+    if (i >= total) return;
+    const int64_t n = i % NP, v = (i / NP) % nv, e = i / ((int64_t)NP * nv);
+    soa[(v * E + e) * NP + n] = aos[i];
+}
+
+__global__ void k_soa_to_aos(const double* __restrict__ soa, double* __restrict__ aos, int64_t E, int nv) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t total = E * nv * NP;
+    if (i >= total) return;
+    const int64_t n = i % NP, v = (i / NP) % nv, e = i / ((int64_t)NP * nv);
+    aos[i] = soa[(v * E + e) * NP + n];
+}
+
+}  // namespace
+
+cudaError_t launch_ctrl_reset(Control* c, cudaStream_t s) {
+    k_ctrl_reset<<<MAX_GROUPS / 256, 256, 0, s>>>(c);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_ctrl_set_dt(Control* c, double dt, cudaStream_t s) {
+    k_ctrl_set_dt<<<MAX_GROUPS / 256, 256, 0, s>>>(c, dt);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_ctrl_step(Control* c, cudaStream_t s) {
+    k_ctrl_step<<<1, 256, 0, s>>>(c);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_aos_to_soa(const double* aos, double* soa, int64_t E, int nv, cudaStream_t s) {
+    const int64_t total = E * nv * NP;
+    k_aos_to_soa<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(aos, soa, E, nv);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_soa_to_aos(const double* soa, double* aos, int64_t E, int nv, cudaStream_t s) {
+    const int64_t total = E * nv * NP;
+    k_soa_to_aos<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(soa, aos, E, nv);
+    return cudaGetLastError();
+}
+
+}  // namespace nemo

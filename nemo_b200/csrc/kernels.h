@@ -1,0 +1,59 @@
+// kernels.h -- argument blocks and launchers of the device kernels (internal to the library).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/nemo_gpu.h"
+#include "common.cuh"
+
+namespace nemo {
+
+struct StageArgs {
+    int64_t E;
+    const double* u_in;       // [V][E][64]
+    double* u_out;            // [V][E][64]
+    double* reg;              // [V][E][64] LSRK register (FP64)
+    const int32_t* nbr;       // [E][6] conforming face neighbours, -1 domain boundary
+    const double* cdel;       // [E][3] 2/delta
+    const double* delta;      // [E][3]
+    const double* alpha_in;   // raw indicator of u_in [E] (blended runs)
+    double* alpha_out;        // raw indicator of u_out [E] (epilogue) or null
+    double* alpha_used;       // alpha applied in this stage [E] or null
+    const int32_t* group;     // [E] or null (single run)
+    Control* ctrl;
+    double* rhs_out;          // rhs-only launches
+    int32_t stage;            // 0..4
+    int32_t epi_dt;           // last stage: CFL bound of the new state
+    int32_t smooth;           // alpha smoothing
+    int32_t positivity;
+    int32_t surface_flux;
+    int32_t volume_flux;
+};
+
+struct PrepArgs {
+    int64_t E;
+    const double* u;
+    const double* delta;
+    const int32_t* group;
+    double* alpha_out;        // or null
+    int32_t dt_candidates;    // accumulate the CFL bound into ctrl
+    Control* ctrl;
+};
+
+// plain FP64 Euler path (stage_fp64.cu)
+cudaError_t setup_stage_euler64(const OpConsts& ops);
+cudaError_t launch_stage_euler64(const StageArgs& a, bool blend, bool ind, bool rhs_only, cudaStream_t s);
+cudaError_t launch_prepare_euler64(const PrepArgs& a, cudaStream_t s);
+cudaError_t launch_totals64(const double* u, const double* delta, int64_t E, int nv, double* part, double* out,
+                            cudaStream_t s);
+int stage_smem_bytes64();
+
+// control kernels (control.cu)
+cudaError_t launch_ctrl_reset(Control* c, cudaStream_t s);
+cudaError_t launch_ctrl_set_dt(Control* c, double dt, cudaStream_t s);
+cudaError_t launch_ctrl_step(Control* c, cudaStream_t s);
+cudaError_t launch_aos_to_soa(const double* aos, double* soa, int64_t E, int nv, cudaStream_t s);
+cudaError_t launch_soa_to_aos(const double* soa, double* aos, int64_t E, int nv, cudaStream_t s);
+
+}  // namespace nemo

@@ -1,0 +1,739 @@
+// nemo_gpu.cu -- host side of the C-ABI in include/nemo_gpu.h.
+//
+// Owns the device memory, the CUDA stream and the captured step graphs; builds the
+// Gauss-Lobatto operators (the same construction as the reference's kernel_share_mod init,
+// source/kernel/dgsem/weakform/2d/kernel_share_mod.f90:56-151, on Gauss-Lobatto nodes);
+// converts the reference's side connectivity into per-element face-neighbour tables.
+// Compiled with -ffp-contract=off so that the operator matrices are bit-identical to every
+// other IEEE-exact construction of them.
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "kernels.h"
+
+using namespace nemo;
+
+namespace {
+
+// ---- operator construction ------------------------------------------------------------------
+
+// Gauss-Lobatto nodes/weights by Newton on q = L_{N+1} - L_{N-1}, as LegendreGaussLobattoNodesAndWeights
+// (source/utils/interpol_mod.f90:513-582) with its qAndLEvaluation helper.
+void gl_qeval(int N, double x, double& q, double& dq, double& LN) {
+    double a2 = 1.0, a1 = x, d2 = 0.0, d1 = 1.0, dd = 0.0;
+    LN = 0.0;
+    for (int k = 2; k <= N; ++k) {
+        LN = (2.0 * k - 1.0) / k * x * a1 - (k - 1.0) / k * a2;
+        dd = d2 + (2.0 * k - 1.0) * a1;
+        a2 = a1; a1 = LN; d2 = d1; d1 = dd;
+    }
+    const int k = N + 1;
+    const double Lk = (2.0 * k - 1.0) / k * x * LN - (k - 1.0) / k * a2;
+    const double dLk = d2 + (2.0 * k - 1.0) * a1;
+    q = Lk - a2;
+    dq = dLk - d2;
+}
+
+void gl_nodes(int N, double* x, double* w) {
+    const double pi = 4.0 * std::atan(1.0);
+    x[0] = -1.0; w[0] = 2.0 / (N * (N + 1.0)); x[N] = 1.0; w[N] = w[0];
+    double q, dq, LN;
+    for (int j = 1; j <= (N + 1) / 2 - 1; ++j) {
+        x[j] = -std::cos(((j + 0.25) * pi) / N - (3.0 / (8.0 * N * pi)) * (1.0 / (j + 0.25)));
+        for (int it = 0; it <= 4; ++it) {
+            gl_qeval(N, x[j], q, dq, LN);
+            const double step = -q / dq;
+            x[j] = x[j] + step;
+            if (std::fabs(step) <= 4.0e-16 * std::fabs(x[j])) break;
+        }
+        gl_qeval(N, x[j], q, dq, LN);
+        x[N - j] = -x[j];
+        w[j] = 2.0 / (N * (N + 1.0) * (LN * LN));
+        w[N - j] = w[j];
+    }
+    if (N % 2 == 0) {
+        gl_qeval(N, 0.0, q, dq, LN);
+        x[N / 2] = 0.0;
+        w[N / 2] = 2.0 / (N * (N + 1.0) * (LN * LN));
+    }
+}
+
+// Barycentric differentiation matrix (source/utils/interpol_mod.f90:38-81), D[i*n+m] = l_m'(x_i).
+void bary_diff(int n, const double* x, double* D) {
+    double wb[NN];
+    for (int i = 0; i < n; ++i) wb[i] = 1.0;
+    for (int i = 1; i < n; ++i)
+        for (int j = 0; j < i; ++j) {
+            wb[j] = wb[j] * (x[j] - x[i]);
+            wb[i] = wb[i] * (x[i] - x[j]);
+        }
+    for (int i = 0; i < n; ++i) wb[i] = 1.0 / wb[i];
+    for (int i = 0; i < n * n; ++i) D[i] = 0.0;
+    for (int l = 0; l < n; ++l)
+        for (int g = 0; g < n; ++g)
+            if (l != g) {
+                D[g * n + l] = wb[l] / (wb[g] * (x[g] - x[l]));
+                D[g * n + g] = D[g * n + g] - D[g * n + l];
+            }
+}
+
+// Normalised Legendre polynomial (source/utils/interpol_mod.f90:274-311).
+double leg_norm(int N, double x) {
+    double L;
+    if (N == 0) L = 1.0;
+    else if (N == 1) L = x;
+    else {
+        double m2 = 1.0, m1 = x;
+        L = 0.0;
+        for (int i = 2; i <= N; ++i) {
+            L = ((2 * i - 1) * x * m1 - (i - 1) * m2) / i;
+            m2 = m1; m1 = L;
+        }
+    }
+    return L * std::sqrt(N + 0.5);
+}
+
+// Inverse by Doolittle LU without pivoting (source/utils/linalg_mod.f90:123-201).
+void lu_inverse(int n, const double* A, double* C) {
+    double a[NN * NN], L[NN * NN], U[NN * NN], b[NN], d[NN], xx[NN];
+    std::memcpy(a, A, sizeof(double) * n * n);
+    std::fill(L, L + n * n, 0.0);
+    std::fill(U, U + n * n, 0.0);
+    for (int k = 0; k < n - 1; ++k)
+        for (int i = k + 1; i < n; ++i) {
+            const double coeff = a[i * n + k] / a[k * n + k];
+            L[i * n + k] = coeff;
+            for (int j = k + 1; j < n; ++j) a[i * n + j] = a[i * n + j] - coeff * a[k * n + j];
+        }
+    for (int i = 0; i < n; ++i) L[i * n + i] = 1.0;
+    for (int j = 0; j < n; ++j)
+        for (int i = 0; i <= j; ++i) U[i * n + j] = a[i * n + j];
+    for (int col = 0; col < n; ++col) {
+        for (int i = 0; i < n; ++i) b[i] = 0.0;
+        b[col] = 1.0;
+        d[0] = b[0];
+        for (int i = 1; i < n; ++i) {
+            d[i] = b[i];
+            for (int j = 0; j < i; ++j) d[i] = d[i] - L[i * n + j] * d[j];
+        }
+        xx[n - 1] = d[n - 1] / U[(n - 1) * n + n - 1];
+        for (int i = n - 2; i >= 0; --i) {
+            xx[i] = d[i];
+            for (int j = n - 1; j > i; --j) xx[i] = xx[i] - U[i * n + j] * xx[j];
+            xx[i] = xx[i] / U[i * n + i];
+        }
+        for (int i = 0; i < n; ++i) C[i * n + col] = xx[i];
+    }
+}
+
+struct HostOps {
+    double x[NN], w[NN], D[NN * NN], S[NN * NN], V[NN * NN], Vinv[NN * NN];
+};
+
+void build_host_ops(HostOps& h) {
+    gl_nodes(NN - 1, h.x, h.w);
+    bary_diff(NN, h.x, h.D);
+    // split-form matrix S = 2D - W^-1 B (Gassner-Winters-Kopriva 2016); zero diagonal on LGL nodes
+    for (int i = 0; i < NN; ++i)
+        for (int m = 0; m < NN; ++m) h.S[i * NN + m] = i == m ? 0.0 : 2.0 * h.D[i * NN + m];
+    for (int i = 0; i < NN; ++i)
+        for (int j = 0; j < NN; ++j) h.V[i * NN + j] = leg_norm(j, h.x[i]);
+    lu_inverse(NN, h.V, h.Vinv);
+}
+
+// ---- library state ----------------------------------------------------------------------------
+
+struct Lib {
+    bool inited = false;
+    nemo_cfg cfg{};
+    HostOps hops{};
+    OpConsts ops{};
+    cudaStream_t stream = nullptr;
+    std::string err;
+
+    int64_t E = 0;
+    int V = 5;
+    bool has_mesh = false, has_state = false;
+    int ngroups = 1;
+
+    double* u[2] = {nullptr, nullptr};
+    double* reg = nullptr;
+    double* stagebuf = nullptr;   // AoS staging for upload/download
+    double* alpha[2] = {nullptr, nullptr};
+    double* alpha_used = nullptr;
+    int32_t* nbr = nullptr;
+    double* cdel = nullptr;
+    double* delta = nullptr;
+    int32_t* group = nullptr;
+    Control* ctrl = nullptr;
+    double* part = nullptr;       // totals partials [V][E]
+    double* tot = nullptr;        // totals [10]
+    int cur = 0;                  // u[cur] holds the state, alpha[cur] its raw indicator
+    bool prepared = false;        // alpha[cur] and the CFL bound in ctrl are valid for u[cur]
+    bool reg_valid = false;
+
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+
+    bool timing = false;
+    double t_stage_ms = 0.0, t_total_ms = 0.0;
+    int64_t n_stage = 0, n_total = 0;
+};
+
+Lib g;
+
+int fail(int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    std::vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g.err = buf;
+    return code;
+}
+
+#define CK(call)                                                                                 \
+    do {                                                                                         \
+        cudaError_t e_ = (call);                                                                 \
+        if (e_ != cudaSuccess) return fail(NEMO_ERR_CUDA, "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+    } while (0)
+
+void free_dev(void* p) {
+    if (p) cudaFree(p);
+}
+
+void release_graphs() {
+    for (auto& ge : g.graph)
+        if (ge) {
+            cudaGraphExecDestroy(ge);
+            ge = nullptr;
+        }
+}
+
+void release_mesh() {
+    release_graphs();
+    free_dev(g.u[0]); free_dev(g.u[1]); free_dev(g.reg); free_dev(g.stagebuf);
+    free_dev(g.alpha[0]); free_dev(g.alpha[1]); free_dev(g.alpha_used);
+    free_dev(g.nbr); free_dev(g.cdel); free_dev(g.delta); free_dev(g.group);
+    free_dev(g.part);
+    g.u[0] = g.u[1] = g.reg = g.stagebuf = nullptr;
+    g.alpha[0] = g.alpha[1] = g.alpha_used = nullptr;
+    g.nbr = nullptr; g.cdel = g.delta = nullptr; g.group = nullptr; g.part = nullptr;
+    g.has_mesh = g.has_state = false;
+    g.prepared = false;
+}
+
+bool blended() { return g.cfg.indicator != NEMO_IND_NONE; }
+
+StageArgs stage_args(int st, bool rhs_only) {
+    StageArgs a{};
+    a.E = g.E;
+    a.u_in = g.u[g.cur];
+    a.u_out = g.u[g.cur ^ 1];
+    a.reg = g.reg;
+    a.nbr = g.nbr;
+    a.cdel = g.cdel;
+    a.delta = g.delta;
+    a.alpha_in = blended() ? g.alpha[g.cur] : nullptr;
+    a.alpha_out = (blended() && !rhs_only) ? g.alpha[g.cur ^ 1] : nullptr;
+    a.alpha_used = blended() ? g.alpha_used : nullptr;
+    a.group = g.ngroups > 1 ? g.group : nullptr;
+    a.ctrl = g.ctrl;
+    a.rhs_out = nullptr;
+    a.stage = st;
+    a.epi_dt = (st == 4 && !rhs_only) ? 1 : 0;
+    a.smooth = g.cfg.alpha_smoothing;
+    a.positivity = g.cfg.positivity;
+    a.surface_flux = g.cfg.surface_flux;
+    a.volume_flux = g.cfg.volume_flux;
+    return a;
+}
+
+cudaError_t launch_stage(int st, cudaStream_t s) {
+    StageArgs a = stage_args(st, false);
+    cudaError_t e = launch_stage_euler64(a, blended(), blended(), false, s);
+    g.cur ^= 1;
+    return e;
+}
+
+cudaError_t launch_prepare(bool dt_cand, cudaStream_t s) {
+    PrepArgs p{};
+    p.E = g.E;
+    p.u = g.u[g.cur];
+    p.delta = g.delta;
+    p.group = g.ngroups > 1 ? g.group : nullptr;
+    p.alpha_out = blended() ? g.alpha[g.cur] : nullptr;
+    p.dt_candidates = dt_cand ? 1 : 0;
+    p.ctrl = g.ctrl;
+    return launch_prepare_euler64(p, s);
+}
+
+int ensure_ready() {
+    if (!g.inited) return fail(NEMO_ERR_STATE, "nemo_gpu_init has not been called");
+    if (!g.has_mesh) return fail(NEMO_ERR_STATE, "no mesh (nemo_gpu_set_mesh)");
+    if (!g.has_state) return fail(NEMO_ERR_STATE, "no state (nemo_gpu_upload_state)");
+    return NEMO_OK;
+}
+
+// Make alpha[cur] and the CFL bounds in ctrl valid for u[cur].
+int prepare_if_needed() {
+    if (g.prepared) return NEMO_OK;
+    CK(launch_ctrl_reset(g.ctrl, g.stream));
+    CK(launch_prepare(true, g.stream));
+    g.prepared = true;
+    return NEMO_OK;
+}
+
+int check_ctrl_error() {
+    int32_t err = 0;
+    CK(cudaMemcpyAsync(&err, &g.ctrl->error, sizeof err, cudaMemcpyDeviceToHost, g.stream));
+    CK(cudaStreamSynchronize(g.stream));
+    if (err & 1) return fail(NEMO_ERR_CUDA, "a bounded device wait expired (TMA copy did not complete)");
+    if (err & 2) return fail(NEMO_ERR_NONFINITE, "non-finite or negative time step");
+    return NEMO_OK;
+}
+
+int build_graph(int start) {
+    // [ctrl step, stage 1..5] starting from u[start]
+    const int saved = g.cur;
+    g.cur = start;
+    cudaGraph_t graph = nullptr;
+    CK(cudaStreamBeginCapture(g.stream, cudaStreamCaptureModeThreadLocal));
+    cudaError_t e = launch_ctrl_step(g.ctrl, g.stream);
+    for (int st = 0; st < 5 && e == cudaSuccess; ++st) e = launch_stage(st, g.stream);
+    cudaError_t e2 = cudaStreamEndCapture(g.stream, &graph);
+    g.cur = saved;
+    if (e != cudaSuccess) return fail(NEMO_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
+    if (e2 != cudaSuccess) return fail(NEMO_ERR_CUDA, "graph capture end: %s", cudaGetErrorString(e2));
+    cudaError_t e3 = cudaGraphInstantiate(&g.graph[start], graph, 0);
+    cudaGraphDestroy(graph);
+    if (e3 != cudaSuccess) return fail(NEMO_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e3));
+    return NEMO_OK;
+}
+
+}  // namespace
+
+// ================================================================================================
+extern "C" {
+
+int nemo_gpu_default_cfg(nemo_cfg* cfg) {
+    if (!cfg) return fail(NEMO_ERR_ARG, "cfg is NULL");
+    std::memset(cfg, 0, sizeof *cfg);
+    cfg->n_nodes = NN;
+    cfg->n_vars = 5;
+    cfg->eqn = NEMO_EQN_EULER;
+    cfg->volume_flux = NEMO_VOLFLUX_CHANDRASHEKAR;
+    cfg->surface_flux = NEMO_SURFFLUX_HLLC;
+    cfg->precision = NEMO_PREC_FP64;
+    cfg->indicator = NEMO_IND_NONE;
+    cfg->alpha_smoothing = 1;
+    cfg->positivity = 0;
+    cfg->kappa = 1.4;
+    cfg->mu0 = 1.0;
+    cfg->cfl = 0.5;
+    cfg->alpha_max = 0.5;
+    cfg->alpha_min = 0.001;
+    cfg->repair_decr = 0.01;
+    return NEMO_OK;
+}
+
+int nemo_gpu_operators(int32_t n, double* nodes, double* weights, double* dmat, double* smat, double* vinv) {
+    if (n != NN) return fail(NEMO_ERR_ARG, "only n = %d Gauss-Lobatto nodes are compiled (got %d)", NN, n);
+    HostOps h;
+    build_host_ops(h);
+    if (nodes) std::memcpy(nodes, h.x, sizeof h.x);
+    if (weights) std::memcpy(weights, h.w, sizeof h.w);
+    if (dmat) std::memcpy(dmat, h.D, sizeof h.D);
+    if (smat) std::memcpy(smat, h.S, sizeof h.S);
+    if (vinv) std::memcpy(vinv, h.Vinv, sizeof h.Vinv);
+    return NEMO_OK;
+}
+
+int nemo_gpu_init(const nemo_cfg* cfg) {
+    if (!cfg) return fail(NEMO_ERR_ARG, "cfg is NULL");
+    if (cfg->n_nodes != NN) return fail(NEMO_ERR_ARG, "n_nodes must be %d", NN);
+    if (cfg->eqn != NEMO_EQN_EULER || cfg->n_vars != 5)
+        return fail(NEMO_ERR_ARG, "only the Euler equations (n_vars 5) are supported by this build");
+    if (cfg->volume_flux != NEMO_VOLFLUX_CHANDRASHEKAR && cfg->volume_flux != NEMO_VOLFLUX_CENTRAL)
+        return fail(NEMO_ERR_ARG, "unsupported volume flux %d", cfg->volume_flux);
+    if (cfg->surface_flux != NEMO_SURFFLUX_HLLC && cfg->surface_flux != NEMO_SURFFLUX_RUSANOV)
+        return fail(NEMO_ERR_ARG, "unsupported surface flux %d", cfg->surface_flux);
+    if (cfg->precision != NEMO_PREC_FP64) return fail(NEMO_ERR_ARG, "unsupported precision %d", cfg->precision);
+    if (cfg->indicator != NEMO_IND_NONE && cfg->indicator != NEMO_IND_MODAL)
+        return fail(NEMO_ERR_ARG, "unsupported indicator %d", cfg->indicator);
+    if (!(cfg->kappa > 1.0)) return fail(NEMO_ERR_ARG, "kappa must be > 1");
+    int ndev = 0;
+    CK(cudaGetDeviceCount(&ndev));
+    if (ndev < 1) return fail(NEMO_ERR_CUDA, "no CUDA device");
+    if (g.inited) nemo_gpu_finalize();
+    g.cfg = *cfg;
+    g.V = cfg->n_vars;
+    build_host_ops(g.hops);
+    OpConsts& o = g.ops;
+    std::memcpy(o.S, g.hops.S, sizeof o.S);
+    for (int i = 0; i < NN; ++i) o.winv[i] = 1.0 / g.hops.w[i];
+    std::memcpy(o.Vinv, g.hops.Vinv, sizeof o.Vinv);
+    for (int i = 0; i < NN; ++i) o.wt[i] = 0.5 * g.hops.w[i];
+    o.kappa = cfg->kappa;
+    o.km1 = cfg->kappa - 1.0;
+    o.c_enth = 0.5 / (cfg->kappa - 1.0);
+    o.hllc_beta = std::sqrt(0.5 * (cfg->kappa - 1) / cfg->kappa);
+    o.ind_T = 0.5 * std::pow(10.0, -1.8 * std::pow((double)NN, 0.25));
+    const double s = std::log((1.0 - 0.0001) / 0.0001);
+    o.ind_k = -s / o.ind_T;
+    o.alpha_min = cfg->alpha_min;
+    o.alpha_max = cfg->alpha_max;
+    o.one_m_alpha_min = 1.0 - cfg->alpha_min;
+    o.repair_decr = cfg->repair_decr;
+    o.mu0 = cfg->mu0;
+    CK(cudaStreamCreateWithFlags(&g.stream, cudaStreamNonBlocking));
+    CK(setup_stage_euler64(o));
+    CK(cudaMalloc(&g.ctrl, sizeof(Control)));
+    CK(cudaMemset(g.ctrl, 0, sizeof(Control)));
+    CK(cudaMalloc(&g.tot, 16 * sizeof(double)));
+    g.inited = true;
+    g.ngroups = 1;
+    return NEMO_OK;
+}
+
+int nemo_gpu_set_mesh(int64_t nelems, const double* delta, const double* center, int64_t nsides,
+                      const int32_t* side_quads, const int8_t* side_faceid, const int8_t* side_nquads,
+                      const int32_t* boundary) {
+    if (!g.inited) return fail(NEMO_ERR_STATE, "nemo_gpu_init has not been called");
+    if (nelems <= 0 || nsides <= 0) return fail(NEMO_ERR_ARG, "nelems and nsides must be positive");
+    if (!delta || !side_quads || !side_faceid || !side_nquads || !boundary)
+        return fail(NEMO_ERR_ARG, "NULL mesh array");
+    (void)center;
+    const int64_t E = nelems;
+    std::vector<int32_t> nbr(E * 6, -2);
+    for (int64_t s = 0; s < nsides; ++s) {
+        const int n0 = side_nquads[s * 2 + 0], n1 = side_nquads[s * 2 + 1];
+        const int f0 = side_faceid[s * 2 + 0], f1 = side_faceid[s * 2 + 1];
+        const int32_t q0 = side_quads[s * 8 + 0], q1 = side_quads[s * 8 + 4];
+        if (n0 > 1 || n1 > 1) return fail(NEMO_ERR_ARG, "side %lld: 2:1 mortar sides are not supported by this build", (long long)s);
+        if (n0 != 1) return fail(NEMO_ERR_ARG, "side %lld: first half must hold one element", (long long)s);
+        if (f0 < 0 || f0 > 5 || q0 < 0 || q0 >= E) return fail(NEMO_ERR_ARG, "side %lld: bad element/face", (long long)s);
+        if (n1 == 0 || boundary[s] > 0) {
+            nbr[q0 * 6 + f0] = -1;
+        } else {
+            if (f1 < 0 || f1 > 5 || q1 < 0 || q1 >= E) return fail(NEMO_ERR_ARG, "side %lld: bad element/face", (long long)s);
+            if ((f0 >> 1) != (f1 >> 1) || f0 == f1)
+                return fail(NEMO_ERR_ARG, "side %lld: faces %d/%d are not opposite faces of one direction", (long long)s, f0, f1);
+            nbr[q0 * 6 + f0] = q1;
+            nbr[q1 * 6 + f1] = q0;
+        }
+    }
+    for (int64_t i = 0; i < E * 6; ++i)
+        if (nbr[i] == -2) return fail(NEMO_ERR_ARG, "element %lld face %d has no side", (long long)(i / 6), (int)(i % 6));
+    std::vector<double> cd(E * 3);
+    for (int64_t i = 0; i < E * 3; ++i) {
+        if (!(delta[i] > 0.0)) return fail(NEMO_ERR_ARG, "element %lld has non-positive size", (long long)(i / 3));
+        cd[i] = 2.0 / delta[i];
+    }
+    release_mesh();
+    g.E = E;
+    const size_t bytes = sizeof(double) * (size_t)g.V * E * NP;
+    CK(cudaMalloc(&g.u[0], bytes));
+    CK(cudaMalloc(&g.u[1], bytes));
+    CK(cudaMalloc(&g.reg, bytes));
+    CK(cudaMalloc(&g.stagebuf, bytes));
+    CK(cudaMalloc(&g.alpha[0], sizeof(double) * E));
+    CK(cudaMalloc(&g.alpha[1], sizeof(double) * E));
+    CK(cudaMalloc(&g.alpha_used, sizeof(double) * E));
+    CK(cudaMemset(g.alpha[0], 0, sizeof(double) * E));
+    CK(cudaMemset(g.alpha[1], 0, sizeof(double) * E));
+    CK(cudaMemset(g.alpha_used, 0, sizeof(double) * E));
+    CK(cudaMalloc(&g.nbr, sizeof(int32_t) * E * 6));
+    CK(cudaMalloc(&g.cdel, sizeof(double) * E * 3));
+    CK(cudaMalloc(&g.delta, sizeof(double) * E * 3));
+    CK(cudaMalloc(&g.part, sizeof(double) * (size_t)g.V * E));
+    CK(cudaMemcpy(g.nbr, nbr.data(), sizeof(int32_t) * E * 6, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(g.cdel, cd.data(), sizeof(double) * E * 3, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(g.delta, delta, sizeof(double) * E * 3, cudaMemcpyHostToDevice));
+    g.ngroups = 1;
+    Control c{};
+    c.ngroups = 1;
+    c.dt_factor = 0.25 * g.cfg.cfl / (double)(2 * NN - 1);
+    CK(cudaMemcpy(g.ctrl, &c, sizeof c, cudaMemcpyHostToDevice));
+    g.has_mesh = true;
+    return NEMO_OK;
+}
+
+int nemo_gpu_set_groups(int32_t ngroups, const int32_t* group_of_elem) {
+    if (!g.has_mesh) return fail(NEMO_ERR_STATE, "set the mesh first");
+    if (ngroups < 1 || ngroups > MAX_GROUPS) return fail(NEMO_ERR_ARG, "ngroups must be in [1, %d]", MAX_GROUPS);
+    if (ngroups > 1 && !group_of_elem) return fail(NEMO_ERR_ARG, "group_of_elem is NULL");
+    if (ngroups > 1) {
+        for (int64_t e = 0; e < g.E; ++e)
+            if (group_of_elem[e] < 0 || group_of_elem[e] >= ngroups)
+                return fail(NEMO_ERR_ARG, "element %lld has group %d outside [0,%d)", (long long)e, group_of_elem[e], ngroups);
+        if (!g.group) CK(cudaMalloc(&g.group, sizeof(int32_t) * g.E));
+        CK(cudaMemcpy(g.group, group_of_elem, sizeof(int32_t) * g.E, cudaMemcpyHostToDevice));
+    }
+    release_graphs();
+    g.ngroups = ngroups;
+    CK(cudaMemcpy(&g.ctrl->ngroups, &ngroups, sizeof(int32_t), cudaMemcpyHostToDevice));
+    g.prepared = false;
+    return NEMO_OK;
+}
+
+int nemo_gpu_upload_state(const double* host, int64_t stride) {
+    if (!g.has_mesh) return fail(NEMO_ERR_STATE, "set the mesh first");
+    if (!host) return fail(NEMO_ERR_ARG, "host is NULL");
+    const size_t row = sizeof(double) * (size_t)g.V * NP;
+    if (stride < (int64_t)row) return fail(NEMO_ERR_ARG, "element stride %lld < %zu bytes", (long long)stride, row);
+    if (stride == (int64_t)row) CK(cudaMemcpyAsync(g.stagebuf, host, row * g.E, cudaMemcpyHostToDevice, g.stream));
+    else CK(cudaMemcpy2DAsync(g.stagebuf, row, host, (size_t)stride, row, (size_t)g.E, cudaMemcpyHostToDevice, g.stream));
+    g.cur = 0;
+    CK(launch_aos_to_soa(g.stagebuf, g.u[0], g.E, g.V, g.stream));
+    CK(cudaMemsetAsync(g.reg, 0, row * g.E, g.stream));
+    // reset the simulation time and counters
+    Control c{};
+    c.ngroups = g.ngroups;
+    c.dt_factor = 0.25 * g.cfg.cfl / (double)(2 * NN - 1);
+    CK(cudaMemcpyAsync(g.ctrl, &c, sizeof c, cudaMemcpyHostToDevice, g.stream));
+    CK(cudaStreamSynchronize(g.stream));
+    g.has_state = true;
+    g.prepared = false;
+    return NEMO_OK;
+}
+
+int nemo_gpu_download_state(double* host, int64_t stride) {
+    int st = ensure_ready();
+    if (st) return st;
+    if (!host) return fail(NEMO_ERR_ARG, "host is NULL");
+    const size_t row = sizeof(double) * (size_t)g.V * NP;
+    if (stride < (int64_t)row) return fail(NEMO_ERR_ARG, "element stride %lld < %zu bytes", (long long)stride, row);
+    CK(launch_soa_to_aos(g.u[g.cur], g.stagebuf, g.E, g.V, g.stream));
+    if (stride == (int64_t)row) CK(cudaMemcpyAsync(host, g.stagebuf, row * g.E, cudaMemcpyDeviceToHost, g.stream));
+    else CK(cudaMemcpy2DAsync(host, (size_t)stride, g.stagebuf, row, row, (size_t)g.E, cudaMemcpyDeviceToHost, g.stream));
+    CK(cudaStreamSynchronize(g.stream));
+    return NEMO_OK;
+}
+
+int nemo_gpu_calc_timestep(double cfl, double* dt_out, double* lmax_out) {
+    int st = ensure_ready();
+    if (st) return st;
+    if (!(cfl > 0.0)) return fail(NEMO_ERR_ARG, "cfl must be positive");
+    CK(launch_ctrl_reset(g.ctrl, g.stream));
+    CK(launch_prepare(true, g.stream));
+    unsigned long long bits[2];
+    CK(cudaMemcpyAsync(&bits[0], &g.ctrl->dtmin_bits[0], 8, cudaMemcpyDeviceToHost, g.stream));
+    CK(cudaMemcpyAsync(&bits[1], &g.ctrl->lmax_bits[0], 8, cudaMemcpyDeviceToHost, g.stream));
+    CK(cudaStreamSynchronize(g.stream));
+    double dtmin, lmax;
+    std::memcpy(&dtmin, &bits[0], 8);
+    std::memcpy(&lmax, &bits[1], 8);
+    const double dt = 0.25 * cfl / (double)(2 * NN - 1) * dtmin;
+    if (!std::isfinite(dt) || !(dt > 0.0)) return fail(NEMO_ERR_NONFINITE, "time step %g is not positive and finite", dt);
+    if (dt_out) *dt_out = dt;
+    if (lmax_out) *lmax_out = lmax;
+    g.prepared = true;
+    return NEMO_OK;
+}
+
+int nemo_gpu_stage(int32_t stage, double dt, double t_stage, int32_t* nbad_out) {
+    int st = ensure_ready();
+    if (st) return st;
+    (void)t_stage;
+    if (stage < 1 || stage > 5) return fail(NEMO_ERR_ARG, "stage must be 1..5");
+    if (!(dt >= 0.0) || !std::isfinite(dt)) return fail(NEMO_ERR_ARG, "dt must be finite and >= 0");
+    unsigned long long nb0 = 0, nb1 = 0;
+    CK(cudaMemcpyAsync(&nb0, &g.ctrl->nbad, 8, cudaMemcpyDeviceToHost, g.stream));
+    if ((st = prepare_if_needed())) return st;
+    CK(launch_ctrl_set_dt(g.ctrl, dt, g.stream));
+    CK(launch_stage(stage - 1, g.stream));
+    CK(cudaMemcpyAsync(&nb1, &g.ctrl->nbad, 8, cudaMemcpyDeviceToHost, g.stream));
+    if ((st = check_ctrl_error())) return st;
+    if (nbad_out) *nbad_out = (int32_t)(nb1 - nb0);
+    if (nb1 > nb0) return fail(NEMO_ERR_REPAIR, "positivity repair failed on %llu elements", nb1 - nb0);
+    return NEMO_OK;
+}
+
+int nemo_gpu_step(double dt) {
+    int st = ensure_ready();
+    if (st) return st;
+    if (!(dt >= 0.0) || !std::isfinite(dt)) return fail(NEMO_ERR_ARG, "dt must be finite and >= 0");
+    if ((st = prepare_if_needed())) return st;
+    CK(launch_ctrl_set_dt(g.ctrl, dt, g.stream));
+    for (int s = 0; s < 5; ++s) CK(launch_stage(s, g.stream));
+    return check_ctrl_error();
+}
+
+int nemo_gpu_run(int64_t nsteps, double t_end, double* t_out, int64_t* steps_out) {
+    int st = ensure_ready();
+    if (st) return st;
+    if (nsteps <= 0 && !(t_end > 0.0)) return fail(NEMO_ERR_ARG, "give nsteps > 0 or t_end > 0");
+    g.prepared = false;  // the CFL bound must belong to the current state
+    if ((st = prepare_if_needed())) return st;
+    const int64_t prep_launches = 2;
+    CK(cudaMemcpyAsync(&g.ctrl->t_end, &t_end, sizeof(double), cudaMemcpyHostToDevice, g.stream));
+    const int32_t zero = 0;
+    CK(cudaMemcpyAsync(&g.ctrl->done, &zero, sizeof zero, cudaMemcpyHostToDevice, g.stream));
+    unsigned long long steps0 = 0, steps1 = 0;
+    CK(cudaMemcpyAsync(&steps0, &g.ctrl->steps, 8, cudaMemcpyDeviceToHost, g.stream));
+    CK(cudaStreamSynchronize(g.stream));
+    const int start_cur = g.cur;
+    int64_t issued = 0;
+    const int64_t limit = nsteps > 0 ? nsteps : INT64_MAX;
+    cudaEvent_t evs[7] = {};
+    if (g.timing) {
+        for (auto& ev : evs) CK(cudaEventCreate(&ev));
+        g.t_stage_ms = g.t_total_ms = 0.0;
+        g.n_stage = 0;
+        g.n_total = prep_launches;  // counted, not timed
+    } else {
+        for (int s = 0; s < 2; ++s)
+            if (!g.graph[s] && (st = build_graph(s))) return st;
+    }
+    while (issued < limit) {
+        const int64_t chunk = std::min<int64_t>(limit - issued, t_end > 0.0 ? 16 : limit);
+        for (int64_t i = 0; i < chunk; ++i) {
+            if (g.timing) {
+                CK(cudaEventRecord(evs[0], g.stream));
+                CK(launch_ctrl_step(g.ctrl, g.stream));
+                CK(cudaEventRecord(evs[1], g.stream));
+                for (int s = 0; s < 5; ++s) {
+                    CK(launch_stage(s, g.stream));
+                    CK(cudaEventRecord(evs[2 + s], g.stream));
+                }
+                CK(cudaEventSynchronize(evs[6]));
+                float ms;
+                CK(cudaEventElapsedTime(&ms, evs[0], evs[1]));
+                g.t_total_ms += ms;
+                for (int s = 0; s < 5; ++s) {
+                    CK(cudaEventElapsedTime(&ms, evs[1 + s], evs[2 + s]));
+                    g.t_stage_ms += ms;
+                    g.t_total_ms += ms;
+                }
+                g.n_stage += 5;
+                g.n_total += 6;
+            } else {
+                CK(cudaGraphLaunch(g.graph[g.cur], g.stream));
+                g.cur ^= 1;
+            }
+        }
+        issued += chunk;
+        if (t_end > 0.0) {
+            int32_t done = 0;
+            CK(cudaMemcpyAsync(&done, &g.ctrl->done, sizeof done, cudaMemcpyDeviceToHost, g.stream));
+            CK(cudaStreamSynchronize(g.stream));
+            if (done) break;
+        }
+    }
+    if (g.timing)
+        for (auto& ev : evs) cudaEventDestroy(ev);
+    CK(cudaMemcpyAsync(&steps1, &g.ctrl->steps, 8, cudaMemcpyDeviceToHost, g.stream));
+    double t0 = 0.0;
+    CK(cudaMemcpyAsync(&t0, &g.ctrl->t[0], 8, cudaMemcpyDeviceToHost, g.stream));
+    if ((st = check_ctrl_error())) return st;
+    const int64_t done_steps = (int64_t)(steps1 - steps0);
+    g.cur = start_cur ^ (int)(done_steps & 1);
+    if (t_out) *t_out = t0;
+    if (steps_out) *steps_out = done_steps;
+    return NEMO_OK;
+}
+
+int nemo_gpu_rhs(double* rhs_host) {
+    int st = ensure_ready();
+    if (st) return st;
+    if (!rhs_host) return fail(NEMO_ERR_ARG, "rhs_host is NULL");
+    if ((st = prepare_if_needed())) return st;
+    StageArgs a = stage_args(0, true);
+    a.rhs_out = g.stagebuf;
+    a.alpha_out = nullptr;
+    CK(launch_stage_euler64(a, blended(), blended(), true, g.stream));
+    // rhs is in SoA order in stagebuf: convert to AoS via the second state buffer as scratch
+    double* scratch = g.u[g.cur ^ 1];
+    CK(launch_soa_to_aos(g.stagebuf, scratch, g.E, g.V, g.stream));
+    CK(cudaMemcpyAsync(rhs_host, scratch, sizeof(double) * (size_t)g.V * g.E * NP, cudaMemcpyDeviceToHost, g.stream));
+    return check_ctrl_error();
+}
+
+int nemo_gpu_alpha(double* alpha_host) {
+    int st = ensure_ready();
+    if (st) return st;
+    if (!alpha_host) return fail(NEMO_ERR_ARG, "alpha_host is NULL");
+    if (!blended()) {
+        for (int64_t e = 0; e < g.E; ++e) alpha_host[e] = 0.0;
+        return NEMO_OK;
+    }
+    if ((st = prepare_if_needed())) return st;
+    // smoothed alpha as the next stage would use it: run a throw-away rhs launch that records it
+    StageArgs a = stage_args(0, true);
+    a.rhs_out = g.stagebuf;
+    a.alpha_out = nullptr;
+    CK(launch_stage_euler64(a, true, true, true, g.stream));
+    CK(cudaMemcpyAsync(alpha_host, g.alpha_used, sizeof(double) * g.E, cudaMemcpyDeviceToHost, g.stream));
+    return check_ctrl_error();
+}
+
+int nemo_gpu_totals(double* out) {
+    int st = ensure_ready();
+    if (st) return st;
+    if (!out) return fail(NEMO_ERR_ARG, "out is NULL");
+    CK(launch_totals64(g.u[g.cur], g.delta, g.E, g.V, g.part, g.tot, g.stream));
+    double tmp[16] = {0};
+    CK(cudaMemcpyAsync(tmp, g.tot, sizeof(double) * g.V, cudaMemcpyDeviceToHost, g.stream));
+    CK(cudaStreamSynchronize(g.stream));
+    for (int v = 0; v < 10; ++v) out[v] = v < g.V ? tmp[v] : 0.0;
+    return NEMO_OK;
+}
+
+int nemo_gpu_status(double* t_out, int64_t* nbad_out) {
+    int st = ensure_ready();
+    if (st) return st;
+    double t = 0;
+    unsigned long long nb = 0;
+    CK(cudaMemcpyAsync(&t, &g.ctrl->t[0], 8, cudaMemcpyDeviceToHost, g.stream));
+    CK(cudaMemcpyAsync(&nb, &g.ctrl->nbad, 8, cudaMemcpyDeviceToHost, g.stream));
+    CK(cudaStreamSynchronize(g.stream));
+    if (t_out) *t_out = t;
+    if (nbad_out) *nbad_out = (int64_t)nb;
+    return NEMO_OK;
+}
+
+int nemo_gpu_set_timing(int32_t on) {
+    g.timing = on != 0;
+    return NEMO_OK;
+}
+
+int nemo_gpu_kernel_timing(double* stage_ms, int64_t* stage_launches, double* total_ms, int64_t* total_launches) {
+    if (stage_ms) *stage_ms = g.t_stage_ms;
+    if (stage_launches) *stage_launches = g.n_stage;
+    if (total_ms) *total_ms = g.t_total_ms;
+    if (total_launches) *total_launches = g.n_total;
+    return NEMO_OK;
+}
+
+int nemo_gpu_stream(uint64_t* out) {
+    if (!g.inited) return fail(NEMO_ERR_STATE, "nemo_gpu_init has not been called");
+    if (out) *out = (uint64_t)(uintptr_t)g.stream;
+    return NEMO_OK;
+}
+
+int nemo_gpu_finalize(void) {
+    if (!g.inited) return NEMO_OK;
+    cudaStreamSynchronize(g.stream);
+    release_mesh();
+    free_dev(g.ctrl);
+    free_dev(g.tot);
+    g.ctrl = nullptr;
+    g.tot = nullptr;
+    cudaStreamDestroy(g.stream);
+    g.stream = nullptr;
+    g.inited = false;
+    return NEMO_OK;
+}
+
+int nemo_gpu_last_error(char* buf, int32_t len) {
+    if (!buf || len <= 0) return NEMO_ERR_ARG;
+    std::snprintf(buf, (size_t)len, "%s", g.err.c_str());
+    return NEMO_OK;
+}
+
+}  // extern "C"

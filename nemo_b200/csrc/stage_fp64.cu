@@ -1,0 +1,666 @@
+// stage_fp64.cu -- plain FP64 path: one fused kernel per LSRK stage (compiled with -fmad=false).
+//
+// One CTA owns EPC = 8 consecutive elements (a 2x2x2 block on a Morton-ordered brick) and runs
+// 48 threads per element, one per (direction d, line (a,b)).  Per stage and element it does what
+// the reference spreads over hook_pre_rk_timestep_300 and hook_mid_rk_timestep_500:
+//   1. TMA bulk copy (cp.async.bulk, mbarrier) of the 8 elements' SoA state into shared memory;
+//   2. per-node primitives (velocities, pressure, beta = rho/(2p));
+//   3. the two face fluxes at the ends of the thread's line (kernel_fill_faceflux,
+//      source/kernel/mcfv/3d/kernel_flux_mod.f90:47-278; neighbour traces from shared memory
+//      when the neighbour is in the CTA, else from global memory);
+//   4. split-form flux differencing along the line, 6 node pairs in a fixed order, plus the
+//      surface lift, plus (alpha > 0) first-order FV subcells and the convex blend;
+//   5. the LSRK 5-4 register/state update (timedisc_probe, source/timedisc/rungekutta/
+//      low-storage/4-5/timedisc_probe_mod.f90:7-39; rkstep_cb :19-49);
+//   6. the positivity repair (dgfv_repair_3d, source/kernel/mcfv/3d/kernel_validate_mod.f90:159-272);
+//   7. epilogue on the new state: the modal indicator for the next stage and, on the last
+//      stage, the per-element CFL bound for the next time step (kernel_timestep_mod.f90:348-394).
+// The arithmetic follows oracle/nemo_oracle.cpp expression by expression, so the two agree to
+// the last bit except where log/exp enter.
+#include "common.cuh"
+#include "euler_fp64.cuh"
+#include "kernels.h"
+
+namespace nemo {
+
+__constant__ OpConsts c_ops64;
+
+namespace {
+
+constexpr int EPC = 8;          // elements per CTA
+constexpr int TPE = 48;         // threads per element
+constexpr int NT = EPC * TPE;   // 384 threads
+constexpr int V = 5;
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) {
+    return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+
+// Bounded wait on an mbarrier phase; returns false if the bound expired.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned phase) {
+    unsigned addr = smem_u32(bar);
+    for (int it = 0; it < (1 << 24); ++it) {
+        unsigned ok;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(ok) : "r"(addr), "r"(phase) : "memory");
+        if (ok) return true;
+    }
+    return false;
+}
+
+// Stage the tile's state (V arrays of nel*64 doubles, contiguous per variable) into smem.
+__device__ __forceinline__ bool tile_load(double* su, const double* __restrict__ u, int64_t E, int64_t e0, int nel,
+                                          uint64_t* bar, Control* ctrl) {
+    if (threadIdx.x == 0) {
+        unsigned b = smem_u32(bar);
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(b) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned b = smem_u32(bar);
+        unsigned bytes = (unsigned)(nel * NP * 8);
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(b), "r"(bytes * V) : "memory");
+        for (int v = 0; v < V; ++v) {
+            const double* src = u + ((int64_t)v * E + e0) * NP;
+            asm volatile(
+                "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                    smem_u32(su + v * EPC * NP)),
+                "l"(src), "r"(bytes), "r"(b)
+                : "memory");
+        }
+    }
+    bool ok = mbar_wait(bar, 0);
+    if (!ok) {
+        atomicOr(&ctrl->error, 1);
+        mbar_wait(bar, 0);  // second bounded wait for the copies still in flight
+    }
+    return ok;
+}
+
+// Serial repair of one element held in smem (rare path), dgfv_repair_3d with N_NODES = 4.
+__device__ bool repair_elem(double* su, int el, const OpConsts& k) {
+    auto at = [&](int v, int p) -> double& { return su[(v * EPC + el) * NP + p]; };
+    auto node_ok = [&](int p) {
+        double q[5];
+        for (int v = 0; v < V; ++v) q[v] = at(v, p);
+        return isvalid64(q, k);
+    };
+    bool ok = true;
+    for (int p = 0; p < NP; ++p) ok = ok && node_ok(p);
+    if (ok) return true;
+    for (int level = 1; level <= 2; ++level) {
+        int mm = 1 << (level - 1), nn = 1 << (2 - level);
+        double ws = 1.0 / (double)(nn * nn * nn);
+        for (int r = 0; r < mm; ++r)
+            for (int pp = 0; pp < mm; ++pp)
+                for (int q = 0; q < mm; ++q) {
+                    double tiles[8][V], means[V];
+                    for (int t = 0; t < 8; ++t)
+                        for (int v = 0; v < V; ++v) tiles[t][v] = 0.0;
+                    for (int v = 0; v < V; ++v)
+                        for (int kk = 0; kk < 2; ++kk)
+                            for (int jj = 0; jj < 2; ++jj)
+                                for (int ii = 0; ii < 2; ++ii)
+                                    for (int kx = (2 * r + kk) * nn; kx < (2 * r + kk + 1) * nn; ++kx)
+                                        for (int jx = (2 * pp + jj) * nn; jx < (2 * pp + jj + 1) * nn; ++jx)
+                                            for (int ix = (2 * q + ii) * nn; ix < (2 * q + ii + 1) * nn; ++ix) {
+                                                int t = ii + 2 * (jj + 2 * kk);
+                                                tiles[t][v] = tiles[t][v] + ws * at(v, nidx(ix, jx, kx));
+                                            }
+                    bool tv = true;
+                    for (int t = 0; t < 8; ++t) tv = tv && isvalid64(tiles[t], k);
+                    if (tv) continue;
+                    for (int v = 0; v < V; ++v) {
+                        double s = 0.0;
+                        for (int t = 0; t < 8; ++t) s = s + tiles[t][v];
+                        means[v] = 0.125 * s;
+                    }
+                    double hiles[8][V];
+                    for (int t = 0; t < 8; ++t)
+                        for (int v = 0; v < V; ++v) hiles[t][v] = tiles[t][v] - means[v];
+                    double squeeze = 1.0;
+                    while (squeeze > 0.0) {
+                        squeeze = fmax(0.0, squeeze - k.repair_decr);
+                        for (int t = 0; t < 8; ++t)
+                            for (int v = 0; v < V; ++v) tiles[t][v] = means[v] + squeeze * hiles[t][v];
+                        bool tv2 = true;
+                        for (int t = 0; t < 8; ++t) tv2 = tv2 && isvalid64(tiles[t], k);
+                        if (tv2) break;
+                    }
+                    for (int v = 0; v < V; ++v)
+                        for (int kx = 2 * r * nn; kx < (2 * r + 2) * nn; ++kx)
+                            for (int jx = 2 * pp * nn; jx < (2 * pp + 2) * nn; ++jx)
+                                for (int ix = 2 * q * nn; ix < (2 * q + 2) * nn; ++ix) {
+                                    int p = nidx(ix, jx, kx);
+                                    at(v, p) = means[v] + squeeze * (at(v, p) - means[v]);
+                                }
+                }
+    }
+    ok = true;
+    for (int p = 0; p < NP; ++p) ok = ok && node_ok(p);
+    return ok;
+}
+
+}  // namespace
+
+template <bool BLEND, bool IND, bool RHS_ONLY>
+__global__ void __launch_bounds__(NT, 1) k_stage_euler64(StageArgs a) {
+    extern __shared__ __align__(128) double smem[];
+    double* su = smem;                    // [V][EPC][64] state, later the new state
+    double* sp = su + V * EPC * NP;       // [5][EPC][64] vn-free primitives: vx,vy,vz,p,beta; later R_x
+    double* sR = sp + 5 * EPC * NP;       // [2][V][EPC][64] R_y, R_z
+    __shared__ uint64_t bar;
+    __shared__ double s_alpha[EPC];
+    __shared__ int s_bad[EPC];
+    __shared__ unsigned long long s_lam[EPC][3];
+
+    const OpConsts& k = c_ops64;
+    Control* ctrl = a.ctrl;
+    if (!RHS_ONLY && ctrl->done) return;
+
+    const int tid = threadIdx.x;
+    const int64_t E = a.E;
+    const int64_t e0 = (int64_t)blockIdx.x * EPC;
+    const int nel = (int)min((int64_t)EPC, E - e0);
+
+    if (tid < EPC) {
+        s_bad[tid] = 0;
+        s_lam[tid][0] = s_lam[tid][1] = s_lam[tid][2] = 0ull;
+        double al = 0.0;
+        if (IND && tid < nel) {
+            int64_t e = e0 + tid;
+            al = a.alpha_in[e];
+            if (a.smooth) {
+#pragma unroll
+                for (int f = 0; f < 6; ++f) {
+                    int32_t ne = a.nbr[e * 6 + f];
+                    if (ne >= 0) al = fmax(al, 0.5 * a.alpha_in[ne]);
+                }
+            }
+            if (a.alpha_used) a.alpha_used[e] = al;
+        }
+        s_alpha[tid] = al;
+    }
+    if (!tile_load(su, a.u_in, E, e0, nel, &bar, ctrl)) return;
+
+    // per-node primitives
+    for (int p = tid; p < nel * NP; p += NT) {
+        int el = p / NP, n = p % NP;
+        double q[5];
+#pragma unroll
+        for (int v = 0; v < V; ++v) q[v] = su[(v * EPC + el) * NP + n];
+        double pr = pressure64(q, k);
+        sp[(0 * EPC + el) * NP + n] = q[1] / q[0];
+        sp[(1 * EPC + el) * NP + n] = q[2] / q[0];
+        sp[(2 * EPC + el) * NP + n] = q[3] / q[0];
+        sp[(3 * EPC + el) * NP + n] = pr;
+        sp[(4 * EPC + el) * NP + n] = 0.5 * q[0] / pr;
+    }
+    __syncthreads();
+
+    const int el = tid / TPE;
+    const int r = tid % TPE;
+    const int d = r / NF;
+    const int ab = r % NF;
+    const int la = ab & 3, lb = ab >> 2;
+    const bool active = el < nel;
+    const int64_t e = e0 + el;
+    // rotated component c (0..2) of the momentum/velocity -> original index (d + c) % 3
+    const int c0 = d, c1 = (d + 1) % 3, c2 = (d + 2) % 3;
+
+    double t[NN][V];  // direction-d contribution per line node, rotated frame
+    if (active) {
+        // ---- surface fluxes at the two ends of the line (faces 2d, 2d+1 at (la,lb))
+        double Fs[2][V];
+#pragma unroll
+        for (int side = 0; side < 2; ++side) {
+            const int f = 2 * d + side;
+            const int own = line_node(d, la, lb, side ? NN - 1 : 0);
+            double uo[V], un[V];
+            uo[0] = su[(0 * EPC + el) * NP + own];
+            uo[1] = su[((1 + c0) * EPC + el) * NP + own];
+            uo[2] = su[((1 + c1) * EPC + el) * NP + own];
+            uo[3] = su[((1 + c2) * EPC + el) * NP + own];
+            uo[4] = su[(4 * EPC + el) * NP + own];
+            const int32_t ne = a.nbr[e * 6 + f];
+            if (ne >= 0) {
+                const int nn = line_node(d, la, lb, side ? 0 : NN - 1);
+                const int64_t nl = (int64_t)ne - e0;
+                if (nl >= 0 && nl < nel) {
+                    const int nli = (int)nl;
+                    un[0] = su[(0 * EPC + nli) * NP + nn];
+                    un[1] = su[((1 + c0) * EPC + nli) * NP + nn];
+                    un[2] = su[((1 + c1) * EPC + nli) * NP + nn];
+                    un[3] = su[((1 + c2) * EPC + nli) * NP + nn];
+                    un[4] = su[(4 * EPC + nli) * NP + nn];
+                } else {
+                    const double* g = a.u_in;
+                    un[0] = __ldg(g + ((int64_t)0 * E + ne) * NP + nn);
+                    un[1] = __ldg(g + ((int64_t)(1 + c0) * E + ne) * NP + nn);
+                    un[2] = __ldg(g + ((int64_t)(1 + c1) * E + ne) * NP + nn);
+                    un[3] = __ldg(g + ((int64_t)(1 + c2) * E + ne) * NP + nn);
+                    un[4] = __ldg(g + ((int64_t)4 * E + ne) * NP + nn);
+                }
+            } else {
+#pragma unroll
+                for (int v = 0; v < V; ++v) un[v] = uo[v];
+            }
+            if (side) riemann64(a.surface_flux, uo, un, Fs[1], k);
+            else riemann64(a.surface_flux, un, uo, Fs[0], k);
+        }
+
+        // ---- split-form volume flux differencing along the line
+        int idx[NN];
+#pragma unroll
+        for (int i = 0; i < NN; ++i) idx[i] = line_node(d, la, lb, i);
+#pragma unroll
+        for (int i = 0; i < NN; ++i)
+#pragma unroll
+            for (int v = 0; v < V; ++v) t[i][v] = 0.0;
+        const int PI_[6] = {0, 0, 0, 1, 1, 2};
+        const int PM_[6] = {1, 2, 3, 2, 3, 3};
+#pragma unroll
+        for (int pq = 0; pq < 6; ++pq) {
+            const int i = PI_[pq], m = PM_[pq];
+            double F[V];
+            if (a.volume_flux == NEMO_VOLFLUX_CENTRAL) {
+                double ui[V], um[V];
+                ui[0] = su[(0 * EPC + el) * NP + idx[i]];
+                ui[1] = su[((1 + c0) * EPC + el) * NP + idx[i]];
+                ui[2] = su[((1 + c1) * EPC + el) * NP + idx[i]];
+                ui[3] = su[((1 + c2) * EPC + el) * NP + idx[i]];
+                ui[4] = su[(4 * EPC + el) * NP + idx[i]];
+                um[0] = su[(0 * EPC + el) * NP + idx[m]];
+                um[1] = su[((1 + c0) * EPC + el) * NP + idx[m]];
+                um[2] = su[((1 + c1) * EPC + el) * NP + idx[m]];
+                um[3] = su[((1 + c2) * EPC + el) * NP + idx[m]];
+                um[4] = su[(4 * EPC + el) * NP + idx[m]];
+                central64(ui, sp[(3 * EPC + el) * NP + idx[i]], um, sp[(3 * EPC + el) * NP + idx[m]], F);
+            } else {
+                Node5 ni, nm;
+                ni.rho = su[(0 * EPC + el) * NP + idx[i]];
+                ni.vn = sp[(c0 * EPC + el) * NP + idx[i]];
+                ni.vt1 = sp[(c1 * EPC + el) * NP + idx[i]];
+                ni.vt2 = sp[(c2 * EPC + el) * NP + idx[i]];
+                ni.beta = sp[(4 * EPC + el) * NP + idx[i]];
+                nm.rho = su[(0 * EPC + el) * NP + idx[m]];
+                nm.vn = sp[(c0 * EPC + el) * NP + idx[m]];
+                nm.vt1 = sp[(c1 * EPC + el) * NP + idx[m]];
+                nm.vt2 = sp[(c2 * EPC + el) * NP + idx[m]];
+                nm.beta = sp[(4 * EPC + el) * NP + idx[m]];
+                chandrashekar64(ni, nm, F, k);
+            }
+            const double sim = k.S[i * NN + m], smi = k.S[m * NN + i];
+#pragma unroll
+            for (int v = 0; v < V; ++v) {
+                t[i][v] = t[i][v] + sim * F[v];
+                t[m][v] = t[m][v] + smi * F[v];
+            }
+        }
+        // ---- surface lift at the line ends
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+            t[0][v] = t[0][v] + k.winv[0] * (-Fs[0][v]);
+            t[NN - 1][v] = t[NN - 1][v] + k.winv[NN - 1] * Fs[1][v];
+        }
+        // ---- FV subcells and convex blend
+        if (BLEND) {
+            const double al = s_alpha[el];
+            if (al > 0.0) {
+                double Fl[V], Fr[V];
+#pragma unroll
+                for (int v = 0; v < V; ++v) Fl[v] = Fs[0][v];
+#pragma unroll
+                for (int i = 0; i < NN; ++i) {
+                    if (i < NN - 1) {
+                        double uL[V], uR[V];
+                        uL[0] = su[(0 * EPC + el) * NP + idx[i]];
+                        uL[1] = su[((1 + c0) * EPC + el) * NP + idx[i]];
+                        uL[2] = su[((1 + c1) * EPC + el) * NP + idx[i]];
+                        uL[3] = su[((1 + c2) * EPC + el) * NP + idx[i]];
+                        uL[4] = su[(4 * EPC + el) * NP + idx[i]];
+                        uR[0] = su[(0 * EPC + el) * NP + idx[i + 1]];
+                        uR[1] = su[((1 + c0) * EPC + el) * NP + idx[i + 1]];
+                        uR[2] = su[((1 + c1) * EPC + el) * NP + idx[i + 1]];
+                        uR[3] = su[((1 + c2) * EPC + el) * NP + idx[i + 1]];
+                        uR[4] = su[(4 * EPC + el) * NP + idx[i + 1]];
+                        riemann64(a.surface_flux, uL, uR, Fr, k);
+                    } else {
+#pragma unroll
+                        for (int v = 0; v < V; ++v) Fr[v] = Fs[1][v];
+                    }
+#pragma unroll
+                    for (int v = 0; v < V; ++v) {
+                        double fv = k.winv[i] * (Fr[v] - Fl[v]);
+                        t[i][v] = (1.0 - al) * t[i][v] + al * fv;
+                        Fl[v] = Fr[v];
+                    }
+                }
+            }
+        }
+    }
+    __syncthreads();  // all reads of the primitives done: sp becomes R_x
+    if (active) {
+        const double cd = a.cdel[e * 3 + d];
+        double* R = d == 0 ? sp : sR + (d - 1) * V * EPC * NP;
+#pragma unroll
+        for (int i = 0; i < NN; ++i) {
+            const int n = line_node(d, la, lb, i);
+            R[(0 * EPC + el) * NP + n] = cd * t[i][0];
+            R[((1 + c0) * EPC + el) * NP + n] = cd * t[i][1];
+            R[((1 + c1) * EPC + el) * NP + n] = cd * t[i][2];
+            R[((1 + c2) * EPC + el) * NP + n] = cd * t[i][3];
+            R[(4 * EPC + el) * NP + n] = cd * t[i][4];
+        }
+    }
+    __syncthreads();
+
+    // ---- rhs, LSRK register and state update
+    const int st = a.stage;
+    const double A = rk_a(st);
+    const double Cdt = rk_c(st) * ctrl->dt[0];
+    for (int p = tid; p < nel * NP; p += NT) {
+        const int pel = p / NP, n = p % NP;
+        const int64_t pe = e0 + pel;
+        const double cdt = a.group ? rk_c(st) * ctrl->dt[a.group[pe]] : Cdt;
+        bool ok = true;
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+            const int s = (v * EPC + pel) * NP + n;
+            const double Rv = (sp[s] + sR[s]) + sR[V * EPC * NP + s];
+            const double rhs = -Rv;
+            const int64_t g = ((int64_t)v * E + pe) * NP + n;
+            if (RHS_ONLY) {
+                a.rhs_out[g] = rhs;
+            } else {
+                const double rr = st == 0 ? rhs : A * a.reg[g] + rhs;
+                a.reg[g] = rr;
+                su[s] = su[s] + cdt * rr;
+            }
+        }
+        if (!RHS_ONLY && a.positivity) {
+            double q[V];
+#pragma unroll
+            for (int v = 0; v < V; ++v) q[v] = su[(v * EPC + pel) * NP + n];
+            ok = isvalid64(q, k);
+            if (!ok) s_bad[pel] = 1;
+        }
+    }
+    if (RHS_ONLY) return;
+    __syncthreads();
+    if (a.positivity && tid < nel && s_bad[tid]) {
+        if (!repair_elem(su, tid, k)) atomicAdd(&ctrl->nbad, 1ull);
+    }
+    __syncthreads();
+    // ---- store the new state
+    for (int p = tid; p < nel * NP; p += NT) {
+        const int pel = p / NP, n = p % NP;
+#pragma unroll
+        for (int v = 0; v < V; ++v) a.u_out[((int64_t)v * E + e0 + pel) * NP + n] = su[(v * EPC + pel) * NP + n];
+    }
+    if (st == 4 && blockIdx.x == 0 && tid == 0) {
+        for (int g = 0; g < ctrl->ngroups; ++g) ctrl->t[g] = ctrl->t[g] + ctrl->dt[g];
+        ctrl->steps += 1;
+    }
+
+    // ---- epilogue: indicator of the new state (for the next stage)
+    if (a.alpha_out) {
+        double* q = sp;                    // [EPC][64] rho*p
+        double* t1 = sp + EPC * NP;        // [EPC][64]
+        double* t2 = sp + 2 * EPC * NP;    // [EPC][64]
+        for (int p = tid; p < nel * NP; p += NT) {
+            const int pel = p / NP, n = p % NP;
+            double uu[V];
+#pragma unroll
+            for (int v = 0; v < V; ++v) uu[v] = su[(v * EPC + pel) * NP + n];
+            q[pel * NP + n] = uu[0] * pressure64(uu, k);
+        }
+        __syncthreads();
+        // 1D transforms, one output per thread (x, then y, then z)
+        for (int p = tid; p < nel * NP; p += NT) {
+            const int pel = p / NP, n = p % NP;
+            const int ai = n % NN, j = (n / NN) % NN, kk = n / NF;
+            double s = 0.0;
+#pragma unroll
+            for (int i = 0; i < NN; ++i) s = s + k.Vinv[ai * NN + i] * q[pel * NP + nidx(i, j, kk)];
+            t1[pel * NP + n] = s;
+        }
+        __syncthreads();
+        for (int p = tid; p < nel * NP; p += NT) {
+            const int pel = p / NP, n = p % NP;
+            const int ai = n % NN, bj = (n / NN) % NN, kk = n / NF;
+            double s = 0.0;
+#pragma unroll
+            for (int j = 0; j < NN; ++j) s = s + k.Vinv[bj * NN + j] * t1[pel * NP + nidx(ai, j, kk)];
+            t2[pel * NP + n] = s;
+        }
+        __syncthreads();
+        for (int p = tid; p < nel * NP; p += NT) {
+            const int pel = p / NP, n = p % NP;
+            const int ai = n % NN, bj = (n / NN) % NN, cc = n / NF;
+            double s = 0.0;
+#pragma unroll
+            for (int kk = 0; kk < NN; ++kk) s = s + k.Vinv[cc * NN + kk] * t2[pel * NP + nidx(ai, bj, kk)];
+            q[pel * NP + n] = s;  // modal coefficients
+        }
+        __syncthreads();
+        if (tid < nel) {
+            const double* m = q + tid * NP;
+            double total = 0.0, clip1 = 0.0, clip2 = 0.0;
+            for (int cc = 0; cc < NN; ++cc)
+                for (int bj = 0; bj < NN; ++bj)
+                    for (int ai = 0; ai < NN; ++ai) {
+                        const double mv = m[nidx(ai, bj, cc)];
+                        const double e2 = mv * mv;
+                        total = total + e2;
+                        if (ai < NN - 1 && bj < NN - 1 && cc < NN - 1) clip1 = clip1 + e2;
+                        if (ai < NN - 2 && bj < NN - 2 && cc < NN - 2) clip2 = clip2 + e2;
+                    }
+            const double e1 = (total - clip1) / total;
+            const double e2 = (clip1 - clip2) / clip1;
+            const double energy = fmax(e1, e2);
+            double al = 1.0 / (1.0 + exp(k.ind_k * (energy - k.ind_T)));
+            if (al < k.alpha_min) al = 0.0;
+            else if (al > k.one_m_alpha_min) al = 1.0;
+            a.alpha_out[e0 + tid] = fmin(k.alpha_max, al);
+        }
+    }
+
+    // ---- epilogue: CFL bound of the new state (last stage only)
+    if (a.epi_dt) {
+        for (int p = tid; p < nel * NP; p += NT) {
+            const int pel = p / NP, n = p % NP;
+            double uu[V];
+#pragma unroll
+            for (int v = 0; v < V; ++v) uu[v] = su[(v * EPC + pel) * NP + n];
+            double rr[V];
+#pragma unroll
+            for (int dd = 0; dd < 3; ++dd) {
+                rr[0] = uu[0];
+                rr[1] = uu[1 + dd];
+                rr[2] = uu[1 + (dd + 1) % 3];
+                rr[3] = uu[1 + (dd + 2) % 3];
+                rr[4] = uu[4];
+                const double lam = xlambda64(rr, k);
+                atomicMax(&s_lam[pel][dd], (unsigned long long)__double_as_longlong(lam));
+            }
+        }
+        __syncthreads();
+        if (tid < nel) {
+            const int64_t pe = e0 + tid;
+            const double lf = __longlong_as_double((long long)s_lam[tid][0]);
+            const double lg = __longlong_as_double((long long)s_lam[tid][1]);
+            const double lh = __longlong_as_double((long long)s_lam[tid][2]);
+            const double dte = fmin(fmin(a.delta[pe * 3 + 0] / lf, a.delta[pe * 3 + 1] / lg), a.delta[pe * 3 + 2] / lh);
+            const int g = a.group ? a.group[pe] : 0;
+            atomicMin(&ctrl->dtmin_bits[g], (unsigned long long)__double_as_longlong(dte));
+            atomicMax(&ctrl->lmax_bits[g], (unsigned long long)__double_as_longlong(fmax(fmax(lf, lg), lh)));
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Per-element preparation from a state: raw indicator and CFL bound (used before the first
+// stage and by nemo_gpu_calc_timestep).  One CTA per 4 elements, one thread per node.
+
+__global__ void __launch_bounds__(256) k_prepare_euler64(PrepArgs a) {
+    __shared__ double q[4][NP], t1[4][NP], t2[4][NP];
+    __shared__ unsigned long long s_lam[4][3];
+    const OpConsts& k = c_ops64;
+    const int el = threadIdx.x / NP, n = threadIdx.x % NP;
+    const int64_t e = (int64_t)blockIdx.x * 4 + el;
+    const bool act = e < a.E;
+    if (n < 3) s_lam[el][n] = 0ull;
+    double uu[V];
+    if (act) {
+#pragma unroll
+        for (int v = 0; v < V; ++v) uu[v] = a.u[((int64_t)v * a.E + e) * NP + n];
+        q[el][n] = uu[0] * pressure64(uu, k);
+    }
+    __syncthreads();
+    if (act && a.dt_candidates) {
+        double rr[V];
+#pragma unroll
+        for (int dd = 0; dd < 3; ++dd) {
+            rr[0] = uu[0];
+            rr[1] = uu[1 + dd];
+            rr[2] = uu[1 + (dd + 1) % 3];
+            rr[3] = uu[1 + (dd + 2) % 3];
+            rr[4] = uu[4];
+            atomicMax(&s_lam[el][dd], (unsigned long long)__double_as_longlong(xlambda64(rr, k)));
+        }
+    }
+    if (a.alpha_out) {
+        const int ai = n % NN, j = (n / NN) % NN, kk = n / NF;
+        double s = 0.0;
+        if (act) {
+#pragma unroll
+            for (int i = 0; i < NN; ++i) s = s + k.Vinv[ai * NN + i] * q[el][nidx(i, j, kk)];
+        }
+        t1[el][n] = s;
+        __syncthreads();
+        s = 0.0;
+        if (act) {
+#pragma unroll
+            for (int jj = 0; jj < NN; ++jj) s = s + k.Vinv[j * NN + jj] * t1[el][nidx(ai, jj, kk)];
+        }
+        t2[el][n] = s;
+        __syncthreads();
+        s = 0.0;
+        if (act) {
+#pragma unroll
+            for (int kx = 0; kx < NN; ++kx) s = s + k.Vinv[kk * NN + kx] * t2[el][nidx(ai, j, kx)];
+        }
+        q[el][n] = s;
+    }
+    __syncthreads();
+    if (!act || n != 0) return;
+    if (a.alpha_out) {
+        const double* m = q[el];
+        double total = 0.0, clip1 = 0.0, clip2 = 0.0;
+        for (int cc = 0; cc < NN; ++cc)
+            for (int bj = 0; bj < NN; ++bj)
+                for (int ai = 0; ai < NN; ++ai) {
+                    const double mv = m[nidx(ai, bj, cc)];
+                    const double e2 = mv * mv;
+                    total = total + e2;
+                    if (ai < NN - 1 && bj < NN - 1 && cc < NN - 1) clip1 = clip1 + e2;
+                    if (ai < NN - 2 && bj < NN - 2 && cc < NN - 2) clip2 = clip2 + e2;
+                }
+        const double e1 = (total - clip1) / total;
+        const double e2 = (clip1 - clip2) / clip1;
+        const double energy = fmax(e1, e2);
+        double al = 1.0 / (1.0 + exp(k.ind_k * (energy - k.ind_T)));
+        if (al < k.alpha_min) al = 0.0;
+        else if (al > k.one_m_alpha_min) al = 1.0;
+        a.alpha_out[e] = fmin(k.alpha_max, al);
+    }
+    if (a.dt_candidates) {
+        const double lf = __longlong_as_double((long long)s_lam[el][0]);
+        const double lg = __longlong_as_double((long long)s_lam[el][1]);
+        const double lh = __longlong_as_double((long long)s_lam[el][2]);
+        const double dte = fmin(fmin(a.delta[e * 3 + 0] / lf, a.delta[e * 3 + 1] / lg), a.delta[e * 3 + 2] / lh);
+        const int g = a.group ? a.group[e] : 0;
+        atomicMin(&a.ctrl->dtmin_bits[g], (unsigned long long)__double_as_longlong(dte));
+        atomicMax(&a.ctrl->lmax_bits[g], (unsigned long long)__double_as_longlong(fmax(fmax(lf, lg), lh)));
+    }
+}
+
+// Conserved totals: per-element weighted sums in the oracle's order, then a serial sum per
+// variable (deterministic, bit-reproducible).
+__global__ void k_totals_elem64(const double* __restrict__ u, const double* __restrict__ delta, int64_t E, int nv,
+                                double* __restrict__ part) {
+    const OpConsts& k = c_ops64;
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= E) return;
+    const double vol = delta[e * 3 + 0] * delta[e * 3 + 1] * delta[e * 3 + 2];
+    for (int v = 0; v < nv; ++v) {
+        double s = 0.0;
+        const double* ue = u + ((int64_t)v * E + e) * NP;
+        for (int kk = 0; kk < NN; ++kk)
+            for (int j = 0; j < NN; ++j)
+                for (int i = 0; i < NN; ++i) s = s + k.wt[i] * k.wt[j] * k.wt[kk] * ue[nidx(i, j, kk)];
+        part[(int64_t)v * E + e] = vol * s;
+    }
+}
+
+__global__ void k_totals_sum64(const double* __restrict__ part, int64_t E, int nv, double* __restrict__ out) {
+    const int v = threadIdx.x;
+    if (v >= nv) return;
+    double tot = 0.0;
+    for (int64_t e = 0; e < E; ++e) tot = tot + part[(int64_t)v * E + e];
+    out[v] = tot;
+}
+
+// ---------------------------------------------------------------------------------------------
+// launchers
+
+int stage_smem_bytes64() { return (V * EPC * NP + 5 * EPC * NP + 2 * V * EPC * NP) * (int)sizeof(double); }
+
+cudaError_t launch_stage_euler64(const StageArgs& a, bool blend, bool ind, bool rhs_only, cudaStream_t s) {
+    const int grid = (int)((a.E + EPC - 1) / EPC);
+    const int smem = stage_smem_bytes64();
+    (void)ind;
+    if (rhs_only) {
+        if (blend) k_stage_euler64<true, true, true><<<grid, NT, smem, s>>>(a);
+        else k_stage_euler64<false, false, true><<<grid, NT, smem, s>>>(a);
+    } else {
+        if (blend) k_stage_euler64<true, true, false><<<grid, NT, smem, s>>>(a);
+        else k_stage_euler64<false, false, false><<<grid, NT, smem, s>>>(a);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t setup_stage_euler64(const OpConsts& ops) {
+    const int smem = stage_smem_bytes64();
+    cudaError_t err;
+    err = cudaFuncSetAttribute(k_stage_euler64<true, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (err != cudaSuccess) return err;
+    err = cudaFuncSetAttribute(k_stage_euler64<false, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (err != cudaSuccess) return err;
+    err = cudaFuncSetAttribute(k_stage_euler64<true, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (err != cudaSuccess) return err;
+    err = cudaFuncSetAttribute(k_stage_euler64<false, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (err != cudaSuccess) return err;
+    return cudaMemcpyToSymbol(c_ops64, &ops, sizeof(OpConsts));
+}
+
+cudaError_t launch_prepare_euler64(const PrepArgs& a, cudaStream_t s) {
+    const int grid = (int)((a.E + 3) / 4);
+    k_prepare_euler64<<<grid, 256, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_totals64(const double* u, const double* delta, int64_t E, int nv, double* part, double* out,
+                            cudaStream_t s) {
+    k_totals_elem64<<<(unsigned)((E + 127) / 128), 128, 0, s>>>(u, delta, E, nv, part);
+    k_totals_sum64<<<1, 32, 0, s>>>(part, E, nv, out);
+    return cudaGetLastError();
+}
+
+}  // namespace nemo

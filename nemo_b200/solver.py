@@ -1,0 +1,163 @@
+"""Host-side mirror of the reference's kernel/timedisc hook interface, on top of the C-ABI.
+
+The reference's driver (source/driver_mod.f90:62-150) calls, per time step,
+    hook_calc_timestep  -> kernel_timestep_mod::hook_calc_timestep_200   (dt from the CFL bound)
+    hook_evolve         -> timedisc_evolve_mod::hook_evolve_500          (5 LSRK stages, each
+                            hook_pre_rk_timestep_300 [face fluxes] + hook_mid_rk_timestep_500
+                            [rkstep_cb: kernel_evolve + register update])
+and hook_analyze for conserved totals.  `Solver` is the GPU module: the same hooks with the same
+meaning, each a call into libnemo_gpu.so.  Errors come back as NemoError (the reference's
+raise_error path); nothing here computes physics on the CPU.
+
+States on the Python side are structure-of-arrays float64 u[V, E, n^3] (Fortran node order).
+"""
+import ctypes
+
+import numpy as np
+
+from . import abi
+from .abi import call
+
+# LSRK 5-4 (Kennedy-Carpenter 2N) coefficients as the reference's timedisc_const_mod
+# (source/timedisc/rungekutta/low-storage/4-5/timedisc_const_mod.f90:5-29).
+nstages = 5
+a_rk = np.array([0.0, -567301805773.0 / 1357537059087.0, -2404267990393.0 / 2016746695238.0,
+                 -3550918686646.0 / 2091501179385.0, -1275806237668.0 / 842570457699.0])
+b_rk = np.array([0.0, 1432997174477.0 / 9575080441755.0, 2526269341429.0 / 6820363962896.0,
+                 2006345519317.0 / 3224310063776.0, 2802321613138.0 / 2924317926251.0])
+c_rk = np.array([1432997174477.0 / 9575080441755.0, 5161836677717.0 / 13612068292357.0,
+                 1720146321549.0 / 2090206949498.0, 3134564353537.0 / 4481467310338.0,
+                 2277821191437.0 / 14882151754819.0])
+dt_coeffs = b_rk
+
+
+class Runtime:
+    """The fields of the reference's runtime_t the hooks read and write (source/runtime_mod.f90)."""
+
+    def __init__(self, simtime=0.0):
+        self.simtime = simtime
+        self.timestep = 0.0
+        self.maxtimestep = 0.0
+        self.rkstage = 0
+        self.rktimestep = 0.0
+        self.rksimtime = simtime
+        self.nsteps = 0
+        self.ok = True
+        self.message = ""
+
+
+class Solver:
+    """One GPU spatial-operator instance (the library holds one per process)."""
+
+    def __init__(self, cfg, mesh, groups=None):
+        self.cfg = cfg
+        self.mesh = mesh
+        self.V = int(cfg.n_vars)
+        self.E = mesh.E
+        self.n = 4
+        call("nemo_gpu_init", ctypes.byref(cfg))
+        call("nemo_gpu_set_mesh", mesh.E, abi.ptr(mesh.delta), abi.ptr(mesh.center), mesh.S,
+             abi.ptr(mesh.side_quads), abi.ptr(mesh.side_faceid), abi.ptr(mesh.side_nquads),
+             abi.ptr(mesh.boundary))
+        if groups is not None:
+            g = np.ascontiguousarray(groups, dtype=np.int32)
+            call("nemo_gpu_set_groups", int(g.max()) + 1, abi.ptr(g))
+        self.nodes, self.weights = abi.operators()[:2]
+
+    # ---- state transfer (SoA numpy <-> the library's per-element Fortran layout) -------------
+    def upload(self, u):
+        u = np.asarray(u, dtype=np.float64)
+        assert u.shape == (self.V, self.E, self.n ** 3), u.shape
+        aos = np.ascontiguousarray(u.transpose(1, 0, 2))
+        call("nemo_gpu_upload_state", abi.ptr(aos), self.V * self.n ** 3 * 8)
+
+    def upload_aos(self, aos, stride_bytes):
+        """Upload from a host buffer laid out like the reference's quad array (per-element stride)."""
+        call("nemo_gpu_upload_state", ctypes.c_void_p(aos), int(stride_bytes))
+
+    def download(self):
+        aos = np.empty((self.E, self.V, self.n ** 3))
+        call("nemo_gpu_download_state", abi.ptr(aos), self.V * self.n ** 3 * 8)
+        return np.ascontiguousarray(aos.transpose(1, 0, 2))
+
+    # ---- hooks ---------------------------------------------------------------------------------
+    def calc_timestep(self, cfl=None):
+        dt, lm = ctypes.c_double(), ctypes.c_double()
+        call("nemo_gpu_calc_timestep", float(cfl if cfl is not None else self.cfg.cfl), ctypes.byref(dt),
+             ctypes.byref(lm))
+        return dt.value, lm.value
+
+    def stage(self, stage, dt, t_stage=0.0):
+        nbad = ctypes.c_int32(0)
+        call("nemo_gpu_stage", int(stage), float(dt), float(t_stage), ctypes.byref(nbad))
+        return nbad.value
+
+    def step(self, dt):
+        call("nemo_gpu_step", float(dt))
+
+    def run(self, nsteps=0, t_end=0.0):
+        t, s = ctypes.c_double(), ctypes.c_int64()
+        call("nemo_gpu_run", int(nsteps), float(t_end), ctypes.byref(t), ctypes.byref(s))
+        return t.value, s.value
+
+    def rhs(self):
+        aos = np.empty((self.E, self.V, self.n ** 3))
+        call("nemo_gpu_rhs", abi.ptr(aos))
+        return np.ascontiguousarray(aos.transpose(1, 0, 2))
+
+    def alpha(self):
+        a = np.empty(self.E)
+        call("nemo_gpu_alpha", abi.ptr(a))
+        return a
+
+    def totals(self):
+        out = np.zeros(10)
+        call("nemo_gpu_totals", abi.ptr(out))
+        return out[: self.V]
+
+    def status(self):
+        t, nb = ctypes.c_double(), ctypes.c_int64()
+        call("nemo_gpu_status", ctypes.byref(t), ctypes.byref(nb))
+        return t.value, nb.value
+
+    def finalize(self):
+        call("nemo_gpu_finalize")
+
+    # reference-named hooks ------------------------------------------------------------------------
+    def hook_calc_timestep_200(self, rt, cfl=None):
+        """kernel_timestep_mod::hook_calc_timestep_200 (source/kernel/mcfv/3d/kernel_timestep_mod.f90:17-58)."""
+        rt.maxtimestep, _ = self.calc_timestep(cfl)
+        return rt.maxtimestep
+
+    def hook_pre_rk_timestep_300(self, rt):
+        """Face fill + face flux (kernel_hooks_mod.f90:7-20): fused into the stage kernel; no-op."""
+
+    def hook_mid_rk_timestep_500(self, rt):
+        """rkstep_cb over all quads (timedisc_hooks_mod.f90:19-58): one fused stage launch."""
+        try:
+            self.stage(rt.rkstage, rt.timestep, rt.rksimtime)
+        except abi.NemoError as exc:
+            rt.ok, rt.message = False, str(exc)
+
+    def hook_evolve_500(self, rt):
+        """The stage loop of timedisc_evolve_mod::hook_evolve_500 (timedisc_evolve_mod.f90:20-84)."""
+        for stage in range(1, nstages + 1):
+            rt.rkstage = stage
+            rt.rktimestep = rt.timestep * dt_coeffs[stage - 1]
+            rt.rksimtime = rt.simtime + rt.rktimestep
+            self.hook_pre_rk_timestep_300(rt)
+            self.hook_mid_rk_timestep_500(rt)
+            if not rt.ok:
+                return
+
+    def mainloop(self, rt, stop_time, max_steps=None):
+        """driver_mod::mainloop (source/driver_mod.f90:62-150) without I/O: dt, clamp, evolve."""
+        while rt.simtime < stop_time and (max_steps is None or rt.nsteps < max_steps):
+            self.hook_calc_timestep_200(rt)
+            rt.timestep = min(rt.maxtimestep, stop_time - rt.simtime)
+            self.hook_evolve_500(rt)
+            if not rt.ok:
+                break
+            rt.simtime = rt.simtime + rt.timestep
+            rt.nsteps += 1
+        return rt

@@ -1,0 +1,187 @@
+"""ctypes wrapper of the CPU FP64 oracle (liboracle.so, built from nemo_oracle.cpp).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, by __graft_entry__.smoke() and by bench.py's
+CPU-baseline leg, never by the nemo_b200 package.  See nemo_oracle.cpp for what the oracle
+restates and how far its parity with the reference is pinned.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_ip = ctypes.POINTER(ctypes.c_int32)
+
+
+def build(force=False):
+    so = os.path.join(_HERE, "liboracle.so")
+    src = os.path.join(_HERE, "nemo_oracle.cpp")
+    if force or not os.path.exists(so) or os.path.getmtime(so) < os.path.getmtime(src):
+        subprocess.run(["make", "-C", _HERE, "-B" if force else "all"], check=True,
+                       stdout=subprocess.DEVNULL)
+    return so
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        so = os.path.join(_HERE, "liboracle.so")
+        if not os.path.exists(so):
+            build()
+        L = ctypes.CDLL(so)
+        L.or_logmean.restype = ctypes.c_double
+        L.or_logmean.argtypes = [ctypes.c_double, ctypes.c_double]
+        L.or_pressure.restype = ctypes.c_double
+        L.or_pressure.argtypes = [_dp, ctypes.c_double]
+        L.or_flux.argtypes = [ctypes.c_int, _dp, _dp, ctypes.c_double]
+        L.or_riemann.argtypes = [ctypes.c_int, ctypes.c_int, _dp, _dp, _dp, ctypes.c_double]
+        L.or_twopoint.argtypes = [ctypes.c_int, ctypes.c_int, _dp, _dp, _dp, ctypes.c_double]
+        L.or_lgl.argtypes = [ctypes.c_int, _dp, _dp]
+        L.or_operators.argtypes = [_dp] * 5
+        L.or_rk_coeffs.argtypes = [_dp] * 3
+        L.or_alpha.argtypes = [ctypes.c_void_p, ctypes.c_int64, _ip, _dp, _dp, _dp, ctypes.c_int]
+        L.or_rhs.argtypes = [ctypes.c_void_p, ctypes.c_int64, _ip, _dp, _dp, ctypes.c_void_p, _dp,
+                             ctypes.c_int]
+        L.or_timestep.restype = ctypes.c_double
+        L.or_timestep.argtypes = [ctypes.c_void_p, ctypes.c_int64, _dp, _dp, _dp]
+        L.or_stage.restype = ctypes.c_int64
+        L.or_stage.argtypes = [ctypes.c_void_p, ctypes.c_int64, _ip, _dp, ctypes.c_int,
+                               ctypes.c_double, _dp, _dp, ctypes.c_int]
+        L.or_run.restype = ctypes.c_int64
+        L.or_run.argtypes = [ctypes.c_void_p, ctypes.c_int64, _ip, _dp, _dp, ctypes.c_int64,
+                             ctypes.c_double, _dp, ctypes.POINTER(ctypes.c_int64), ctypes.c_int]
+        L.or_totals.argtypes = [ctypes.c_void_p, ctypes.c_int64, _dp, _dp, _dp]
+        L.or_max_threads.restype = ctypes.c_int
+        L.or_repair.restype = ctypes.c_int
+        L.or_repair.argtypes = [ctypes.c_void_p, _dp]
+        _LIB = L
+    return _LIB
+
+
+def _p(a, t=_dp):
+    return a.ctypes.data_as(t)
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def nthreads_default():
+    return int(lib().or_max_threads())
+
+
+def operators():
+    n = 4
+    x, w = np.zeros(n), np.zeros(n)
+    D, S, Vi = np.zeros((n, n)), np.zeros((n, n)), np.zeros((n, n))
+    lib().or_operators(_p(x), _p(w), _p(D), _p(S), _p(Vi))
+    return x, w, D, S, Vi
+
+
+def lgl(N):
+    x, w = np.zeros(N + 1), np.zeros(N + 1)
+    lib().or_lgl(N, _p(x), _p(w))
+    return x, w
+
+
+def rk_coeffs():
+    a, b, c = np.zeros(5), np.zeros(5), np.zeros(5)
+    lib().or_rk_coeffs(_p(a), _p(b), _p(c))
+    return a, b, c
+
+
+def repair(cfg, st):
+    """Positivity repair of one element st[V,64] (copy returned) and whether it succeeded."""
+    st = _f64(st).copy()
+    ok = lib().or_repair(ctypes.byref(cfg), _p(st))
+    return st, bool(ok)
+
+
+def logmean(a, b):
+    return lib().or_logmean(float(a), float(b))
+
+
+def pressure(u, kappa=1.4):
+    u = _f64(u)
+    return lib().or_pressure(_p(u), kappa)
+
+
+def flux(d, u, kappa=1.4):
+    u = _f64(u)
+    f = np.zeros(5)
+    lib().or_flux(d, _p(u), _p(f), kappa)
+    return f
+
+
+def riemann(kind, d, uL, uR, kappa=1.4):
+    uL, uR = _f64(uL), _f64(uR)
+    f = np.zeros(5)
+    lib().or_riemann(kind, d, _p(uL), _p(uR), _p(f), kappa)
+    return f
+
+
+def twopoint(kind, d, u, v, kappa=1.4):
+    u, v = _f64(u), _f64(v)
+    f = np.zeros(5)
+    lib().or_twopoint(kind, d, _p(u), _p(v), _p(f), kappa)
+    return f
+
+
+class Oracle:
+    """Oracle bound to one configuration and mesh (nbr = per-element face neighbours)."""
+
+    def __init__(self, cfg, nbr, delta, nthreads=None):
+        self.cfg = cfg                       # a nemo_b200.abi.NemoCfg (ctypes struct)
+        self.nbr = np.ascontiguousarray(nbr, dtype=np.int32)
+        self.delta = _f64(delta)
+        self.E = self.nbr.shape[0]
+        self.V = int(cfg.n_vars)
+        self.nthreads = nthreads or nthreads_default()
+
+    def _c(self):
+        return ctypes.byref(self.cfg)
+
+    def alpha(self, u):
+        u = _f64(u)
+        a = np.zeros(self.E)
+        lib().or_alpha(self._c(), self.E, _p(self.nbr, _ip), _p(self.delta), _p(u), _p(a), self.nthreads)
+        return a
+
+    def rhs(self, u, alpha=None):
+        u = _f64(u)
+        r = np.zeros_like(u)
+        ap = None
+        if alpha is not None:
+            alpha = _f64(alpha)
+            ap = alpha.ctypes.data
+        lib().or_rhs(self._c(), self.E, _p(self.nbr, _ip), _p(self.delta), _p(u), ap, _p(r), self.nthreads)
+        return r
+
+    def timestep(self, u):
+        u = _f64(u)
+        lm = ctypes.c_double(0)
+        dt = lib().or_timestep(self._c(), self.E, _p(self.delta), _p(u), ctypes.byref(lm))
+        return dt, lm.value
+
+    def stage(self, u, reg, stage, dt):
+        """In place on u and reg (float64 C-contiguous); stage is 0-based."""
+        return lib().or_stage(self._c(), self.E, _p(self.nbr, _ip), _p(self.delta), stage, dt, _p(u), _p(reg),
+                              self.nthreads)
+
+    def run(self, u, nsteps=0, t_end=0.0, t0=0.0):
+        u = _f64(u).copy()
+        t = ctypes.c_double(t0)
+        nbad = ctypes.c_int64(0)
+        steps = lib().or_run(self._c(), self.E, _p(self.nbr, _ip), _p(self.delta), _p(u), int(nsteps),
+                             float(t_end), ctypes.byref(t), ctypes.byref(nbad), self.nthreads)
+        return u, t.value, int(steps), int(nbad.value)
+
+    def totals(self, u):
+        u = _f64(u)
+        out = np.zeros(10)
+        lib().or_totals(self._c(), self.E, _p(self.delta), _p(u), _p(out))
+        return out[: self.V]

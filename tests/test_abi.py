@@ -1,0 +1,96 @@
+"""CPU tests of the C-ABI library: it loads, exports every entry point include/nemo_gpu.h declares,
+its host-built operators equal the oracle's bit for bit, and its argument checks fail cleanly without
+touching a GPU.  No compute call is made here."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+from nemo_b200 import abi, build, mesh
+from oracle import oracle as orc
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+@pytest.fixture(scope="module")
+def lib():
+    build.build()
+    return abi.load()
+
+
+def header_symbols():
+    txt = open(os.path.join(ROOT, "include", "nemo_gpu.h")).read()
+    return sorted(set(re.findall(r"^int\s+(nemo_gpu_\w+)\s*\(", txt, flags=re.M)))
+
+
+def test_exports_every_declared_symbol(lib):
+    syms = header_symbols()
+    assert len(syms) >= 15
+    for s in syms:
+        assert hasattr(lib, s), s
+    assert sorted(abi.EXPORTS) == syms
+
+
+def test_operators_bit_identical_to_oracle(lib):
+    x, w, D, S, Vi = abi.operators()
+    ox, ow, oD, oS, oVi = orc.operators()
+    for a, b in ((x, ox), (w, ow), (D, oD), (S, oS), (Vi, oVi)):
+        assert np.array_equal(a, b)
+    np.testing.assert_allclose(Vi @ np.array([[orc_leg(j, xi) for j in range(4)] for xi in x]), np.eye(4),
+                               atol=1e-14)
+
+
+def orc_leg(n, x):
+    from numpy.polynomial import legendre
+    c = np.zeros(n + 1)
+    c[n] = 1
+    return legendre.legval(x, c) * np.sqrt(n + 0.5)
+
+
+def test_sbp_property_of_split_matrix(lib):
+    """W S is skew-symmetric (S = 2D - W^-1 B with Q + Q^T = B)."""
+    x, w, D, S, Vi = abi.operators()
+    WS = np.diag(w) @ S
+    assert np.max(np.abs(WS + WS.T)) < 1e-14
+    Q = np.diag(w) @ D
+    B = np.diag([-1.0, 0, 0, 1.0])
+    assert np.max(np.abs(Q + Q.T - B)) < 1e-14
+
+
+def test_argument_errors_without_gpu(lib):
+    bad = abi.default_cfg(n_nodes=5)
+    rc = lib.nemo_gpu_init(ctypes.byref(bad))
+    assert rc == 1 and "n_nodes" in abi.last_error()
+    rc = lib.nemo_gpu_operators(3, None, None, None, None, None)
+    assert rc == 1
+    m = mesh.brick(2)
+    rc = lib.nemo_gpu_upload_state(abi.ptr(np.zeros(10)), 8)
+    assert rc == 2   # no mesh yet
+    buf = ctypes.create_string_buffer(8)
+    assert lib.nemo_gpu_last_error(buf, 8) == 0 and len(buf.value) <= 7
+    del m
+
+
+def test_default_cfg(lib):
+    c = abi.default_cfg()
+    assert (c.n_nodes, c.n_vars, c.volume_flux, c.surface_flux, c.precision) == (4, 5, 0, 0, 0)
+    assert c.kappa == 1.4 and c.alpha_max == 0.5 and c.repair_decr == 0.01
+
+
+def test_mesh_generator_invariants():
+    m = mesh.brick(4, 2, 3)
+    nbr = m.neighbors()
+    E = m.E
+    for e in range(E):
+        for f in range(6):
+            ne = nbr[e, f]
+            assert nbr[ne, f ^ 1] == e
+    # Morton order: the first 8 elements of a 4^3 brick form a 2x2x2 block
+    m4 = mesh.brick(4)
+    c = m4.center[:8]
+    assert np.ptp(c, axis=0).max() <= 0.25 + 1e-12
+    mb = mesh.brick(3, 3, 3, periodic=(False, True, False))
+    nb = mb.neighbors()
+    assert (nb[:, 0] == -1).sum() == 9 and (nb[:, 1] == -1).sum() == 9 and (nb[:, 2] >= 0).all()
