@@ -168,6 +168,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="sedov32", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
     args = ap.parse_args()
     assert args.warmup >= 3 or args.impl == "reference" or os.environ.get("NEMO_BENCH_ALLOW_SHORT")
 
@@ -239,34 +240,35 @@ def main():
         with open(tpath) as f:
             traffic = json.load(f).get(args.workload)
 
-    # ---- end to end through the C-ABI: pinned host state in, one step, state out (every step)
-    nbytes = u.nbytes
-    host_in = torch.empty(nbytes // 8, dtype=torch.float64, pin_memory=True)
-    host_out = torch.empty(nbytes // 8, dtype=torch.float64, pin_memory=True)
-    host_in.numpy()[:] = np.ascontiguousarray(u.transpose(1, 0, 2)).ravel()
-    row = V * 64 * 8
-    for _ in range(2):  # warm-up
-        s.upload_aos(host_in.data_ptr(), row)
-        s.run(nsteps=1)
-        abi.call("nemo_gpu_download_state", ctypes.c_void_p(host_out.data_ptr()), row)
-    e2e_steps = max(3, min(args.steps, 10))
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(e2e_steps):
-        s.upload_aos(host_in.data_ptr(), row)
-        s.run(nsteps=1)
-        abi.call("nemo_gpu_download_state", ctypes.c_void_p(host_out.data_ptr()), row)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    e2e_ms = e0.elapsed_time(e1)
-    if dist:
-        t = torch.tensor([e2e_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e_val = world * dof_per_step * e2e_steps / (e2e_ms * 1e-3)
+    e2e_val, e2e_steps, nbytes = None, 0, u.nbytes
+    if not args.no_e2e:
+        # ---- end to end through the C-ABI: pinned host state in, one step, state out (every step)
+        host_in = torch.empty(nbytes // 8, dtype=torch.float64, pin_memory=True)
+        host_out = torch.empty(nbytes // 8, dtype=torch.float64, pin_memory=True)
+        host_in.numpy()[:] = np.ascontiguousarray(u.transpose(1, 0, 2)).ravel()
+        row = V * 64 * 8
+        for _ in range(2):  # warm-up
+            s.upload_aos(host_in.data_ptr(), row)
+            s.run(nsteps=1)
+            abi.call("nemo_gpu_download_state", ctypes.c_void_p(host_out.data_ptr()), row)
+        e2e_steps = max(3, min(args.steps, 10))
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(e2e_steps):
+            s.upload_aos(host_in.data_ptr(), row)
+            s.run(nsteps=1)
+            abi.call("nemo_gpu_download_state", ctypes.c_void_p(host_out.data_ptr()), row)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        e2e_ms = e0.elapsed_time(e1)
+        if dist:
+            t = torch.tensor([e2e_ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_ms = float(t.item())
+        e2e_val = world * dof_per_step * e2e_steps / (e2e_ms * 1e-3)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -295,7 +297,8 @@ def main():
                          "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
                          "kernel": "k_stage_euler64", "algorithmic_bytes_per_launch": bytes_per_launch,
                          "avg_launch_ms": avg_stage_s * 1e3},
-            "e2e": {"value": e2e_val, "unit": "DOF-updates/s", "h2d_bytes_per_step": nbytes,
+            "e2e": None if e2e_val is None else {
+                    "value": e2e_val, "unit": "DOF-updates/s", "h2d_bytes_per_step": nbytes,
                     "d2h_bytes_per_step": nbytes,
                     "note": "per step: upload of the full state from pinned host memory, one time step, "
                             "download of the full state"},

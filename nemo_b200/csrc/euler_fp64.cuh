@@ -8,6 +8,7 @@
 #pragma once
 
 #include "common.cuh"
+#include "pmath64.cuh"
 
 namespace nemo {
 
@@ -107,7 +108,7 @@ __device__ __forceinline__ double logmean64(double a, double b) {
         double u = (x * (x - 2.0) + 1.0) / (x * (x + 2.0) + 1.0);
         return (a + b) * (0.5 - u * (c1 - u * (c2 - c3 * u)));
     }
-    return (a - b) / log(x);
+    return (a - b) / plog64(x);
 }
 
 // Per-node primitive data of the two-point flux: rho, normal/tangential velocities, beta.

@@ -580,42 +580,48 @@ int nemo_gpu_run(int64_t nsteps, double t_end, double* t_out, int64_t* steps_out
     const int start_cur = g.cur;
     int64_t issued = 0;
     const int64_t limit = nsteps > 0 ? nsteps : INT64_MAX;
-    cudaEvent_t evs[7] = {};
+    std::vector<cudaEvent_t> evs;
     if (g.timing) {
+        // one event before the first kernel and one after every kernel; read after the run
+        const int64_t nk = 6 * (nsteps > 0 ? nsteps : 0);
+        if (nk <= 0 || nk > 600000) return fail(NEMO_ERR_ARG, "timing mode needs 0 < nsteps <= 100000");
+        evs.resize(nk + 1);
         for (auto& ev : evs) CK(cudaEventCreate(&ev));
         g.t_stage_ms = g.t_total_ms = 0.0;
         g.n_stage = 0;
         g.n_total = prep_launches;  // counted, not timed
+        CK(cudaEventRecord(evs[0], g.stream));
+        int64_t k = 1;
+        for (int64_t i = 0; i < nsteps; ++i) {
+            CK(launch_ctrl_step(g.ctrl, g.stream));
+            CK(cudaEventRecord(evs[k++], g.stream));
+            for (int s = 0; s < 5; ++s) {
+                CK(launch_stage(s, g.stream));
+                CK(cudaEventRecord(evs[k++], g.stream));
+            }
+        }
+        CK(cudaEventSynchronize(evs[nk]));
+        for (int64_t j = 0; j < nk; ++j) {
+            float ms = 0.f;
+            CK(cudaEventElapsedTime(&ms, evs[j], evs[j + 1]));
+            g.t_total_ms += ms;
+            if (j % 6 != 0) {  // stage kernels; j % 6 == 0 is the control kernel
+                g.t_stage_ms += ms;
+                g.n_stage += 1;
+            }
+            g.n_total += 1;
+        }
+        for (auto& ev : evs) cudaEventDestroy(ev);
+        issued = nsteps;
     } else {
         for (int s = 0; s < 2; ++s)
             if (!g.graph[s] && (st = build_graph(s))) return st;
     }
-    while (issued < limit) {
+    while (!g.timing && issued < limit) {
         const int64_t chunk = std::min<int64_t>(limit - issued, t_end > 0.0 ? 16 : limit);
         for (int64_t i = 0; i < chunk; ++i) {
-            if (g.timing) {
-                CK(cudaEventRecord(evs[0], g.stream));
-                CK(launch_ctrl_step(g.ctrl, g.stream));
-                CK(cudaEventRecord(evs[1], g.stream));
-                for (int s = 0; s < 5; ++s) {
-                    CK(launch_stage(s, g.stream));
-                    CK(cudaEventRecord(evs[2 + s], g.stream));
-                }
-                CK(cudaEventSynchronize(evs[6]));
-                float ms;
-                CK(cudaEventElapsedTime(&ms, evs[0], evs[1]));
-                g.t_total_ms += ms;
-                for (int s = 0; s < 5; ++s) {
-                    CK(cudaEventElapsedTime(&ms, evs[1 + s], evs[2 + s]));
-                    g.t_stage_ms += ms;
-                    g.t_total_ms += ms;
-                }
-                g.n_stage += 5;
-                g.n_total += 6;
-            } else {
-                CK(cudaGraphLaunch(g.graph[g.cur], g.stream));
-                g.cur ^= 1;
-            }
+            CK(cudaGraphLaunch(g.graph[g.cur], g.stream));
+            g.cur ^= 1;
         }
         issued += chunk;
         if (t_end > 0.0) {
@@ -625,8 +631,6 @@ int nemo_gpu_run(int64_t nsteps, double t_end, double* t_out, int64_t* steps_out
             if (done) break;
         }
     }
-    if (g.timing)
-        for (auto& ev : evs) cudaEventDestroy(ev);
     CK(cudaMemcpyAsync(&steps1, &g.ctrl->steps, 8, cudaMemcpyDeviceToHost, g.stream));
     double t0 = 0.0;
     CK(cudaMemcpyAsync(&t0, &g.ctrl->t[0], 8, cudaMemcpyDeviceToHost, g.stream));

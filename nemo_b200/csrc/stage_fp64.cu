@@ -464,7 +464,7 @@ __global__ void __launch_bounds__(NT, 1) k_stage_euler64(StageArgs a) {
             const double e1 = (total - clip1) / total;
             const double e2 = (clip1 - clip2) / clip1;
             const double energy = fmax(e1, e2);
-            double al = 1.0 / (1.0 + exp(k.ind_k * (energy - k.ind_T)));
+            double al = 1.0 / (1.0 + pexp64(k.ind_k * (energy - k.ind_T)));
             if (al < k.alpha_min) al = 0.0;
             else if (al > k.one_m_alpha_min) al = 1.0;
             a.alpha_out[e0 + tid] = fmin(k.alpha_max, al);
@@ -575,7 +575,7 @@ __global__ void __launch_bounds__(256) k_prepare_euler64(PrepArgs a) {
         const double e1 = (total - clip1) / total;
         const double e2 = (clip1 - clip2) / clip1;
         const double energy = fmax(e1, e2);
-        double al = 1.0 / (1.0 + exp(k.ind_k * (energy - k.ind_T)));
+        double al = 1.0 / (1.0 + pexp64(k.ind_k * (energy - k.ind_T)));
         if (al < k.alpha_min) al = 0.0;
         else if (al > k.one_m_alpha_min) al = 1.0;
         a.alpha_out[e] = fmin(k.alpha_max, al);

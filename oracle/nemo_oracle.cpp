@@ -176,6 +176,62 @@ void build_ops(Ops& op) {
     invert_lu(NN, op.V, op.Vinv);
 }
 
+
+// ------------------------------------------------------------------------------------------
+// log and exp from IEEE + - * / only.  The reference calls the Fortran intrinsics; the CPU and
+// GPU libraries differ by up to an ulp, which the logarithmic mean's switch amplifies over many
+// stages, so the oracle and the plain CUDA path both use this construction (the CUDA copy is
+// nemo_b200/csrc/pmath64.cuh).  log: x = 2^e m, m in [sqrt(1/2), sqrt(2)), log m = 2 atanh(s),
+// s = (m-1)/(m+1), atanh series to s^21; e ln2 in a Cody-Waite split.  exp: y = k ln2 + r,
+// Taylor polynomial of e^r to r^13/13!, 2^k through the exponent bits.  Within 3 ulp.
+constexpr double LN2_HI = 0x1.62e42feep-1;
+constexpr double LN2_LO = 0x1.a39ef35793c76p-33;
+constexpr double INV_LN2 = 0x1.71547652b82fep+0;
+
+double own_log(double x) {
+    if (!(x > 0.0)) return x == 0.0 ? -HUGE_VAL : std::nan("");
+    if (std::isinf(x)) return x;
+    int shift = 0;
+    if (x < 2.2250738585072014e-308) { x = x * 18014398509481984.0; shift = 54; }
+    uint64_t b;
+    std::memcpy(&b, &x, 8);
+    int e = (int)((b >> 52) & 0x7ff) - 1023 - shift;
+    uint64_t mb = (b & 0x000fffffffffffffULL) | 0x3ff0000000000000ULL;
+    double m;
+    std::memcpy(&m, &mb, 8);
+    if (m > 1.4142135623730951) { m = 0.5 * m; e = e + 1; }
+    double s = (m - 1.0) / (m + 1.0);
+    double z = s * s;
+    double p = 1.0 / 21.0;
+    const double c[10] = {1.0 / 19.0, 1.0 / 17.0, 1.0 / 15.0, 1.0 / 13.0, 1.0 / 11.0,
+                          1.0 / 9.0,  1.0 / 7.0,  1.0 / 5.0,  1.0 / 3.0,  1.0};
+    for (int i = 0; i < 10; ++i) p = p * z + c[i];
+    double lm = (2.0 * s) * p;
+    double de = (double)e;
+    return de * LN2_HI + (lm + de * LN2_LO);
+}
+
+double own_exp(double y) {
+    if (y != y) return y;
+    if (y > 709.78) return HUGE_VAL;
+    if (y < -745.2) return 0.0;
+    double kd = std::nearbyint(y * INV_LN2);
+    double r = (y - kd * LN2_HI) - kd * LN2_LO;
+    const double c[13] = {1.0 / 479001600.0, 1.0 / 39916800.0, 1.0 / 3628800.0, 1.0 / 362880.0,
+                          1.0 / 40320.0,     1.0 / 5040.0,     1.0 / 720.0,     1.0 / 120.0,
+                          1.0 / 24.0,        1.0 / 6.0,        0.5,             1.0,
+                          1.0};
+    double p = 1.0 / 6227020800.0;
+    for (int i = 0; i < 13; ++i) p = p * r + c[i];
+    int k = (int)kd;
+    if (k > 1023) { p = p * 0x1p1023; k -= 1023; }
+    if (k < -1022) { p = p * 0x1p-1022; k += 1022; if (k < -1022) return 0.0; }
+    uint64_t sb = (uint64_t)(int64_t)(k + 1023) << 52;
+    double sc;
+    std::memcpy(&sc, &sb, 8);
+    return p * sc;
+}
+
 // ------------------------------------------------------------------------------------------
 // Euler physics (source/equations/euler/equations_mod.f90)
 
@@ -285,7 +341,7 @@ inline double logmean_abs(double a, double b) {
         double u = (x * (x - 2.0) + 1.0) / (x * (x + 2.0) + 1.0);
         return (a + b) * (0.5 - u * (c1 - u * (c2 - c3 * u)));
     }
-    return (a - b) / std::log(x);
+    return (a - b) / own_log(x);
 }
 
 // Chandrashekar EC/KEP flux, two_point_flux_mod.f90:34-77
@@ -409,7 +465,7 @@ double indicator_alpha(const Ctx& c, const double (*ue)[VMAX]) {
     double energy = std::max(e1, e2);
     const double T = 0.5 * std::pow(10.0, -1.8 * std::pow((double)NN, 0.25));
     const double s = std::log((1.0 - 0.0001) / 0.0001);
-    double alpha = 1.0 / (1.0 + std::exp(-s / T * (energy - T)));
+    double alpha = 1.0 / (1.0 + own_exp(-s / T * (energy - T)));
     if (alpha < c.cfg.alpha_min) alpha = 0.0;
     else if (alpha > 1.0 - c.cfg.alpha_min) alpha = 1.0;
     return std::min(c.cfg.alpha_max, alpha);
@@ -790,6 +846,9 @@ int or_repair(const nemo_cfg* cfg, double* st) {
         for (int p = 0; p < NP; ++p) st[v * NP + p] = s[p][v];
     return ok ? 1 : 0;
 }
+
+double or_log(double x) { return own_log(x); }
+double or_exp(double x) { return own_exp(x); }
 
 int or_max_threads(void) {
 #ifdef _OPENMP

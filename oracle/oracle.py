@@ -56,6 +56,10 @@ def lib():
                              ctypes.c_double, _dp, ctypes.POINTER(ctypes.c_int64), ctypes.c_int]
         L.or_totals.argtypes = [ctypes.c_void_p, ctypes.c_int64, _dp, _dp, _dp]
         L.or_max_threads.restype = ctypes.c_int
+        L.or_log.restype = ctypes.c_double
+        L.or_log.argtypes = [ctypes.c_double]
+        L.or_exp.restype = ctypes.c_double
+        L.or_exp.argtypes = [ctypes.c_double]
         L.or_repair.restype = ctypes.c_int
         L.or_repair.argtypes = [ctypes.c_void_p, _dp]
         _LIB = L

@@ -136,6 +136,32 @@ def test_twopoint_symmetry():
         np.testing.assert_allclose(orc.twopoint(0, 0, u, v), orc.twopoint(0, 0, v, u), rtol=1e-13, atol=1e-14)
 
 
+def test_own_log_exp_accuracy():
+    """The oracle's (and the plain CUDA path's) log/exp stay within 3 ulp (log) and 2 ulp (exp) of the correctly rounded
+    values: about as close to the reference's intrinsic log/exp as two libms are to each other."""
+    rng = np.random.default_rng(0)
+    L = orc.lib()
+    xs = np.concatenate([rng.uniform(0.5, 2.0, 3000), np.exp(rng.uniform(-700, 700, 3000)),
+                         1.0 + rng.uniform(-1e-4, 1e-4, 2000), [1.0, 2.0, 0.5, 1e-310]])
+    worst = 0.0
+    for x in xs:
+        ref = np.log(np.longdouble(x))
+        got = L.or_log(float(x))
+        if ref != 0:
+            worst = max(worst, float(abs(np.longdouble(got) - ref) / np.spacing(np.float64(abs(ref)))))
+    assert worst <= 3.0, worst
+    assert L.or_log(1.0) == 0.0
+    ys = np.concatenate([rng.uniform(-700, 700, 4000), rng.uniform(-1, 1, 2000), [0.0, -745.0, 709.7]])
+    worst = 0.0
+    for y in ys:
+        ref = np.exp(np.longdouble(y))
+        got = L.or_exp(float(y))
+        if np.isfinite(ref) and ref > 2.3e-308:
+            worst = max(worst, float(abs(np.longdouble(got) - ref) / np.spacing(np.float64(ref))))
+    assert worst <= 2.0, worst
+    assert L.or_exp(0.0) == 1.0 and L.or_exp(-800.0) == 0.0 and np.isinf(L.or_exp(800.0))
+
+
 def test_logmean_series_branch():
     # near the switch the series and the direct formula agree to the conditioning of the latter
     for a in (0.5, 1.0, 3.0):
