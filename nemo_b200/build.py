@@ -19,6 +19,7 @@ SOURCES = {
     "nemo_gpu.cu": [],
     "control.cu": [],
     "stage_fp64.cu": ["-fmad=false"],
+    "stage_fp32.cu": ["--use_fast_math"],
 }
 
 

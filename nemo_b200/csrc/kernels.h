@@ -49,6 +49,11 @@ cudaError_t launch_totals64(const double* u, const double* delta, int64_t E, int
                             cudaStream_t s);
 int stage_smem_bytes64();
 
+// FP32-bulk Euler path (stage_fp32.cu)
+cudaError_t setup_stage_euler32(const OpConsts& ops);
+cudaError_t launch_stage_euler32(const StageArgs& a, bool blend, bool rhs_only, cudaStream_t s);
+int stage_smem_bytes32();
+
 // control kernels (control.cu)
 cudaError_t launch_ctrl_reset(Control* c, cudaStream_t s);
 cudaError_t launch_ctrl_set_dt(Control* c, double dt, cudaStream_t s);

@@ -253,9 +253,14 @@ StageArgs stage_args(int st, bool rhs_only) {
     return a;
 }
 
+cudaError_t launch_stage_any(const StageArgs& a, bool rhs_only, cudaStream_t s) {
+    if (g.cfg.precision == NEMO_PREC_FP32) return launch_stage_euler32(a, blended(), rhs_only, s);
+    return launch_stage_euler64(a, blended(), blended(), rhs_only, s);
+}
+
 cudaError_t launch_stage(int st, cudaStream_t s) {
     StageArgs a = stage_args(st, false);
-    cudaError_t e = launch_stage_euler64(a, blended(), blended(), false, s);
+    cudaError_t e = launch_stage_any(a, false, s);
     g.cur ^= 1;
     return e;
 }
@@ -362,7 +367,8 @@ int nemo_gpu_init(const nemo_cfg* cfg) {
         return fail(NEMO_ERR_ARG, "unsupported volume flux %d", cfg->volume_flux);
     if (cfg->surface_flux != NEMO_SURFFLUX_HLLC && cfg->surface_flux != NEMO_SURFFLUX_RUSANOV)
         return fail(NEMO_ERR_ARG, "unsupported surface flux %d", cfg->surface_flux);
-    if (cfg->precision != NEMO_PREC_FP64) return fail(NEMO_ERR_ARG, "unsupported precision %d", cfg->precision);
+    if (cfg->precision != NEMO_PREC_FP64 && cfg->precision != NEMO_PREC_FP32)
+        return fail(NEMO_ERR_ARG, "unsupported precision %d", cfg->precision);
     if (cfg->indicator != NEMO_IND_NONE && cfg->indicator != NEMO_IND_MODAL)
         return fail(NEMO_ERR_ARG, "unsupported indicator %d", cfg->indicator);
     if (!(cfg->kappa > 1.0)) return fail(NEMO_ERR_ARG, "kappa must be > 1");
@@ -392,6 +398,7 @@ int nemo_gpu_init(const nemo_cfg* cfg) {
     o.mu0 = cfg->mu0;
     CK(cudaStreamCreateWithFlags(&g.stream, cudaStreamNonBlocking));
     CK(setup_stage_euler64(o));
+    CK(setup_stage_euler32(o));
     CK(cudaMalloc(&g.ctrl, sizeof(Control)));
     CK(cudaMemset(g.ctrl, 0, sizeof(Control)));
     CK(cudaMalloc(&g.tot, 16 * sizeof(double)));
@@ -650,7 +657,7 @@ int nemo_gpu_rhs(double* rhs_host) {
     StageArgs a = stage_args(0, true);
     a.rhs_out = g.stagebuf;
     a.alpha_out = nullptr;
-    CK(launch_stage_euler64(a, blended(), blended(), true, g.stream));
+    CK(launch_stage_any(a, true, g.stream));
     // rhs is in SoA order in stagebuf: convert to AoS via the second state buffer as scratch
     double* scratch = g.u[g.cur ^ 1];
     CK(launch_soa_to_aos(g.stagebuf, scratch, g.E, g.V, g.stream));
@@ -671,7 +678,7 @@ int nemo_gpu_alpha(double* alpha_host) {
     StageArgs a = stage_args(0, true);
     a.rhs_out = g.stagebuf;
     a.alpha_out = nullptr;
-    CK(launch_stage_euler64(a, true, true, true, g.stream));
+    CK(launch_stage_any(a, true, g.stream));
     CK(cudaMemcpyAsync(alpha_host, g.alpha_used, sizeof(double) * g.E, cudaMemcpyDeviceToHost, g.stream));
     return check_ctrl_error();
 }

@@ -4,7 +4,7 @@
 // 48 threads per element, one per (direction d, line (a,b)).  Per stage and element it does what
 // the reference spreads over hook_pre_rk_timestep_300 and hook_mid_rk_timestep_500:
 //   1. TMA bulk copy (cp.async.bulk, mbarrier) of the 8 elements' SoA state into shared memory;
-//   2. per-node primitives (velocities, pressure, beta = rho/(2p));
+//   2. per-node primitives (velocities, beta_d = rho/(2 p_d) per direction);
 //   3. the two face fluxes at the ends of the thread's line (kernel_fill_faceflux,
 //      source/kernel/mcfv/3d/kernel_flux_mod.f90:47-278; neighbour traces from shared memory
 //      when the neighbour is in the CTA, else from global memory);
@@ -20,6 +20,7 @@
 #include "common.cuh"
 #include "euler_fp64.cuh"
 #include "kernels.h"
+#include "repair64.cuh"
 
 namespace nemo {
 
@@ -82,78 +83,14 @@ __device__ __forceinline__ bool tile_load(double* su, const double* __restrict__
     return ok;
 }
 
-// Serial repair of one element held in smem (rare path), dgfv_repair_3d with N_NODES = 4.
-__device__ bool repair_elem(double* su, int el, const OpConsts& k) {
-    auto at = [&](int v, int p) -> double& { return su[(v * EPC + el) * NP + p]; };
-    auto node_ok = [&](int p) {
-        double q[5];
-        for (int v = 0; v < V; ++v) q[v] = at(v, p);
-        return isvalid64(q, k);
-    };
-    bool ok = true;
-    for (int p = 0; p < NP; ++p) ok = ok && node_ok(p);
-    if (ok) return true;
-    for (int level = 1; level <= 2; ++level) {
-        int mm = 1 << (level - 1), nn = 1 << (2 - level);
-        double ws = 1.0 / (double)(nn * nn * nn);
-        for (int r = 0; r < mm; ++r)
-            for (int pp = 0; pp < mm; ++pp)
-                for (int q = 0; q < mm; ++q) {
-                    double tiles[8][V], means[V];
-                    for (int t = 0; t < 8; ++t)
-                        for (int v = 0; v < V; ++v) tiles[t][v] = 0.0;
-                    for (int v = 0; v < V; ++v)
-                        for (int kk = 0; kk < 2; ++kk)
-                            for (int jj = 0; jj < 2; ++jj)
-                                for (int ii = 0; ii < 2; ++ii)
-                                    for (int kx = (2 * r + kk) * nn; kx < (2 * r + kk + 1) * nn; ++kx)
-                                        for (int jx = (2 * pp + jj) * nn; jx < (2 * pp + jj + 1) * nn; ++jx)
-                                            for (int ix = (2 * q + ii) * nn; ix < (2 * q + ii + 1) * nn; ++ix) {
-                                                int t = ii + 2 * (jj + 2 * kk);
-                                                tiles[t][v] = tiles[t][v] + ws * at(v, nidx(ix, jx, kx));
-                                            }
-                    bool tv = true;
-                    for (int t = 0; t < 8; ++t) tv = tv && isvalid64(tiles[t], k);
-                    if (tv) continue;
-                    for (int v = 0; v < V; ++v) {
-                        double s = 0.0;
-                        for (int t = 0; t < 8; ++t) s = s + tiles[t][v];
-                        means[v] = 0.125 * s;
-                    }
-                    double hiles[8][V];
-                    for (int t = 0; t < 8; ++t)
-                        for (int v = 0; v < V; ++v) hiles[t][v] = tiles[t][v] - means[v];
-                    double squeeze = 1.0;
-                    while (squeeze > 0.0) {
-                        squeeze = fmax(0.0, squeeze - k.repair_decr);
-                        for (int t = 0; t < 8; ++t)
-                            for (int v = 0; v < V; ++v) tiles[t][v] = means[v] + squeeze * hiles[t][v];
-                        bool tv2 = true;
-                        for (int t = 0; t < 8; ++t) tv2 = tv2 && isvalid64(tiles[t], k);
-                        if (tv2) break;
-                    }
-                    for (int v = 0; v < V; ++v)
-                        for (int kx = 2 * r * nn; kx < (2 * r + 2) * nn; ++kx)
-                            for (int jx = 2 * pp * nn; jx < (2 * pp + 2) * nn; ++jx)
-                                for (int ix = 2 * q * nn; ix < (2 * q + 2) * nn; ++ix) {
-                                    int p = nidx(ix, jx, kx);
-                                    at(v, p) = means[v] + squeeze * (at(v, p) - means[v]);
-                                }
-                }
-    }
-    ok = true;
-    for (int p = 0; p < NP; ++p) ok = ok && node_ok(p);
-    return ok;
-}
-
 }  // namespace
 
 template <bool BLEND, bool IND, bool RHS_ONLY>
 __global__ void __launch_bounds__(NT, 1) k_stage_euler64(StageArgs a) {
     extern __shared__ __align__(128) double smem[];
     double* su = smem;                    // [V][EPC][64] state, later the new state
-    double* sp = su + V * EPC * NP;       // [5][EPC][64] vn-free primitives: vx,vy,vz,p,beta; later R_x
-    double* sR = sp + 5 * EPC * NP;       // [2][V][EPC][64] R_y, R_z
+    double* sp = su + V * EPC * NP;       // [6][EPC][64] vx,vy,vz,beta_x,beta_y,beta_z; later R_x
+    double* sR = sp + 6 * EPC * NP;       // [2][V][EPC][64] R_y, R_z
     __shared__ uint64_t bar;
     __shared__ double s_alpha[EPC];
     __shared__ int s_bad[EPC];
@@ -188,18 +125,22 @@ __global__ void __launch_bounds__(NT, 1) k_stage_euler64(StageArgs a) {
     }
     if (!tile_load(su, a.u_in, E, e0, nel, &bar, ctrl)) return;
 
-    // per-node primitives
+    // per-node primitives: velocities and, per direction d, beta_d = rho/(2 p_d) where p_d is the
+    // pressure of the state rotated into direction d (the reference evaluates the two-point flux on
+    // the rotated state, so the kinetic-energy sum runs in the rotated component order)
     for (int p = tid; p < nel * NP; p += NT) {
         int el = p / NP, n = p % NP;
         double q[5];
 #pragma unroll
         for (int v = 0; v < V; ++v) q[v] = su[(v * EPC + el) * NP + n];
-        double pr = pressure64(q, k);
         sp[(0 * EPC + el) * NP + n] = q[1] / q[0];
         sp[(1 * EPC + el) * NP + n] = q[2] / q[0];
         sp[(2 * EPC + el) * NP + n] = q[3] / q[0];
-        sp[(3 * EPC + el) * NP + n] = pr;
-        sp[(4 * EPC + el) * NP + n] = 0.5 * q[0] / pr;
+#pragma unroll
+        for (int dd = 0; dd < 3; ++dd) {
+            double r[5] = {q[0], q[1 + dd], q[1 + (dd + 1) % 3], q[1 + (dd + 2) % 3], q[4]};
+            sp[((3 + dd) * EPC + el) * NP + n] = 0.5 * q[0] / pressure64(r, k);
+        }
     }
     __syncthreads();
 
@@ -280,19 +221,19 @@ __global__ void __launch_bounds__(NT, 1) k_stage_euler64(StageArgs a) {
                 um[2] = su[((1 + c1) * EPC + el) * NP + idx[m]];
                 um[3] = su[((1 + c2) * EPC + el) * NP + idx[m]];
                 um[4] = su[(4 * EPC + el) * NP + idx[m]];
-                central64(ui, sp[(3 * EPC + el) * NP + idx[i]], um, sp[(3 * EPC + el) * NP + idx[m]], F);
+                central64(ui, pressure64(ui, k), um, pressure64(um, k), F);
             } else {
                 Node5 ni, nm;
                 ni.rho = su[(0 * EPC + el) * NP + idx[i]];
                 ni.vn = sp[(c0 * EPC + el) * NP + idx[i]];
                 ni.vt1 = sp[(c1 * EPC + el) * NP + idx[i]];
                 ni.vt2 = sp[(c2 * EPC + el) * NP + idx[i]];
-                ni.beta = sp[(4 * EPC + el) * NP + idx[i]];
+                ni.beta = sp[((3 + d) * EPC + el) * NP + idx[i]];
                 nm.rho = su[(0 * EPC + el) * NP + idx[m]];
                 nm.vn = sp[(c0 * EPC + el) * NP + idx[m]];
                 nm.vt1 = sp[(c1 * EPC + el) * NP + idx[m]];
                 nm.vt2 = sp[(c2 * EPC + el) * NP + idx[m]];
-                nm.beta = sp[(4 * EPC + el) * NP + idx[m]];
+                nm.beta = sp[((3 + d) * EPC + el) * NP + idx[m]];
                 chandrashekar64(ni, nm, F, k);
             }
             const double sim = k.S[i * NN + m], smi = k.S[m * NN + i];
@@ -394,7 +335,7 @@ __global__ void __launch_bounds__(NT, 1) k_stage_euler64(StageArgs a) {
     if (RHS_ONLY) return;
     __syncthreads();
     if (a.positivity && tid < nel && s_bad[tid]) {
-        if (!repair_elem(su, tid, k)) atomicAdd(&ctrl->nbad, 1ull);
+        if (!repair_elem<EPC>(su, tid, k)) atomicAdd(&ctrl->nbad, 1ull);
     }
     __syncthreads();
     // ---- store the new state
@@ -620,7 +561,7 @@ __global__ void k_totals_sum64(const double* __restrict__ part, int64_t E, int n
 // ---------------------------------------------------------------------------------------------
 // launchers
 
-int stage_smem_bytes64() { return (V * EPC * NP + 5 * EPC * NP + 2 * V * EPC * NP) * (int)sizeof(double); }
+int stage_smem_bytes64() { return (V * EPC * NP + 6 * EPC * NP + 2 * V * EPC * NP) * (int)sizeof(double); }
 
 cudaError_t launch_stage_euler64(const StageArgs& a, bool blend, bool ind, bool rhs_only, cudaStream_t s) {
     const int grid = (int)((a.E + EPC - 1) / EPC);

@@ -65,3 +65,21 @@ def kelvin_helmholtz(m, seed=7, kappa=1.4, nodes=LGL4, amp=0.01):
     vz = np.zeros_like(x)
     p = 2.5 * np.ones_like(x)
     return np.ascontiguousarray(prim2cons(rho, vx, vy, vz, p, kappa))
+
+
+def smooth_random(m, seed=0, kappa=1.4, nodes=LGL4, amp=0.2):
+    """Smooth periodic state on [0,1]^3 with distinct, seeded sinusoidal density, velocity components
+    and pressure (a parity workload in which no two momentum components coincide)."""
+    x, y, z = m.node_coords(nodes)
+    rng = np.random.default_rng(seed)
+    ph = rng.uniform(0, 2 * np.pi, size=(5, 3))
+    kk = rng.integers(1, 3, size=(5, 3))
+
+    def wave(i):
+        return (np.sin(2 * np.pi * kk[i, 0] * x + ph[i, 0]) * np.cos(2 * np.pi * kk[i, 1] * y + ph[i, 1])
+                + np.sin(2 * np.pi * kk[i, 2] * z + ph[i, 2]))
+
+    rho = 1.0 + amp * wave(0)
+    vx, vy, vz = 0.5 * wave(1), -0.4 * wave(2), 0.3 * wave(3)
+    p = 1.0 + amp * wave(4)
+    return np.ascontiguousarray(prim2cons(rho, vx, vy, vz, p, kappa))
