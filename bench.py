@@ -55,10 +55,36 @@ def make_state(wl):
     return m, u
 
 
-def make_cfg(wl):
+def make_cfg(wl, precision=0):
     from nemo_b200 import abi
     w = WORKLOADS[wl]
-    return abi.default_cfg(indicator=w["indicator"], positivity=w["positivity"], cfl=0.5)
+    return abi.default_cfg(indicator=w["indicator"], positivity=w["positivity"], cfl=0.5, precision=precision)
+
+
+def timed_run(s, steps, stream, dist, torch, ctypes, abi):
+    """K steps with per-kernel CUDA events on the library stream; returns (ms, stage_ms, stage_n,
+    total_ms, total_n, t_sim, steps_done)."""
+    abi.call("nemo_gpu_set_timing", 1)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    t_sim, nst = s.run(nsteps=steps)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    ms = ev0.elapsed_time(ev1)
+    st_ms, st_n, tot_ms, tot_n = (ctypes.c_double(), ctypes.c_int64(), ctypes.c_double(), ctypes.c_int64())
+    abi.call("nemo_gpu_kernel_timing", ctypes.byref(st_ms), ctypes.byref(st_n), ctypes.byref(tot_ms),
+             ctypes.byref(tot_n))
+    abi.call("nemo_gpu_set_timing", 0)
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    return ms, st_ms.value, st_n.value, tot_ms.value, tot_n.value, t_sim, nst
 
 
 class ClockSampler:
@@ -127,6 +153,26 @@ def cpu_baseline(wl, u, m, nthreads=None, sample_stages=5):
                       f"{o.nthreads} OpenMP threads, {el:.2f} s"}
 
 
+def accuracy_check(wl, m, u, abi, Solver, t_end=0.05):
+    """Both forms to t_end; relative L1 density error of the chosen form against the plain FP64 form
+    (which reproduces the FP64 oracle bit for bit, see tests/test_gpu_parity.py)."""
+    res = {}
+    for prec in (abi.PREC_FP64, abi.PREC_FP32):
+        s = Solver(make_cfg(wl, prec), m)
+        s.upload(u)
+        t0 = time.perf_counter()
+        t, n = s.run(t_end=t_end)
+        el = time.perf_counter() - t0
+        res[prec] = (s.download()[0], t, n, el, s.status()[1])
+        s.finalize()
+    r64, r32 = res[abi.PREC_FP64][0], res[abi.PREC_FP32][0]
+    return {"t_end": t_end, "steps_fp64": res[abi.PREC_FP64][2], "steps_fp32": res[abi.PREC_FP32][2],
+            "rel_l1_density_fp32_vs_fp64": float(np.sum(np.abs(r32 - r64)) / np.sum(np.abs(r64))),
+            "rel_linf_density_fp32_vs_fp64": float(np.max(np.abs(r32 - r64)) / np.max(np.abs(r64))),
+            "repair_failures": [res[abi.PREC_FP64][4], res[abi.PREC_FP32][4]],
+            "wall_s_to_t_end": [res[abi.PREC_FP64][3], res[abi.PREC_FP32][3]]}
+
+
 def run_reference(args, rank, world):
     """--impl reference: the reference's CPU implementation of the path.  The Fortran reference
     cannot be built here (no Fortran compiler / MPI / p4est / HDF5), so this times the C++ FP64
@@ -169,6 +215,7 @@ def main():
     ap.add_argument("--workload", default="sedov32", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
+    ap.add_argument("--no-accuracy", action="store_true", help="skip the run to t_end that checks the L1 error")
     args = ap.parse_args()
     assert args.warmup >= 3 or args.impl == "reference" or os.environ.get("NEMO_BENCH_ALLOW_SHORT")
 
@@ -193,45 +240,35 @@ def main():
     import ctypes
 
     m, u = make_state(args.workload)
-    c = make_cfg(args.workload)
-    s = Solver(c, m)
+    dof_per_step = m.E * 64 * 5
+
+    # ---- the plain FP64 form (the comparison point of the metric)
+    s = Solver(make_cfg(args.workload, abi.PREC_FP64), m)
     s.upload(u)
     stream_ptr = ctypes.c_uint64()
     abi.call("nemo_gpu_stream", ctypes.byref(stream_ptr))
     stream = torch.cuda.ExternalStream(stream_ptr.value)
-
-    # warm-up (graphs are built here)
     s.run(nsteps=args.warmup)
+    ms64, st64, n64, tot64, ntot64, _, _ = timed_run(s, args.steps, stream, dist, torch, ctypes, abi)
+    value64 = world * dof_per_step * args.steps / (ms64 * 1e-3)
+    s.finalize()
 
-    # ---- timed region: K steps, per-kernel CUDA events on the library stream
-    abi.call("nemo_gpu_set_timing", 1)
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    # ---- the chosen form: FP32 bulk, FP64 state/register/update/repair/reductions
+    c = make_cfg(args.workload, abi.PREC_FP32)
+    s = Solver(c, m)
+    s.upload(u)
+    abi.call("nemo_gpu_stream", ctypes.byref(stream_ptr))
+    stream = torch.cuda.ExternalStream(stream_ptr.value)
+    s.run(nsteps=args.warmup)
     with ClockSampler(local) as clk:
-        ev0.record(stream)
-        t_sim, nst = s.run(nsteps=args.steps)
-        ev1.record(stream)
-        torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
-    ms = ev0.elapsed_time(ev1)
-    st_ms, st_n, tot_ms, tot_n = (ctypes.c_double(), ctypes.c_int64(), ctypes.c_double(), ctypes.c_int64())
-    abi.call("nemo_gpu_kernel_timing", ctypes.byref(st_ms), ctypes.byref(st_n), ctypes.byref(tot_ms),
-             ctypes.byref(tot_n))
-    abi.call("nemo_gpu_set_timing", 0)
-    if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    dof_per_step = m.E * 64 * 5
+        ms, st_ms_v, st_n_v, tot_ms_v, tot_n_v, t_sim, nst = timed_run(s, args.steps, stream, dist, torch, ctypes,
+                                                                        abi)
     value = world * dof_per_step * args.steps / (ms * 1e-3)
 
     # ---- roofline of the stage kernel (HBM): algorithmic bytes per launch / avg launch time
     V = 5
     bytes_per_launch = sum(m.E * 64 * V * 8 * (3 if st == 0 else 4) for st in range(5)) / 5.0
-    avg_stage_s = st_ms.value * 1e-3 / max(st_n.value, 1)
+    avg_stage_s = st_ms_v * 1e-3 / max(st_n_v, 1)
     peak, peak_kind = load_peaks()
     achieved = bytes_per_launch / avg_stage_s / 1e9
     traffic = None
@@ -270,6 +307,11 @@ def main():
             e2e_ms = float(t.item())
         e2e_val = world * dof_per_step * e2e_steps / (e2e_ms * 1e-3)
 
+    s.finalize()
+    accuracy = None
+    if not args.no_accuracy and WORKLOADS[args.workload]["setup"] == "sedov":
+        accuracy = accuracy_check(args.workload, m, u, abi, Solver)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(args.workload, u, m)
@@ -286,29 +328,32 @@ def main():
             "higher_is_better": True,
             "scaling": "weak",
             "vs_baseline": None,
-            "dtype": "f64",
+            "dtype": "f32 flux bulk, f64 state/register/update",
             "data": "synthetic",
             "config": {"workload": WORKLOADS[args.workload]["desc"], "elements": m.E, "nodes": m.E * 64,
-                       "stages_per_step": 5, "precision": "plain FP64",
+                       "stages_per_step": 5, "precision": "FP32 bulk + FP64 accumulation (chosen form)",
                        "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
                        "l2": "working set (u in/out + register, 3 x 84 MB) larger than L2"},
             "clocks": clk.summary(),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
-                         "kernel": "k_stage_euler64", "algorithmic_bytes_per_launch": bytes_per_launch,
+                         "kernel": "k_stage_euler32", "algorithmic_bytes_per_launch": bytes_per_launch,
                          "avg_launch_ms": avg_stage_s * 1e3},
             "e2e": None if e2e_val is None else {
                     "value": e2e_val, "unit": "DOF-updates/s", "h2d_bytes_per_step": nbytes,
                     "d2h_bytes_per_step": nbytes,
                     "note": "per step: upload of the full state from pinned host memory, one time step, "
                             "download of the full state"},
-            "gpu_launches": int(tot_n.value),
+            "gpu_launches": int(tot_n_v),
             "sim": {"t": t_sim, "steps": nst},
+            "plain_fp64": {"value": value64, "unit": "DOF-updates/s", "ms_per_step": ms64 / args.steps,
+                           "avg_stage_ms": st64 / max(n64, 1), "kernel": "k_stage_euler64",
+                           "speedup_of_chosen_form": value / value64},
+            "accuracy": accuracy,
         }
         if cpu:
             line["cpu_baseline"] = cpu
         print(json.dumps(line), flush=True)
-    s.finalize()
     if dist:
         dist.barrier()
         dist.destroy_process_group()
