@@ -1,0 +1,82 @@
+!! GPU kernel module, hook part: replaces kernel_hooks_mod of a CPU kernel directory
+!! (source/kernel/mcfv/3d/kernel_hooks_mod.f90).  A setup's preproc.py selects it with
+!!     kernel = home + '/source/kernel/dgsem-gpu/3d'
+!! and links libnemo_gpu.so; nemo.py then wires these hooks into the generated dispatchers
+!! (scripts/nemo.py:245-305) exactly as it wires the CPU kernel's.
+
+module kernel_hooks_mod
+
+use constants_mod
+
+contains
+
+!! hook_init_400: operators and device selection (kernel_share_mod::init on the CPU side).
+subroutine hook_init_400
+
+    use iso_c_binding
+    use nemo_gpu_interfaces_mod
+    use kernel_share_mod, only: nodes, weights, gpu_cfg
+    use setup_config_mod, only: kappa, CFL
+
+    real(c_double) :: x(N_NODES), w(N_NODES), dmat(N_NODES**2), smat(N_NODES**2), vinv(N_NODES**2)
+
+    call nemo_gpu_check(nemo_gpu_default_cfg(gpu_cfg), 'default_cfg')
+    gpu_cfg%kappa = kappa
+    gpu_cfg%cfl = CFL
+# ifdef PP_KERNEL_GPU_PRECISION
+    gpu_cfg%precision = PP_KERNEL_GPU_PRECISION
+# endif
+# ifdef PP_KERNEL_GPU_INDICATOR
+    gpu_cfg%indicator = PP_KERNEL_GPU_INDICATOR
+    gpu_cfg%positivity = 1
+# endif
+    call nemo_gpu_check(nemo_gpu_init(gpu_cfg), 'init')
+
+    !! nodes/weights on [-1/2,1/2] as the mesh layer expects (source/mesh/p4est/quad_utils_mod.f90:11)
+    call nemo_gpu_check(nemo_gpu_operators(int(N_NODES,c_int), x, w, dmat, smat, vinv), 'operators')
+    nodes = 0.5_dp * x
+    weights = 0.5_dp * w
+
+end subroutine
+
+!! hook_init_520 (after the mesh, hook_init_500/510): connectivity to the device.
+subroutine hook_init_520
+
+    use kernel_share_mod, only: kernel_share_set_mesh
+
+    call kernel_share_set_mesh()
+
+end subroutine
+
+!! hook_init_815 (after the setup filled the initial state, hook_init_810): state to the device.
+subroutine hook_init_815
+
+    use kernel_share_mod, only: kernel_share_upload
+
+    call kernel_share_upload()
+
+end subroutine
+
+!! Face fill and face flux are fused into the stage kernel: nothing to do before the stage.
+subroutine hook_pre_rk_timestep_300
+
+end subroutine
+
+!! The setups' analyze and checkpoint hooks read quad%pld%hydro%state: bring it back first.
+subroutine hook_analyze_100
+
+    use kernel_share_mod, only: kernel_share_download
+
+    call kernel_share_download()
+
+end subroutine
+
+subroutine hook_checkpoint_100
+
+    use kernel_share_mod, only: kernel_share_download
+
+    call kernel_share_download()
+
+end subroutine
+
+end module

@@ -1,0 +1,154 @@
+!! nemo_gpu_interfaces_mod -- iso_c_binding interfaces to libnemo_gpu.so (include/nemo_gpu.h).
+!!
+!! Written in the style of the reference's p4wrap bindings
+!! (source/mesh/p4est/wrapper/p4wrap_interfaces_mod.f90): one bind(c) interface per C entry
+!! point, value arguments for scalars, c_ptr for arrays that live in the quad/side structures.
+!! Every function returns a C int status (0 = OK); nemo_gpu_check turns a non-zero status into
+!! raise_error with the library's message (source/utils/status_mod.f90:7-21).
+
+module nemo_gpu_interfaces_mod
+
+use iso_c_binding
+
+implicit none
+
+integer(c_int), parameter :: NEMO_EQN_EULER = 0, NEMO_EQN_MHD = 1
+integer(c_int), parameter :: NEMO_VOLFLUX_CHANDRASHEKAR = 0, NEMO_VOLFLUX_CENTRAL = 1
+integer(c_int), parameter :: NEMO_SURFFLUX_HLLC = 0, NEMO_SURFFLUX_RUSANOV = 1
+integer(c_int), parameter :: NEMO_PREC_FP64 = 0, NEMO_PREC_FP32 = 1
+integer(c_int), parameter :: NEMO_IND_NONE = 0, NEMO_IND_MODAL = 1, NEMO_IND_LEARNED = 2
+
+!! mirrors struct nemo_cfg (include/nemo_gpu.h)
+type, bind(c) :: nemo_cfg_t
+    integer(c_int)  :: n_nodes, n_vars, eqn, volume_flux, surface_flux, precision, indicator
+    integer(c_int)  :: alpha_smoothing, positivity, non_conservative
+    real(c_double)  :: kappa, mu0, cfl, alpha_max, alpha_min, repair_decr, glm_ch, glm_alpha
+    real(c_double)  :: reserved(4)
+end type
+
+interface
+    function nemo_gpu_default_cfg(cfg) result(st) bind(c, name="nemo_gpu_default_cfg")
+        import :: c_int, nemo_cfg_t
+        type(nemo_cfg_t), intent(out) :: cfg
+        integer(c_int) :: st
+    end function
+
+    function nemo_gpu_init(cfg) result(st) bind(c, name="nemo_gpu_init")
+        import :: c_int, nemo_cfg_t
+        type(nemo_cfg_t), intent(in) :: cfg
+        integer(c_int) :: st
+    end function
+
+    function nemo_gpu_operators(n, nodes, weights, dmat, smat, vinv) result(st) bind(c, name="nemo_gpu_operators")
+        import :: c_int, c_double
+        integer(c_int), value :: n
+        real(c_double), intent(out) :: nodes(*), weights(*), dmat(*), smat(*), vinv(*)
+        integer(c_int) :: st
+    end function
+
+    function nemo_gpu_set_mesh(nelems, delta, center, nsides, side_quads, side_faceid, side_nquads, boundary) &
+            result(st) bind(c, name="nemo_gpu_set_mesh")
+        import :: c_int, c_int8_t, c_int32_t, c_int64_t, c_double
+        integer(c_int64_t), value :: nelems, nsides
+        real(c_double), intent(in) :: delta(*), center(*)
+        integer(c_int32_t), intent(in) :: side_quads(*), boundary(*)
+        integer(c_int8_t), intent(in) :: side_faceid(*), side_nquads(*)
+        integer(c_int) :: st
+    end function
+
+    function nemo_gpu_set_groups(ngroups, group_of_elem) result(st) bind(c, name="nemo_gpu_set_groups")
+        import :: c_int, c_int32_t
+        integer(c_int32_t), value :: ngroups
+        integer(c_int32_t), intent(in) :: group_of_elem(*)
+        integer(c_int) :: st
+    end function
+
+    function nemo_gpu_upload_state(host, elem_stride_bytes) result(st) bind(c, name="nemo_gpu_upload_state")
+        import :: c_int, c_int64_t, c_ptr
+        type(c_ptr), value :: host
+        integer(c_int64_t), value :: elem_stride_bytes
+        integer(c_int) :: st
+    end function
+
+    function nemo_gpu_download_state(host, elem_stride_bytes) result(st) bind(c, name="nemo_gpu_download_state")
+        import :: c_int, c_int64_t, c_ptr
+        type(c_ptr), value :: host
+        integer(c_int64_t), value :: elem_stride_bytes
+        integer(c_int) :: st
+    end function
+
+    function nemo_gpu_calc_timestep(cfl, dt, lmax) result(st) bind(c, name="nemo_gpu_calc_timestep")
+        import :: c_int, c_double
+        real(c_double), value :: cfl
+        real(c_double), intent(out) :: dt, lmax
+        integer(c_int) :: st
+    end function
+
+    function nemo_gpu_stage(stage, dt, t_stage, nbad) result(st) bind(c, name="nemo_gpu_stage")
+        import :: c_int, c_int32_t, c_double
+        integer(c_int32_t), value :: stage
+        real(c_double), value :: dt, t_stage
+        integer(c_int32_t), intent(out) :: nbad
+        integer(c_int) :: st
+    end function
+
+    function nemo_gpu_step(dt) result(st) bind(c, name="nemo_gpu_step")
+        import :: c_int, c_double
+        real(c_double), value :: dt
+        integer(c_int) :: st
+    end function
+
+    function nemo_gpu_run(nsteps, t_end, t_out, steps_out) result(st) bind(c, name="nemo_gpu_run")
+        import :: c_int, c_int64_t, c_double
+        integer(c_int64_t), value :: nsteps
+        real(c_double), value :: t_end
+        real(c_double), intent(out) :: t_out
+        integer(c_int64_t), intent(out) :: steps_out
+        integer(c_int) :: st
+    end function
+
+    function nemo_gpu_totals(out) result(st) bind(c, name="nemo_gpu_totals")
+        import :: c_int, c_double
+        real(c_double), intent(out) :: out(10)
+        integer(c_int) :: st
+    end function
+
+    function nemo_gpu_finalize() result(st) bind(c, name="nemo_gpu_finalize")
+        import :: c_int
+        integer(c_int) :: st
+    end function
+
+    function nemo_gpu_last_error(buf, len) result(st) bind(c, name="nemo_gpu_last_error")
+        import :: c_int, c_int32_t, c_char
+        character(kind=c_char), intent(out) :: buf(*)
+        integer(c_int32_t), value :: len
+        integer(c_int) :: st
+    end function
+end interface
+
+contains
+
+!! Forward a non-zero status to the reference's error path.
+subroutine nemo_gpu_check(st, where)
+
+    use status_mod, only: raise_error
+
+    integer(c_int), intent(in) :: st
+    character(len=*), intent(in) :: where
+
+    character(kind=c_char) :: buf(512)
+    character(len=512) :: msg
+    integer :: i, rc
+
+    if (st == 0) return
+    rc = nemo_gpu_last_error(buf, 512_c_int32_t)
+    msg = ''
+    do i = 1, 512
+        if (buf(i) == c_null_char) exit
+        msg(i:i) = buf(i)
+    end do
+    call raise_error('nemo_gpu (' // where // '): ' // trim(msg))
+
+end subroutine
+
+end module
