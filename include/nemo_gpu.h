@@ -150,6 +150,20 @@ int nemo_gpu_totals(double* out);
 /* Simulation time of group 0 and the accumulated repair-failure count. */
 int nemo_gpu_status(double* t_out, int64_t* nbad_total_out);
 
+/* Conserved totals (as nemo_gpu_totals) of a state held in device memory that the caller owns,
+   without allocating anything.  No counterpart in the reference: it serves hosts that cannot
+   allocate device memory at this point (device arrays owned by a Fortran/OpenACC pool sized at
+   start-up, or a fixed device-memory budget where a cudaMalloc/cudaFree would fail or synchronise
+   the device).  u_dev: [nvars][nelems][64] FP64 (the library's layout); delta_dev: [nelems][3];
+   out_dev: nvars doubles; all device pointers.  stream: a cudaStream_t as an integer (0 = the
+   legacy default stream); the call only enqueues work on it.  Limits: 1 <= nelems <= 65536 and
+   1 <= nvars <= 9 (larger sizes are rejected with NEMO_ERR_ARG): the per-element partial sums live
+   in a fixed 4.5 MiB device array inside the library, held by every GPU that loads it until exit.
+   The first call on a device looks up that array's address (make it before any stream capture).
+   Every call overwrites the array, so calls that overlap on the GPU (other streams) race. */
+int nemo_gpu_totals_noalloc(const double* u_dev, const double* delta_dev, int64_t nelems, int32_t nvars,
+                            double* out_dev, uint64_t stream);
+
 int nemo_gpu_finalize(void);
 
 /* Copy the last error message (NUL terminated, truncated to len). */

@@ -25,6 +25,7 @@ EXPORTS = [
     "nemo_gpu_calc_timestep", "nemo_gpu_stage", "nemo_gpu_step", "nemo_gpu_run", "nemo_gpu_rhs",
     "nemo_gpu_alpha", "nemo_gpu_totals", "nemo_gpu_status", "nemo_gpu_finalize",
     "nemo_gpu_last_error", "nemo_gpu_set_timing", "nemo_gpu_kernel_timing", "nemo_gpu_stream",
+    "nemo_gpu_totals_noalloc",
 ]
 
 
@@ -83,6 +84,7 @@ def load(path=LIB_PATH):
         "nemo_gpu_kernel_timing": [ctypes.POINTER(dbl), ctypes.POINTER(i64), ctypes.POINTER(dbl),
                                    ctypes.POINTER(i64)],
         "nemo_gpu_stream": [ctypes.POINTER(ctypes.c_uint64)],
+        "nemo_gpu_totals_noalloc": [vp, vp, i64, i32, vp, ctypes.c_uint64],
     }
     for name, args in sig.items():
         f = getattr(L, name)

@@ -20,6 +20,7 @@ SOURCES = {
     "control.cu": [],
     "stage_fp64.cu": ["-fmad=false"],
     "stage_fp32.cu": ["--use_fast_math"],
+    "noalloc.cu": ["-fmad=false"],
 }
 
 

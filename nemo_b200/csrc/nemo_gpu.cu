@@ -154,7 +154,7 @@ struct Lib {
     HostOps hops{};
     OpConsts ops{};
     cudaStream_t stream = nullptr;
-    std::string err;
+    char err[512] = "";
 
     int64_t E = 0;
     int V = 5;
@@ -187,12 +187,10 @@ struct Lib {
 Lib g;
 
 int fail(int code, const char* fmt, ...) {
-    char buf[512];
     va_list ap;
     va_start(ap, fmt);
-    std::vsnprintf(buf, sizeof buf, fmt, ap);
+    std::vsnprintf(g.err, sizeof g.err, fmt, ap);
     va_end(ap);
-    g.err = buf;
     return code;
 }
 
@@ -321,6 +319,10 @@ int build_graph(int start) {
 }
 
 }  // namespace
+
+namespace nemo {
+void set_last_error(const char* msg) { std::snprintf(g.err, sizeof g.err, "%s", msg); }
+}  // namespace nemo
 
 // ================================================================================================
 extern "C" {
@@ -743,7 +745,7 @@ int nemo_gpu_finalize(void) {
 
 int nemo_gpu_last_error(char* buf, int32_t len) {
     if (!buf || len <= 0) return NEMO_ERR_ARG;
-    std::snprintf(buf, (size_t)len, "%s", g.err.c_str());
+    std::snprintf(buf, (size_t)len, "%s", g.err);
     return NEMO_OK;
 }
 
