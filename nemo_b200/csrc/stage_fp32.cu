@@ -1,7 +1,7 @@
 // stage_fp32.cu -- the FP32-bulk form of the fused LSRK stage (compiled with --use_fast_math).
 //
-// Same decomposition and thread mapping as stage_fp64.cu (one CTA = 8 elements, 48 threads per
-// element, one per (direction, line)), with the precision split of the mixed-precision design:
+// One CTA = 8 elements (a 2x2x2 block on a Morton-ordered brick), 16 threads per element, thread
+// (a,b) owning the three lines through (a,b); precision split of the mixed-precision design:
 //   FP64: the state and the RK register in HBM, the per-node primitive recovery (pressure from
 //         conserved variables, where cancellation between total and kinetic energy lives), the
 //         register/state update, the positivity repair and the CFL minimum;
@@ -21,10 +21,11 @@ __constant__ OpConsts c_ops32;
 
 namespace {
 
-constexpr int EPC = 8;
-constexpr int TPE = 48;
-constexpr int NT = EPC * TPE;
+constexpr int EPC = 8;          // elements per CTA
+constexpr int TPE = 16;         // threads per element, one per line position (a,b)
+constexpr int NT = EPC * TPE;   // 128 threads: a warp holds exactly two elements
 constexpr int V = 5;
+constexpr int NQ = 6;           // FP32 node data: rho, vx, vy, vz, p, beta
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) {
     return static_cast<unsigned>(__cvta_generic_to_shared(p));
@@ -44,8 +45,11 @@ __device__ __forceinline__ bool mbar_wait32(uint64_t* bar, unsigned phase) {
     return false;
 }
 
-__device__ __forceinline__ bool tile_load32(double* su, const double* __restrict__ u, int64_t E, int64_t e0, int nel,
-                                            uint64_t* bar, Control* ctrl) {
+// Stage the tile's state (and, from the second RK stage on, its register) into shared memory with
+// 1D bulk copies (V arrays of nel*64 doubles, contiguous per variable), completing on one mbarrier.
+__device__ __forceinline__ void tile_issue32(double* su, const double* __restrict__ u, double* sg,
+                                             const double* __restrict__ reg, int64_t E, int64_t e0, int nel,
+                                             uint64_t* bar) {
     if (threadIdx.x == 0) {
         unsigned b = smem_u32(bar);
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(b) : "memory");
@@ -56,22 +60,53 @@ __device__ __forceinline__ bool tile_load32(double* su, const double* __restrict
     if (threadIdx.x == 0) {
         unsigned b = smem_u32(bar);
         unsigned bytes = (unsigned)(nel * NP * 8);
-        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(b), "r"(bytes * V) : "memory");
+        unsigned total = bytes * V * (reg ? 2u : 1u);
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(b), "r"(total) : "memory");
         for (int v = 0; v < V; ++v) {
-            const double* src = u + ((int64_t)v * E + e0) * NP;
             asm volatile(
                 "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
                     smem_u32(su + v * EPC * NP)),
-                "l"(src), "r"(bytes), "r"(b)
+                "l"(u + ((int64_t)v * E + e0) * NP), "r"(bytes), "r"(b)
                 : "memory");
         }
+        if (reg)
+            for (int v = 0; v < V; ++v) {
+                asm volatile(
+                    "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                        smem_u32(sg + v * EPC * NP)),
+                    "l"(reg + ((int64_t)v * E + e0) * NP), "r"(bytes), "r"(b)
+                    : "memory");
+            }
     }
+}
+
+__device__ __forceinline__ bool tile_wait32(uint64_t* bar, Control* ctrl) {
     bool ok = mbar_wait32(bar, 0);
     if (!ok) {
         atomicOr(&ctrl->error, 1);
-        mbar_wait32(bar, 0);
+        mbar_wait32(bar, 0);  // second bounded wait for the copies still in flight
     }
     return ok;
+}
+
+// Write the tile's new state and register back with 1D bulk copies from shared memory.  The
+// calling thread waits until the copies have read shared memory before the CTA may exit.
+__device__ __forceinline__ void tile_store32(const double* su, double* __restrict__ u_out, const double* sg,
+                                             double* __restrict__ reg, int64_t E, int64_t e0, int nel) {
+    const unsigned bytes = (unsigned)(nel * NP * 8);
+    for (int v = 0; v < V; ++v) {
+        asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(u_out + ((int64_t)v * E + e0) * NP),
+                     "r"(smem_u32(su + v * EPC * NP)), "r"(bytes)
+                     : "memory");
+        asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(reg + ((int64_t)v * E + e0) * NP),
+                     "r"(smem_u32(sg + v * EPC * NP)), "r"(bytes)
+                     : "memory");
+    }
+    asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+}
+
+__device__ __forceinline__ void tile_store_wait32() {
+    asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
 }
 
 // Per-node FP32 primitives in the frame of direction d.
@@ -171,17 +206,19 @@ __device__ __forceinline__ float lnmean32(float a, float b) {
 
 }  // namespace
 
-// Node data in smem (FP32): rho, vx, vy, vz, p, E, beta, |v|^2 -> 8 arrays [8][EPC][64]
+// One CTA = EPC elements x 16 threads; thread (a,b) of an element owns the x-, y- and z-lines
+// through (a,b) and processes them one direction after the other, accumulating into one shared
+// rhs array (x, then y, then z).  A warp holds exactly two elements.
 template <bool BLEND, bool RHS_ONLY>
-__global__ void __launch_bounds__(NT, 2) k_stage_euler32(StageArgs a) {
+__global__ void __launch_bounds__(NT, 3) k_stage_euler32(StageArgs a) {
     extern __shared__ __align__(128) double smem[];
-    double* su = smem;                                  // [V][EPC][64] FP64 state
-    float* sq = reinterpret_cast<float*>(su + V * EPC * NP);   // [8][EPC][64] FP32 node data
-    float* sR = sq + 8 * EPC * NP;                       // [3][V][EPC][64] FP32 direction terms
+    double* su = smem;                                          // [V][EPC][64] FP64 state
+    double* sg = su + V * EPC * NP;                             // [V][EPC][64] FP64 RK register
+    float* sq = reinterpret_cast<float*>(sg + V * EPC * NP);    // [NQ][EPC][64] FP32 node data
+    float* sR = sq + NQ * EPC * NP;                             // [V][EPC][64] FP32 rhs terms
     __shared__ uint64_t bar;
     __shared__ float s_alpha[EPC];
     __shared__ int s_bad[EPC];
-    __shared__ unsigned s_lam[EPC][3];
 
     const OpConsts& k = c_ops32;
     Control* ctrl = a.ctrl;
@@ -193,7 +230,6 @@ __global__ void __launch_bounds__(NT, 2) k_stage_euler32(StageArgs a) {
 
     if (tid < EPC) {
         s_bad[tid] = 0;
-        s_lam[tid][0] = s_lam[tid][1] = s_lam[tid][2] = 0u;
         float al = 0.0f;
         if (BLEND && tid < nel) {
             const int64_t e = e0 + tid;
@@ -210,213 +246,231 @@ __global__ void __launch_bounds__(NT, 2) k_stage_euler32(StageArgs a) {
         }
         s_alpha[tid] = al;
     }
-    if (!tile_load32(su, a.u_in, E, e0, nel, &bar, ctrl)) return;
+    const bool load_reg = !RHS_ONLY && a.stage > 0;
+    tile_issue32(su, a.u_in, sg, load_reg ? a.reg : nullptr, E, e0, nel, &bar);
+    if (!tile_wait32(&bar, ctrl)) return;
 
-    auto SQ = [&](int q, int el, int n) -> float& { return sq[(q * EPC + el) * NP + n]; };
-    // per-node primitives: recovered in FP64, stored in FP32
-    for (int p = tid; p < nel * NP; p += NT) {
-        const int el = p / NP, n = p % NP;
-        const double r = su[(0 * EPC + el) * NP + n];
-        const double mx = su[(1 * EPC + el) * NP + n], my = su[(2 * EPC + el) * NP + n];
-        const double mz = su[(3 * EPC + el) * NP + n], en = su[(4 * EPC + el) * NP + n];
-        const double ir = 1.0 / r;
-        const double vx = mx * ir, vy = my * ir, vz = mz * ir;
-        const double pr = k.km1 * (en - 0.5 * (mx * vx + my * vy + mz * vz));
-        SQ(0, el, n) = (float)r;
-        SQ(1, el, n) = (float)vx;
-        SQ(2, el, n) = (float)vy;
-        SQ(3, el, n) = (float)vz;
-        SQ(4, el, n) = (float)pr;
-        SQ(5, el, n) = (float)en;
-        SQ(6, el, n) = (float)(0.5 * r / pr);
-        SQ(7, el, n) = (float)(vx * vx + vy * vy + vz * vz);
-    }
-    __syncthreads();
-
-    const int el = tid / TPE;
-    const int rr = tid % TPE;
-    const int d = rr / NF;
-    const int ab = rr % NF;
-    const int la = ab & 3, lb = ab >> 2;
+    const int el = tid >> 4, ab = tid & 15, la = ab & 3, lb = ab >> 2;
     const bool active = el < nel;
     const int64_t e = e0 + el;
-    const int c0 = d, c1 = (d + 1) % 3, c2 = (d + 2) % 3;
+    auto SQ = [&](int q, int elx, int n) -> float& { return sq[(q * EPC + elx) * NP + n]; };
 
-    auto node = [&](int elx, int n) {
-        P32 q;
-        q.rho = SQ(0, elx, n);
-        q.vn = SQ(1 + c0, elx, n);
-        q.vt1 = SQ(1 + c1, elx, n);
-        q.vt2 = SQ(1 + c2, elx, n);
-        q.p = SQ(4, elx, n);
-        q.E = SQ(5, elx, n);
-        return q;
-    };
-
-    float t[NN][V];
+    // per-node primitives of the thread's x-line nodes: recovered in FP64, stored in FP32
     if (active) {
-        float Fs[2][V];
-#pragma unroll
-        for (int side = 0; side < 2; ++side) {
-            const int f = 2 * d + side;
-            const int own = line_node(d, la, lb, side ? NN - 1 : 0);
-            const P32 qo = node(el, own);
-            P32 qn = qo;
-            const int32_t ne = a.nbr[e * 6 + f];
-            if (ne >= 0) {
-                const int nn = line_node(d, la, lb, side ? 0 : NN - 1);
-                const int64_t nl = (int64_t)ne - e0;
-                if (nl >= 0 && nl < nel) {
-                    qn = node((int)nl, nn);
-                } else {
-                    const double* g = a.u_in;
-                    const double r = __ldg(g + ((int64_t)0 * E + ne) * NP + nn);
-                    const double m0 = __ldg(g + ((int64_t)(1 + c0) * E + ne) * NP + nn);
-                    const double m1 = __ldg(g + ((int64_t)(1 + c1) * E + ne) * NP + nn);
-                    const double m2 = __ldg(g + ((int64_t)(1 + c2) * E + ne) * NP + nn);
-                    const double en = __ldg(g + ((int64_t)4 * E + ne) * NP + nn);
-                    const double ir = 1.0 / r;
-                    const double v0 = m0 * ir, v1 = m1 * ir, v2 = m2 * ir;
-                    qn.rho = (float)r;
-                    qn.vn = (float)v0;
-                    qn.vt1 = (float)v1;
-                    qn.vt2 = (float)v2;
-                    qn.p = (float)(k.km1 * (en - 0.5 * (m0 * v0 + m1 * v1 + m2 * v2)));
-                    qn.E = (float)en;
-                }
-            }
-            if (side) riemann32(a.surface_flux, qo, qn, Fs[1], k);
-            else riemann32(a.surface_flux, qn, qo, Fs[0], k);
-        }
-        int idx[NN];
-#pragma unroll
-        for (int i = 0; i < NN; ++i) idx[i] = line_node(d, la, lb, i);
-#pragma unroll
-        for (int i = 0; i < NN; ++i)
-#pragma unroll
-            for (int v = 0; v < V; ++v) t[i][v] = 0.0f;
-        const float c_enth = (float)k.c_enth;
-        const int PI_[6] = {0, 0, 0, 1, 1, 2};
-        const int PM_[6] = {1, 2, 3, 2, 3, 3};
-#pragma unroll
-        for (int pq = 0; pq < 6; ++pq) {
-            const int i = PI_[pq], m = PM_[pq];
-            const int ni = idx[i], nm = idx[m];
-            float F[V];
-            if (a.volume_flux == NEMO_VOLFLUX_CENTRAL) {
-                float fa[V], fb[V];
-                xflux32(node(el, ni), fa);
-                xflux32(node(el, nm), fb);
-#pragma unroll
-                for (int v = 0; v < V; ++v) F[v] = 0.5f * (fa[v] + fb[v]);
-            } else {
-                const float ru = SQ(0, el, ni), rv = SQ(0, el, nm);
-                const float bu = SQ(6, el, ni), bv = SQ(6, el, nm);
-                const float un = SQ(1 + c0, el, ni), vn = SQ(1 + c0, el, nm);
-                const float u1 = SQ(1 + c1, el, ni), v1 = SQ(1 + c1, el, nm);
-                const float u2 = SQ(1 + c2, el, ni), v2 = SQ(1 + c2, el, nm);
-                const float dens = lnmean32(ru, rv);
-                const float velx = 0.5f * (un + vn), vely = 0.5f * (u1 + v1), velz = 0.5f * (u2 + v2);
-                const float pres = 0.5f * (ru + rv) / (bu + bv);
-                const float enth = c_enth / lnmean32(bu, bv) + pres / dens + velx * velx + vely * vely + velz * velz -
-                                   0.25f * (SQ(7, el, ni) + SQ(7, el, nm));
-                F[0] = dens * velx;
-                F[1] = F[0] * velx + pres;
-                F[2] = F[0] * vely;
-                F[3] = F[0] * velz;
-                F[4] = F[0] * enth;
-            }
-            const float sim = (float)k.S[i * NN + m], smi = (float)k.S[m * NN + i];
-#pragma unroll
-            for (int v = 0; v < V; ++v) {
-                t[i][v] += sim * F[v];
-                t[m][v] += smi * F[v];
-            }
-        }
-        const float w0 = (float)k.winv[0], w3 = (float)k.winv[NN - 1];
-#pragma unroll
-        for (int v = 0; v < V; ++v) {
-            t[0][v] -= w0 * Fs[0][v];
-            t[NN - 1][v] += w3 * Fs[1][v];
-        }
-        if (BLEND) {
-            const float al = s_alpha[el];
-            if (al > 0.0f) {
-                float Fl[V], Fr[V];
-#pragma unroll
-                for (int v = 0; v < V; ++v) Fl[v] = Fs[0][v];
-#pragma unroll
-                for (int i = 0; i < NN; ++i) {
-                    if (i < NN - 1) {
-                        riemann32(a.surface_flux, node(el, idx[i]), node(el, idx[i + 1]), Fr, k);
-                    } else {
-#pragma unroll
-                        for (int v = 0; v < V; ++v) Fr[v] = Fs[1][v];
-                    }
-                    const float wi = (float)k.winv[i];
-#pragma unroll
-                    for (int v = 0; v < V; ++v) {
-                        t[i][v] = (1.0f - al) * t[i][v] + al * (wi * (Fr[v] - Fl[v]));
-                        Fl[v] = Fr[v];
-                    }
-                }
-            }
-        }
-        const float cd = (float)a.cdel[e * 3 + d];
-        float* R = sR + d * V * EPC * NP;
 #pragma unroll
         for (int i = 0; i < NN; ++i) {
-            const int n = idx[i];
-            R[(0 * EPC + el) * NP + n] = cd * t[i][0];
-            R[((1 + c0) * EPC + el) * NP + n] = cd * t[i][1];
-            R[((1 + c1) * EPC + el) * NP + n] = cd * t[i][2];
-            R[((1 + c2) * EPC + el) * NP + n] = cd * t[i][3];
-            R[(4 * EPC + el) * NP + n] = cd * t[i][4];
+            const int n = nidx(i, la, lb);
+            const double r = su[(0 * EPC + el) * NP + n];
+            const double mx = su[(1 * EPC + el) * NP + n], my = su[(2 * EPC + el) * NP + n];
+            const double mz = su[(3 * EPC + el) * NP + n], en = su[(4 * EPC + el) * NP + n];
+            const double ir = 1.0 / r;
+            const double vx = mx * ir, vy = my * ir, vz = mz * ir;
+            const double pr = k.km1 * (en - 0.5 * (mx * vx + my * vy + mz * vz));
+            SQ(0, el, n) = (float)r;
+            SQ(1, el, n) = (float)vx;
+            SQ(2, el, n) = (float)vy;
+            SQ(3, el, n) = (float)vz;
+            SQ(4, el, n) = (float)pr;
+            SQ(5, el, n) = (float)(0.5 * r / pr);
         }
     }
     __syncthreads();
 
-    // ---- FP64 register/state update
+    const float kappa = (float)k.kappa, ikm1 = (float)(1.0 / k.km1);
+    const float c_enth = (float)k.c_enth;
+    for (int d = 0; d < 3; ++d) {
+        if (active) {
+            const int c0 = d, c1 = (d + 1) % 3, c2 = (d + 2) % 3;
+            int idx[NN];
+            float rho[NN], vn[NN], w1[NN], w2[NN], pr[NN], bt[NN];
+#pragma unroll
+            for (int i = 0; i < NN; ++i) {
+                const int n = line_node(d, la, lb, i);
+                idx[i] = n;
+                rho[i] = SQ(0, el, n);
+                vn[i] = SQ(1 + c0, el, n);
+                w1[i] = SQ(1 + c1, el, n);
+                w2[i] = SQ(1 + c2, el, n);
+                pr[i] = SQ(4, el, n);
+                bt[i] = SQ(5, el, n);
+            }
+            auto prim = [&](int i) {
+                P32 q;
+                q.rho = rho[i];
+                q.vn = vn[i];
+                q.vt1 = w1[i];
+                q.vt2 = w2[i];
+                q.p = pr[i];
+                q.E = pr[i] * ikm1 + 0.5f * rho[i] * (vn[i] * vn[i] + w1[i] * w1[i] + w2[i] * w2[i]);
+                return q;
+            };
+            // ---- surface fluxes at both ends of the line
+            float Fs[2][V];
+#pragma unroll
+            for (int side = 0; side < 2; ++side) {
+                const int f = 2 * d + side;
+                const P32 qo = prim(side ? NN - 1 : 0);
+                P32 qn = qo;
+                const int32_t ne = a.nbr[e * 6 + f];
+                if (ne >= 0) {
+                    const int nn = line_node(d, la, lb, side ? 0 : NN - 1);
+                    const int64_t nl = (int64_t)ne - e0;
+                    if (nl >= 0 && nl < nel) {
+                        const int nli = (int)nl;
+                        qn.rho = SQ(0, nli, nn);
+                        qn.vn = SQ(1 + c0, nli, nn);
+                        qn.vt1 = SQ(1 + c1, nli, nn);
+                        qn.vt2 = SQ(1 + c2, nli, nn);
+                        qn.p = SQ(4, nli, nn);
+                        qn.E = qn.p * ikm1 + 0.5f * qn.rho * (qn.vn * qn.vn + qn.vt1 * qn.vt1 + qn.vt2 * qn.vt2);
+                    } else {
+                        const double* g = a.u_in;
+                        const double r = __ldg(g + ((int64_t)0 * E + ne) * NP + nn);
+                        const double m0 = __ldg(g + ((int64_t)(1 + c0) * E + ne) * NP + nn);
+                        const double m1 = __ldg(g + ((int64_t)(1 + c1) * E + ne) * NP + nn);
+                        const double m2 = __ldg(g + ((int64_t)(1 + c2) * E + ne) * NP + nn);
+                        const double en = __ldg(g + ((int64_t)4 * E + ne) * NP + nn);
+                        const double ir = 1.0 / r;
+                        const double v0 = m0 * ir, v1 = m1 * ir, v2 = m2 * ir;
+                        qn.rho = (float)r;
+                        qn.vn = (float)v0;
+                        qn.vt1 = (float)v1;
+                        qn.vt2 = (float)v2;
+                        qn.p = (float)(k.km1 * (en - 0.5 * (m0 * v0 + m1 * v1 + m2 * v2)));
+                        qn.E = (float)en;
+                    }
+                }
+                if (side) riemann32(a.surface_flux, qo, qn, Fs[1], k);
+                else riemann32(a.surface_flux, qn, qo, Fs[0], k);
+            }
+            // ---- volume: 6 node pairs of the line from registers
+            float t[NN][V];
+#pragma unroll
+            for (int i = 0; i < NN; ++i)
+#pragma unroll
+                for (int v = 0; v < V; ++v) t[i][v] = 0.0f;
+#pragma unroll
+            for (int i = 0; i < NN - 1; ++i) {
+#pragma unroll
+                for (int m = i + 1; m < NN; ++m) {
+                    float F[V];
+                    if (a.volume_flux == NEMO_VOLFLUX_CENTRAL) {
+                        float fa[V], fb[V];
+                        xflux32(prim(i), fa);
+                        xflux32(prim(m), fb);
+#pragma unroll
+                        for (int v = 0; v < V; ++v) F[v] = 0.5f * (fa[v] + fb[v]);
+                    } else {
+                        const float dens = lnmean32(rho[i], rho[m]);
+                        const float velx = 0.5f * (vn[i] + vn[m]), vely = 0.5f * (w1[i] + w1[m]);
+                        const float velz = 0.5f * (w2[i] + w2[m]);
+                        const float pres = 0.5f * (rho[i] + rho[m]) / (bt[i] + bt[m]);
+                        const float vsq = (vn[i] * vn[i] + w1[i] * w1[i] + w2[i] * w2[i]) +
+                                          (vn[m] * vn[m] + w1[m] * w1[m] + w2[m] * w2[m]);
+                        const float enth = c_enth / lnmean32(bt[i], bt[m]) + pres / dens + velx * velx + vely * vely +
+                                           velz * velz - 0.25f * vsq;
+                        F[0] = dens * velx;
+                        F[1] = F[0] * velx + pres;
+                        F[2] = F[0] * vely;
+                        F[3] = F[0] * velz;
+                        F[4] = F[0] * enth;
+                    }
+                    const float sim = (float)k.S[i * NN + m], smi = (float)k.S[m * NN + i];
+#pragma unroll
+                    for (int v = 0; v < V; ++v) {
+                        t[i][v] += sim * F[v];
+                        t[m][v] += smi * F[v];
+                    }
+                }
+            }
+            // ---- lift
+            const float w0 = (float)k.winv[0], w3 = (float)k.winv[NN - 1];
+#pragma unroll
+            for (int v = 0; v < V; ++v) {
+                t[0][v] -= w0 * Fs[0][v];
+                t[NN - 1][v] += w3 * Fs[1][v];
+            }
+            // ---- FV subcells and the convex blend
+            if (BLEND) {
+                const float al = s_alpha[el];
+                if (al > 0.0f) {
+                    float Fl[V], Fr[V];
+#pragma unroll
+                    for (int v = 0; v < V; ++v) Fl[v] = Fs[0][v];
+#pragma unroll
+                    for (int i = 0; i < NN; ++i) {
+                        if (i < NN - 1) {
+                            riemann32(a.surface_flux, prim(i), prim(i + 1), Fr, k);
+                        } else {
+#pragma unroll
+                            for (int v = 0; v < V; ++v) Fr[v] = Fs[1][v];
+                        }
+                        const float wi = (float)k.winv[i];
+#pragma unroll
+                        for (int v = 0; v < V; ++v) {
+                            t[i][v] = (1.0f - al) * t[i][v] + al * (wi * (Fr[v] - Fl[v]));
+                            Fl[v] = Fr[v];
+                        }
+                    }
+                }
+            }
+            // ---- accumulate c_d * t into the element's rhs terms (x writes, y and z add)
+            const float cd = (float)a.cdel[e * 3 + d];
+            const int vo[V] = {0, 1 + c0, 1 + c1, 1 + c2, 4};
+#pragma unroll
+            for (int i = 0; i < NN; ++i)
+#pragma unroll
+                for (int v = 0; v < V; ++v) {
+                    float& R = sR[(vo[v] * EPC + el) * NP + idx[i]];
+                    R = (d == 0 ? 0.0f : R) + cd * t[i][v];
+                }
+        }
+        __syncthreads();
+    }
+
+    // ---- FP64 register/state update of the thread's x-line nodes
     const int st = a.stage;
     const double A = rk_a(st);
-    const double Cdt = rk_c(st) * ctrl->dt[0];
-    for (int p = tid; p < nel * NP; p += NT) {
-        const int pel = p / NP, n = p % NP;
-        const int64_t pe = e0 + pel;
-        const double cdt = a.group ? rk_c(st) * ctrl->dt[a.group[pe]] : Cdt;
+    const double cdt = a.group ? (active ? rk_c(st) * ctrl->dt[a.group[e]] : 0.0) : rk_c(st) * ctrl->dt[0];
+    if (active) {
+        bool ok = true;
 #pragma unroll
-        for (int v = 0; v < V; ++v) {
-            const int s = (v * EPC + pel) * NP + n;
-            const float R3 = (sR[s] + sR[V * EPC * NP + s]) + sR[2 * V * EPC * NP + s];
-            const double rhs = -(double)R3;
-            const int64_t g = ((int64_t)v * E + pe) * NP + n;
-            if (RHS_ONLY) {
-                a.rhs_out[g] = rhs;
-            } else {
-                const double r2 = st == 0 ? rhs : A * a.reg[g] + rhs;
-                a.reg[g] = r2;
-                su[s] = su[s] + cdt * r2;
+        for (int v = 0; v < V; ++v)
+#pragma unroll
+            for (int i = 0; i < NN; ++i) {
+                const int n = nidx(i, la, lb);
+                const int s = (v * EPC + el) * NP + n;
+                const double rhs = -(double)sR[s];
+                const int64_t g = ((int64_t)v * E + e) * NP + n;
+                if (RHS_ONLY) {
+                    a.rhs_out[g] = rhs;
+                } else {
+                    const double r2 = st == 0 ? rhs : A * sg[s] + rhs;
+                    sg[s] = r2;
+                    su[s] = su[s] + cdt * r2;
+                }
             }
-        }
         if (!RHS_ONLY && a.positivity) {
-            double q[V];
 #pragma unroll
-            for (int v = 0; v < V; ++v) q[v] = su[(v * EPC + pel) * NP + n];
-            if (!isvalid64(q, k)) s_bad[pel] = 1;
+            for (int i = 0; i < NN; ++i) {
+                const int n = nidx(i, la, lb);
+                double q[V];
+#pragma unroll
+                for (int v = 0; v < V; ++v) q[v] = su[(v * EPC + el) * NP + n];
+                ok = ok && isvalid64(q, k);
+            }
+            if (!ok) s_bad[el] = 1;
         }
     }
     if (RHS_ONLY) return;
     __syncthreads();
-    if (a.positivity && tid < nel && s_bad[tid]) {
-        // the repair of the plain path, on the FP64 state (rare)
-        if (!repair_elem<EPC>(su, tid, k)) atomicAdd(&ctrl->nbad, 1ull);
+    if (a.positivity && active && ab == 0 && s_bad[el]) {
+        if (!repair_elem<EPC>(su, el, k)) atomicAdd(&ctrl->nbad, 1ull);
     }
+    // make the generic-proxy writes of su/sg visible to the bulk copies, then store the tile
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncthreads();
-    for (int p = tid; p < nel * NP; p += NT) {
-        const int pel = p / NP, n = p % NP;
-#pragma unroll
-        for (int v = 0; v < V; ++v) a.u_out[((int64_t)v * E + e0 + pel) * NP + n] = su[(v * EPC + pel) * NP + n];
-    }
+    if (tid == 0) tile_store32(su, a.u_out, sg, a.reg, E, e0, nel);
     if (st == 4 && blockIdx.x == 0 && tid == 0) {
         for (int g = 0; g < ctrl->ngroups; ++g) ctrl->t[g] = ctrl->t[g] + ctrl->dt[g];
         ctrl->steps += 1;
@@ -424,98 +478,104 @@ __global__ void __launch_bounds__(NT, 2) k_stage_euler32(StageArgs a) {
 
     // ---- epilogue on the new state: modal indicator (FP32) and CFL bound (FP32 speeds, FP64 min)
     const bool need_lam = a.epi_dt != 0;
-    if (a.alpha_out || need_lam) {
-        float* q = sR;                 // [EPC][64]
-        float* t1 = sR + EPC * NP;
-        float* t2 = sR + 2 * EPC * NP;
-        for (int p = tid; p < nel * NP; p += NT) {
-            const int pel = p / NP, n = p % NP;
-            const double r = su[(0 * EPC + pel) * NP + n];
-            const double mx = su[(1 * EPC + pel) * NP + n], my = su[(2 * EPC + pel) * NP + n];
-            const double mz = su[(3 * EPC + pel) * NP + n], en = su[(4 * EPC + pel) * NP + n];
+    if (!a.alpha_out && !need_lam) {
+        if (tid == 0) tile_store_wait32();
+        return;
+    }
+    float qx[NN];
+    float lx = 0.f, ly = 0.f, lz = 0.f;
+    if (active) {
+#pragma unroll
+        for (int i = 0; i < NN; ++i) {
+            const int n = nidx(i, la, lb);
+            const double r = su[(0 * EPC + el) * NP + n];
+            const double mx = su[(1 * EPC + el) * NP + n], my = su[(2 * EPC + el) * NP + n];
+            const double mz = su[(3 * EPC + el) * NP + n], en = su[(4 * EPC + el) * NP + n];
             const double ir = 1.0 / r;
-            const double pr = k.km1 * (en - 0.5 * ir * (mx * mx + my * my + mz * mz));
-            q[pel * NP + n] = (float)(r * pr);
+            const double prd = k.km1 * (en - 0.5 * ir * (mx * mx + my * my + mz * mz));
+            qx[i] = (float)(r * prd);
             if (need_lam) {
-                const float c = sqrtf((float)(k.kappa * pr * ir));
-                const float vx = (float)(mx * ir), vy = (float)(my * ir), vz = (float)(mz * ir);
-                atomicMax(&s_lam[pel][0], __float_as_uint(fabsf(vx) + c));
-                atomicMax(&s_lam[pel][1], __float_as_uint(fabsf(vy) + c));
-                atomicMax(&s_lam[pel][2], __float_as_uint(fabsf(vz) + c));
+                const float c = sqrtf((float)(k.kappa * prd * ir));
+                lx = fmaxf(lx, fabsf((float)(mx * ir)) + c);
+                ly = fmaxf(ly, fabsf((float)(my * ir)) + c);
+                lz = fmaxf(lz, fabsf((float)(mz * ir)) + c);
+            }
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < NN; ++i) qx[i] = 0.f;
+    }
+    if (a.alpha_out) {
+        float* t1 = sq;               // [EPC][64], the node data is dead now
+        float* t2 = sq + EPC * NP;
+        // x transform of the thread's own line, in registers
+        if (active) {
+#pragma unroll
+            for (int o = 0; o < NN; ++o) {
+                float s = 0.f;
+#pragma unroll
+                for (int i = 0; i < NN; ++i) s += (float)k.Vinv[o * NN + i] * qx[i];
+                t1[el * NP + nidx(o, la, lb)] = s;
             }
         }
         __syncthreads();
-        if (a.alpha_out) {
-            for (int p = tid; p < nel * NP; p += NT) {
-                const int pel = p / NP, n = p % NP;
-                const int ai = n % NN, j = (n / NN) % NN, kk = n / NF;
-                float s = 0.0f;
+        if (active) {   // y transform of the line (la, ., lb)
 #pragma unroll
-                for (int i = 0; i < NN; ++i) s += (float)k.Vinv[ai * NN + i] * q[pel * NP + nidx(i, j, kk)];
-                t1[pel * NP + n] = s;
-            }
-            __syncthreads();
-            for (int p = tid; p < nel * NP; p += NT) {
-                const int pel = p / NP, n = p % NP;
-                const int ai = n % NN, bj = (n / NN) % NN, kk = n / NF;
-                float s = 0.0f;
+            for (int o = 0; o < NN; ++o) {
+                float s = 0.f;
 #pragma unroll
-                for (int j = 0; j < NN; ++j) s += (float)k.Vinv[bj * NN + j] * t1[pel * NP + nidx(ai, j, kk)];
-                t2[pel * NP + n] = s;
-            }
-            __syncthreads();
-            for (int p = tid; p < nel * NP; p += NT) {
-                const int pel = p / NP, n = p % NP;
-                const int ai = n % NN, bj = (n / NN) % NN, cc = n / NF;
-                float s = 0.0f;
-#pragma unroll
-                for (int kk = 0; kk < NN; ++kk) s += (float)k.Vinv[cc * NN + kk] * t2[pel * NP + nidx(ai, bj, kk)];
-                q[pel * NP + n] = s * s;  // modal energies
-            }
-            __syncthreads();
-            // energies summed by the 64 modes of each element: one warp-sized group per element
-            if (tid < nel * 32) {
-                const int pel = tid / 32, lane = tid % 32;
-                float tot = 0.f, c1s = 0.f, c2s = 0.f;
-#pragma unroll
-                for (int h = 0; h < 2; ++h) {
-                    const int n = lane + 32 * h;
-                    const int ai = n % NN, bj = (n / NN) % NN, cc = n / NF;
-                    const float e2 = q[pel * NP + n];
-                    tot += e2;
-                    if (ai < NN - 1 && bj < NN - 1 && cc < NN - 1) c1s += e2;
-                    if (ai < NN - 2 && bj < NN - 2 && cc < NN - 2) c2s += e2;
-                }
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) {
-                    tot += __shfl_xor_sync(0xffffffffu, tot, o);
-                    c1s += __shfl_xor_sync(0xffffffffu, c1s, o);
-                    c2s += __shfl_xor_sync(0xffffffffu, c2s, o);
-                }
-                if (lane == 0) {
-                    const float energy = fmaxf((tot - c1s) / tot, (c1s - c2s) / c1s);
-                    float al = 1.0f / (1.0f + __expf((float)k.ind_k * (energy - (float)k.ind_T)));
-                    if (al < (float)k.alpha_min) al = 0.0f;
-                    else if (al > (float)k.one_m_alpha_min) al = 1.0f;
-                    a.alpha_out[e0 + pel] = (double)fminf((float)k.alpha_max, al);
-                }
+                for (int j = 0; j < NN; ++j) s += (float)k.Vinv[o * NN + j] * t1[el * NP + nidx(la, j, lb)];
+                t2[el * NP + nidx(la, o, lb)] = s;
             }
         }
-        if (need_lam && tid < nel) {
-            const int64_t pe = e0 + tid;
-            const double lf = (double)__uint_as_float(s_lam[tid][0]);
-            const double lg = (double)__uint_as_float(s_lam[tid][1]);
-            const double lh = (double)__uint_as_float(s_lam[tid][2]);
-            const double dte = fmin(fmin(a.delta[pe * 3 + 0] / lf, a.delta[pe * 3 + 1] / lg), a.delta[pe * 3 + 2] / lh);
-            const int g = a.group ? a.group[pe] : 0;
-            atomicMin(&ctrl->dtmin_bits[g], (unsigned long long)__double_as_longlong(dte));
-            atomicMax(&ctrl->lmax_bits[g], (unsigned long long)__double_as_longlong(fmax(fmax(lf, lg), lh)));
+        __syncthreads();
+        float tot = 0.f, cl1 = 0.f, cl2 = 0.f;
+        if (active) {   // z transform of the line (la, lb, .), energies of its 4 modes
+#pragma unroll
+            for (int o = 0; o < NN; ++o) {
+                float s = 0.f;
+#pragma unroll
+                for (int kk = 0; kk < NN; ++kk) s += (float)k.Vinv[o * NN + kk] * t2[el * NP + nidx(la, lb, kk)];
+                const float e2 = s * s;
+                tot += e2;
+                if (la < NN - 1 && lb < NN - 1 && o < NN - 1) cl1 += e2;
+                if (la < NN - 2 && lb < NN - 2 && o < NN - 2) cl2 += e2;
+            }
+        }
+#pragma unroll
+        for (int o = 8; o > 0; o >>= 1) {
+            tot += __shfl_xor_sync(0xffffffffu, tot, o);
+            cl1 += __shfl_xor_sync(0xffffffffu, cl1, o);
+            cl2 += __shfl_xor_sync(0xffffffffu, cl2, o);
+        }
+        if (active && ab == 0) {
+            const float energy = fmaxf((tot - cl1) / tot, (cl1 - cl2) / cl1);
+            float al = 1.0f / (1.0f + __expf((float)k.ind_k * (energy - (float)k.ind_T)));
+            if (al < (float)k.alpha_min) al = 0.0f;
+            else if (al > (float)k.one_m_alpha_min) al = 1.0f;
+            a.alpha_out[e] = (double)fminf((float)k.alpha_max, al);
         }
     }
+    if (need_lam) {
+#pragma unroll
+        for (int o = 8; o > 0; o >>= 1) {
+            lx = fmaxf(lx, __shfl_xor_sync(0xffffffffu, lx, o));
+            ly = fmaxf(ly, __shfl_xor_sync(0xffffffffu, ly, o));
+            lz = fmaxf(lz, __shfl_xor_sync(0xffffffffu, lz, o));
+        }
+        if (active && ab == 0) {
+            const double dte = fmin(fmin(a.delta[e * 3 + 0] / (double)lx, a.delta[e * 3 + 1] / (double)ly),
+                                    a.delta[e * 3 + 2] / (double)lz);
+            const int g = a.group ? a.group[e] : 0;
+            atomicMin(&ctrl->dtmin_bits[g], (unsigned long long)__double_as_longlong(dte));
+            atomicMax(&ctrl->lmax_bits[g], (unsigned long long)__double_as_longlong((double)fmaxf(fmaxf(lx, ly), lz)));
+        }
+    }
+    if (tid == 0) tile_store_wait32();
 }
 
 int stage_smem_bytes32() {
-    return V * EPC * NP * (int)sizeof(double) + (8 + 3 * V) * EPC * NP * (int)sizeof(float);
+    return 2 * V * EPC * NP * (int)sizeof(double) + (NQ + V) * EPC * NP * (int)sizeof(float);
 }
 
 cudaError_t launch_stage_euler32(const StageArgs& a, bool blend, bool rhs_only, cudaStream_t s) {
