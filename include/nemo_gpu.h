@@ -150,6 +150,39 @@ int nemo_gpu_totals(double* out);
 /* Simulation time of group 0 and the accumulated repair-failure count. */
 int nemo_gpu_status(double* t_out, int64_t* nbad_total_out);
 
+/* ---- learned shock indicator ---------------------------------------------------------------
+   Network: x = feature/10 + 1 (12 inputs), h1 = SiLU(W1 x + b1) (32), h2 = SiLU(W2 h1 + b2) (32),
+   alpha = alpha_max * sigmoid(W3 . h2 + b3), alpha < alpha_min -> 0.  Packed weights (1505 values):
+   W1[32][12] b1[32] W2[32][32] b2[32] W3[32] b3.  Features per element: for q = rho then p, direction
+   x, y, z and polynomial order N then N-1, log(E_q,d,o / E_q + 1e-12) with E the modal energies.  The
+   modal indicator stays the fallback (inputs outside the training bounds, or an element whose minimum
+   nodal rho or p is below a tenth of its mean) and the judge (mean |alpha_learned - alpha_modal|).
+   No counterpart in the reference (its indicator module is absent from the snapshot). */
+
+/* Load the weights (rounded to BF16; evaluated in FP32 by the FP32 form, in FP64 by the plain form)
+   and the per-input bounds lo[12], hi[12] of the training data (normalised inputs). */
+int nemo_gpu_set_mlp(const float* weights, int32_t nweights, const float* lo, const float* hi);
+
+/* Features [E][12] (FP32) and the modal alpha [E] of the current state. */
+int nemo_gpu_features(float* feat_host, double* alpha_modal_host);
+
+/* Since the last upload: elements that fell back to the modal indicator, elements judged, and the
+   mean |alpha_learned - alpha_modal| over the judged ones. */
+int nemo_gpu_indicator_stats(int64_t* fallback_out, int64_t* judged_out, double* judge_mae_out);
+
+/* Training on the GPU with the library's own forward/backward/Adam kernels (mini-batch Adam,
+   mean squared error against target alphas).  weights: in = initial, out = trained (FP32, 1505).
+   loss_out: per-epoch mean batch loss (epochs values) or NULL. */
+int nemo_gpu_mlp_train(const float* feat, const float* target, int64_t nsamp, float* weights, float alpha_max,
+                       int32_t epochs, int32_t batch, float lr, uint64_t seed, float* loss_out);
+
+/* Loss and gradient of the mean squared error over all nsamp samples (one forward+backward). */
+int nemo_gpu_mlp_grad(const float* feat, const float* target, int64_t nsamp, const float* weights, float alpha_max,
+                      float* loss_out, float* grad_out);
+
+/* Network output alpha_max * sigmoid(z) per sample (before the alpha_min clip). */
+int nemo_gpu_mlp_forward(const float* feat, int64_t nsamp, const float* weights, float alpha_max, float* alpha_out);
+
 /* Conserved totals (as nemo_gpu_totals) of a state held in device memory that the caller owns,
    without allocating anything.  No counterpart in the reference: it serves hosts that cannot
    allocate device memory at this point (device arrays owned by a Fortran/OpenACC pool sized at

@@ -25,7 +25,8 @@ EXPORTS = [
     "nemo_gpu_calc_timestep", "nemo_gpu_stage", "nemo_gpu_step", "nemo_gpu_run", "nemo_gpu_rhs",
     "nemo_gpu_alpha", "nemo_gpu_totals", "nemo_gpu_status", "nemo_gpu_finalize",
     "nemo_gpu_last_error", "nemo_gpu_set_timing", "nemo_gpu_kernel_timing", "nemo_gpu_stream",
-    "nemo_gpu_totals_noalloc",
+    "nemo_gpu_totals_noalloc", "nemo_gpu_set_mlp", "nemo_gpu_features", "nemo_gpu_indicator_stats",
+    "nemo_gpu_mlp_train", "nemo_gpu_mlp_grad", "nemo_gpu_mlp_forward",
 ]
 
 
@@ -85,6 +86,12 @@ def load(path=LIB_PATH):
                                    ctypes.POINTER(i64)],
         "nemo_gpu_stream": [ctypes.POINTER(ctypes.c_uint64)],
         "nemo_gpu_totals_noalloc": [vp, vp, i64, i32, vp, ctypes.c_uint64],
+        "nemo_gpu_set_mlp": [vp, i32, vp, vp],
+        "nemo_gpu_features": [vp, vp],
+        "nemo_gpu_indicator_stats": [ctypes.POINTER(i64), ctypes.POINTER(i64), ctypes.POINTER(dbl)],
+        "nemo_gpu_mlp_train": [vp, vp, i64, vp, ctypes.c_float, i32, i32, ctypes.c_float, ctypes.c_uint64, vp],
+        "nemo_gpu_mlp_grad": [vp, vp, i64, vp, ctypes.c_float, vp, vp],
+        "nemo_gpu_mlp_forward": [vp, i64, vp, ctypes.c_float, vp],
     }
     for name, args in sig.items():
         f = getattr(L, name)

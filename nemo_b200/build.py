@@ -21,6 +21,7 @@ SOURCES = {
     "stage_fp64.cu": ["-fmad=false"],
     "stage_fp32.cu": ["--use_fast_math"],
     "noalloc.cu": ["-fmad=false"],
+    "mlp.cu": ["--use_fast_math"],
 }
 
 

@@ -29,7 +29,14 @@ struct Control {
     unsigned long long nbad;                  // elements whose positivity repair failed
     unsigned long long steps;
     unsigned long long fallback;              // elements that used the modal fallback (learned indicator)
+    double judge_sum;                         // sum |alpha_learned - alpha_modal| over judged elements
+    unsigned long long judge_n;               // number of judged elements
 };
+
+// Learned indicator: packed MLP weights (W1[32][12], b1[32], W2[32][32], b2[32], W3[32], b3)
+// followed by the lower and upper bounds of the 12 normalised inputs.
+constexpr int MLP_NW = 32 * 12 + 32 + 32 * 32 + 32 + 32 + 1;
+constexpr int MLP_NPACK = MLP_NW + 24;
 
 // Operator constants (filled once by nemo_gpu_init from the host-built matrices).
 struct OpConsts {

@@ -29,22 +29,16 @@ struct StageArgs {
     int32_t positivity;
     int32_t surface_flux;
     int32_t volume_flux;
-};
-
-struct PrepArgs {
-    int64_t E;
-    const double* u;
-    const double* delta;
-    const int32_t* group;
-    double* alpha_out;        // or null
-    int32_t dt_candidates;    // accumulate the CFL bound into ctrl
-    Control* ctrl;
+    int32_t prep_only;        // only the epilogue on u_in (indicator and CFL bound of a state)
+    const double* mlp64;      // learned indicator (FP64 values of the BF16 weights) or null
+    const float* mlp32;       // same, FP32
+    float* feat_out;          // FP32 form, prepare launches: indicator features [E][12] or null
+    double* alpha_modal_out;  // FP32 form, prepare launches: modal alpha [E] or null
 };
 
 // plain FP64 Euler path (stage_fp64.cu)
 cudaError_t setup_stage_euler64(const OpConsts& ops);
 cudaError_t launch_stage_euler64(const StageArgs& a, bool blend, bool ind, bool rhs_only, cudaStream_t s);
-cudaError_t launch_prepare_euler64(const PrepArgs& a, cudaStream_t s);
 cudaError_t launch_totals64(const double* u, const double* delta, int64_t E, int nv, double* part, double* out,
                             cudaStream_t s);
 int stage_smem_bytes64();
@@ -53,6 +47,12 @@ int stage_smem_bytes64();
 cudaError_t setup_stage_euler32(const OpConsts& ops);
 cudaError_t launch_stage_euler32(const StageArgs& a, bool blend, bool rhs_only, cudaStream_t s);
 int stage_smem_bytes32();
+
+// learned-indicator training (mlp.cu)
+cudaError_t mlp_grad_launch(const float* feat, const float* target, const int32_t* idx, int64_t n, const float* W,
+                            float amax, float* grad, float* loss, cudaStream_t s);
+cudaError_t mlp_adam_launch(float* W, const float* grad, float* m, float* v, int step, float lr, cudaStream_t s);
+cudaError_t mlp_forward_launch(const float* feat, int64_t n, const float* W, float amax, float* out, cudaStream_t s);
 
 // control kernels (control.cu)
 cudaError_t launch_ctrl_reset(Control* c, cudaStream_t s);

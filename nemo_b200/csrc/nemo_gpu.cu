@@ -179,6 +179,12 @@ struct Lib {
 
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
 
+    // learned indicator: BF16-rounded weights + input bounds, as FP32 and FP64 arrays
+    float* mlp32 = nullptr;
+    double* mlp64 = nullptr;
+    bool mlp_ready = false;
+    float* feat_dev = nullptr;     // [E][12] features of nemo_gpu_features
+
     bool timing = false;
     double t_stage_ms = 0.0, t_total_ms = 0.0;
     int64_t n_stage = 0, n_total = 0;
@@ -218,6 +224,8 @@ void release_mesh() {
     free_dev(g.alpha[0]); free_dev(g.alpha[1]); free_dev(g.alpha_used);
     free_dev(g.nbr); free_dev(g.cdel); free_dev(g.delta); free_dev(g.group);
     free_dev(g.part);
+    free_dev(g.feat_dev);
+    g.feat_dev = nullptr;
     g.u[0] = g.u[1] = g.reg = g.stagebuf = nullptr;
     g.alpha[0] = g.alpha[1] = g.alpha_used = nullptr;
     g.nbr = nullptr; g.cdel = g.delta = nullptr; g.group = nullptr; g.part = nullptr;
@@ -248,6 +256,12 @@ StageArgs stage_args(int st, bool rhs_only) {
     a.positivity = g.cfg.positivity;
     a.surface_flux = g.cfg.surface_flux;
     a.volume_flux = g.cfg.volume_flux;
+    a.prep_only = 0;
+    const bool learned = g.cfg.indicator == NEMO_IND_LEARNED && g.mlp_ready;
+    a.mlp64 = learned ? g.mlp64 : nullptr;
+    a.mlp32 = learned ? g.mlp32 : nullptr;
+    a.feat_out = nullptr;
+    a.alpha_modal_out = nullptr;
     return a;
 }
 
@@ -263,16 +277,17 @@ cudaError_t launch_stage(int st, cudaStream_t s) {
     return e;
 }
 
-cudaError_t launch_prepare(bool dt_cand, cudaStream_t s) {
-    PrepArgs p{};
-    p.E = g.E;
-    p.u = g.u[g.cur];
-    p.delta = g.delta;
-    p.group = g.ngroups > 1 ? g.group : nullptr;
-    p.alpha_out = blended() ? g.alpha[g.cur] : nullptr;
-    p.dt_candidates = dt_cand ? 1 : 0;
-    p.ctrl = g.ctrl;
-    return launch_prepare_euler64(p, s);
+// Indicator (and, if dt_cand, the CFL bound) of the state in u[cur]: the stage kernel's epilogue
+// on the loaded state.
+cudaError_t launch_prepare(bool dt_cand, cudaStream_t s, float* feat = nullptr, double* alpha_modal = nullptr) {
+    StageArgs a = stage_args(0, true);
+    a.prep_only = 1;
+    a.alpha_out = blended() ? g.alpha[g.cur] : (feat ? g.alpha_used : nullptr);
+    a.epi_dt = dt_cand ? 1 : 0;
+    a.feat_out = feat;
+    a.alpha_modal_out = alpha_modal;
+    if (feat) return launch_stage_euler32(a, blended(), false, s);
+    return launch_stage_any(a, false, s);
 }
 
 int ensure_ready() {
@@ -371,7 +386,7 @@ int nemo_gpu_init(const nemo_cfg* cfg) {
         return fail(NEMO_ERR_ARG, "unsupported surface flux %d", cfg->surface_flux);
     if (cfg->precision != NEMO_PREC_FP64 && cfg->precision != NEMO_PREC_FP32)
         return fail(NEMO_ERR_ARG, "unsupported precision %d", cfg->precision);
-    if (cfg->indicator != NEMO_IND_NONE && cfg->indicator != NEMO_IND_MODAL)
+    if (cfg->indicator != NEMO_IND_NONE && cfg->indicator != NEMO_IND_MODAL && cfg->indicator != NEMO_IND_LEARNED)
         return fail(NEMO_ERR_ARG, "unsupported indicator %d", cfg->indicator);
     if (!(cfg->kappa > 1.0)) return fail(NEMO_ERR_ARG, "kappa must be > 1");
     int ndev = 0;
@@ -404,6 +419,9 @@ int nemo_gpu_init(const nemo_cfg* cfg) {
     CK(cudaMalloc(&g.ctrl, sizeof(Control)));
     CK(cudaMemset(g.ctrl, 0, sizeof(Control)));
     CK(cudaMalloc(&g.tot, 16 * sizeof(double)));
+    CK(cudaMalloc(&g.mlp32, sizeof(float) * MLP_NPACK));
+    CK(cudaMalloc(&g.mlp64, sizeof(double) * MLP_NPACK));
+    g.mlp_ready = false;
     g.inited = true;
     g.ngroups = 1;
     return NEMO_OK;
@@ -729,14 +747,176 @@ int nemo_gpu_stream(uint64_t* out) {
     return NEMO_OK;
 }
 
+int nemo_gpu_set_mlp(const float* weights, int32_t nweights, const float* lo, const float* hi) {
+    if (!g.inited) return fail(NEMO_ERR_STATE, "nemo_gpu_init has not been called");
+    if (!weights || !lo || !hi) return fail(NEMO_ERR_ARG, "NULL weights or bounds");
+    if (nweights != MLP_NW) return fail(NEMO_ERR_ARG, "the indicator MLP has %d weights (got %d)", MLP_NW, nweights);
+    std::vector<float> w32(MLP_NPACK);
+    std::vector<double> w64(MLP_NPACK);
+    for (int i = 0; i < MLP_NW; ++i) {
+        // round to BF16 (nearest, ties to even): the network is stored and evaluated from BF16 weights
+        uint32_t b;
+        std::memcpy(&b, &weights[i], 4);
+        if ((b & 0x7f800000u) != 0x7f800000u) b = (b + 0x7fffu + ((b >> 16) & 1u)) & 0xffff0000u;
+        else b &= 0xffff0000u;
+        float r;
+        std::memcpy(&r, &b, 4);
+        w32[i] = r;
+        w64[i] = (double)r;
+    }
+    for (int i = 0; i < 12; ++i) {
+        w32[MLP_NW + i] = lo[i];
+        w32[MLP_NW + 12 + i] = hi[i];
+        w64[MLP_NW + i] = (double)lo[i];
+        w64[MLP_NW + 12 + i] = (double)hi[i];
+    }
+    CK(cudaMemcpy(g.mlp32, w32.data(), sizeof(float) * MLP_NPACK, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(g.mlp64, w64.data(), sizeof(double) * MLP_NPACK, cudaMemcpyHostToDevice));
+    g.mlp_ready = true;
+    release_graphs();
+    g.prepared = false;
+    return NEMO_OK;
+}
+
+int nemo_gpu_features(float* feat_host, double* alpha_modal_host) {
+    int st = ensure_ready();
+    if (st) return st;
+    if (!feat_host) return fail(NEMO_ERR_ARG, "feat_host is NULL");
+    if (!g.feat_dev) CK(cudaMalloc(&g.feat_dev, sizeof(float) * 12 * g.E));
+    double* am = g.part;  // [E] scratch (the totals partials are not live here)
+    CK(launch_ctrl_reset(g.ctrl, g.stream));
+    CK(launch_prepare(false, g.stream, g.feat_dev, am));
+    CK(cudaMemcpyAsync(feat_host, g.feat_dev, sizeof(float) * 12 * g.E, cudaMemcpyDeviceToHost, g.stream));
+    if (alpha_modal_host) CK(cudaMemcpyAsync(alpha_modal_host, am, sizeof(double) * g.E, cudaMemcpyDeviceToHost, g.stream));
+    g.prepared = false;
+    return check_ctrl_error();
+}
+
+int nemo_gpu_indicator_stats(int64_t* fallback_out, int64_t* judged_out, double* judge_mae_out) {
+    int st = ensure_ready();
+    if (st) return st;
+    unsigned long long fb = 0, jn = 0;
+    double js = 0.0;
+    CK(cudaMemcpyAsync(&fb, &g.ctrl->fallback, 8, cudaMemcpyDeviceToHost, g.stream));
+    CK(cudaMemcpyAsync(&jn, &g.ctrl->judge_n, 8, cudaMemcpyDeviceToHost, g.stream));
+    CK(cudaMemcpyAsync(&js, &g.ctrl->judge_sum, 8, cudaMemcpyDeviceToHost, g.stream));
+    CK(cudaStreamSynchronize(g.stream));
+    if (fallback_out) *fallback_out = (int64_t)fb;
+    if (judged_out) *judged_out = (int64_t)jn;
+    if (judge_mae_out) *judge_mae_out = jn ? js / (double)jn : 0.0;
+    return NEMO_OK;
+}
+
+// ---- training (independent of init: own buffers, default stream) -------------------------------
+
+namespace {
+struct DevBuf {
+    void* p = nullptr;
+    ~DevBuf() { if (p) cudaFree(p); }
+};
+}  // namespace
+
+int nemo_gpu_mlp_grad(const float* feat, const float* target, int64_t nsamp, const float* weights, float amax,
+                      float* loss_out, float* grad_out) {
+    if (!feat || !target || !weights || nsamp <= 0) return fail(NEMO_ERR_ARG, "bad training arguments");
+    DevBuf f, t, w, gr, l;
+    CK(cudaMalloc(&f.p, sizeof(float) * 12 * nsamp));
+    CK(cudaMalloc(&t.p, sizeof(float) * nsamp));
+    CK(cudaMalloc(&w.p, sizeof(float) * MLP_NW));
+    CK(cudaMalloc(&gr.p, sizeof(float) * MLP_NW));
+    CK(cudaMalloc(&l.p, sizeof(float)));
+    CK(cudaMemcpy(f.p, feat, sizeof(float) * 12 * nsamp, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(t.p, target, sizeof(float) * nsamp, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(w.p, weights, sizeof(float) * MLP_NW, cudaMemcpyHostToDevice));
+    CK(cudaMemset(gr.p, 0, sizeof(float) * MLP_NW));
+    CK(cudaMemset(l.p, 0, sizeof(float)));
+    CK(mlp_grad_launch((const float*)f.p, (const float*)t.p, nullptr, nsamp, (const float*)w.p, amax, (float*)gr.p,
+                       (float*)l.p, 0));
+    CK(cudaDeviceSynchronize());
+    if (loss_out) CK(cudaMemcpy(loss_out, l.p, sizeof(float), cudaMemcpyDeviceToHost));
+    if (grad_out) CK(cudaMemcpy(grad_out, gr.p, sizeof(float) * MLP_NW, cudaMemcpyDeviceToHost));
+    return NEMO_OK;
+}
+
+int nemo_gpu_mlp_forward(const float* feat, int64_t nsamp, const float* weights, float amax, float* alpha_out) {
+    if (!feat || !weights || !alpha_out || nsamp <= 0) return fail(NEMO_ERR_ARG, "bad forward arguments");
+    DevBuf f, w, o;
+    CK(cudaMalloc(&f.p, sizeof(float) * 12 * nsamp));
+    CK(cudaMalloc(&w.p, sizeof(float) * MLP_NW));
+    CK(cudaMalloc(&o.p, sizeof(float) * nsamp));
+    CK(cudaMemcpy(f.p, feat, sizeof(float) * 12 * nsamp, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(w.p, weights, sizeof(float) * MLP_NW, cudaMemcpyHostToDevice));
+    CK(mlp_forward_launch((const float*)f.p, nsamp, (const float*)w.p, amax, (float*)o.p, 0));
+    CK(cudaDeviceSynchronize());
+    CK(cudaMemcpy(alpha_out, o.p, sizeof(float) * nsamp, cudaMemcpyDeviceToHost));
+    return NEMO_OK;
+}
+
+int nemo_gpu_mlp_train(const float* feat, const float* target, int64_t nsamp, float* weights, float amax,
+                       int32_t epochs, int32_t batch, float lr, uint64_t seed, float* loss_out) {
+    if (!feat || !target || !weights || nsamp <= 0 || epochs <= 0 || batch <= 0 || !(lr > 0.f))
+        return fail(NEMO_ERR_ARG, "bad training arguments");
+    if (nsamp > INT32_MAX) return fail(NEMO_ERR_ARG, "at most 2^31-1 samples");
+    DevBuf f, t, w, gr, m, v, l, ix;
+    CK(cudaMalloc(&f.p, sizeof(float) * 12 * nsamp));
+    CK(cudaMalloc(&t.p, sizeof(float) * nsamp));
+    CK(cudaMalloc(&w.p, sizeof(float) * MLP_NW));
+    CK(cudaMalloc(&gr.p, sizeof(float) * MLP_NW));
+    CK(cudaMalloc(&m.p, sizeof(float) * MLP_NW));
+    CK(cudaMalloc(&v.p, sizeof(float) * MLP_NW));
+    CK(cudaMalloc(&l.p, sizeof(float)));
+    CK(cudaMalloc(&ix.p, sizeof(int32_t) * nsamp));
+    CK(cudaMemcpy(f.p, feat, sizeof(float) * 12 * nsamp, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(t.p, target, sizeof(float) * nsamp, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(w.p, weights, sizeof(float) * MLP_NW, cudaMemcpyHostToDevice));
+    CK(cudaMemset(m.p, 0, sizeof(float) * MLP_NW));
+    CK(cudaMemset(v.p, 0, sizeof(float) * MLP_NW));
+    std::vector<int32_t> perm(nsamp);
+    for (int64_t i = 0; i < nsamp; ++i) perm[i] = (int32_t)i;
+    uint64_t state = seed ? seed : 0x9E3779B97F4A7C15ull;
+    int step = 0;
+    for (int ep = 0; ep < epochs; ++ep) {
+        for (int64_t i = nsamp - 1; i > 0; --i) {  // Fisher-Yates with a splitmix64 stream
+            state += 0x9E3779B97F4A7C15ull;
+            uint64_t z = state;
+            z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+            z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+            z ^= z >> 31;
+            const int64_t j = (int64_t)(z % (uint64_t)(i + 1));
+            std::swap(perm[i], perm[j]);
+        }
+        CK(cudaMemcpy(ix.p, perm.data(), sizeof(int32_t) * nsamp, cudaMemcpyHostToDevice));
+        CK(cudaMemset(l.p, 0, sizeof(float)));
+        int64_t nb = 0;
+        for (int64_t b0 = 0; b0 < nsamp; b0 += batch) {
+            const int64_t nbat = std::min<int64_t>(batch, nsamp - b0);
+            CK(cudaMemsetAsync(gr.p, 0, sizeof(float) * MLP_NW, 0));
+            CK(mlp_grad_launch((const float*)f.p, (const float*)t.p, (const int32_t*)ix.p + b0, nbat,
+                               (const float*)w.p, amax, (float*)gr.p, (float*)l.p, 0));
+            CK(mlp_adam_launch((float*)w.p, (const float*)gr.p, (float*)m.p, (float*)v.p, ++step, lr, 0));
+            ++nb;
+        }
+        float ls = 0.f;
+        CK(cudaMemcpy(&ls, l.p, sizeof(float), cudaMemcpyDeviceToHost));
+        if (loss_out) loss_out[ep] = ls / (float)nb;
+    }
+    CK(cudaMemcpy(weights, w.p, sizeof(float) * MLP_NW, cudaMemcpyDeviceToHost));
+    return NEMO_OK;
+}
+
 int nemo_gpu_finalize(void) {
     if (!g.inited) return NEMO_OK;
     cudaStreamSynchronize(g.stream);
     release_mesh();
     free_dev(g.ctrl);
     free_dev(g.tot);
+    free_dev(g.mlp32);
+    free_dev(g.mlp64);
     g.ctrl = nullptr;
     g.tot = nullptr;
+    g.mlp32 = nullptr;
+    g.mlp64 = nullptr;
+    g.mlp_ready = false;
     cudaStreamDestroy(g.stream);
     g.stream = nullptr;
     g.inited = false;

@@ -204,6 +204,218 @@ __device__ __forceinline__ float lnmean32(float a, float b) {
     return (a - b) / __logf(a / b);
 }
 
+
+// Epilogue on a state held in smem (FP64): the blending coefficient for the next stage (modal
+// indicator, or the learned indicator with the modal one as fallback and judge) and, if requested,
+// the per-element CFL bound.  16 threads per element; thread (a,b) starts from its x-line nodes.
+__device__ __forceinline__ float hsum16(float v) {
+#pragma unroll
+    for (int o = 8; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+__device__ __forceinline__ float hmax16(float v) {
+#pragma unroll
+    for (int o = 8; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+__device__ __forceinline__ float hmin16(float v) {
+#pragma unroll
+    for (int o = 8; o > 0; o >>= 1) v = fminf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+__device__ __forceinline__ void epilogue32(const StageArgs& a, const double* su, float* scratch, int el, int ab, int la,
+                                           int lb, bool active, int64_t e, const OpConsts& k) {
+    Control* ctrl = a.ctrl;
+    const bool need_lam = a.epi_dt != 0;
+    if (!a.alpha_out && !need_lam) return;
+    float qr[NN], qp[NN];
+    float lx = 0.f, ly = 0.f, lz = 0.f;
+#pragma unroll
+    for (int i = 0; i < NN; ++i) {
+        qr[i] = 1.f;
+        qp[i] = 1.f;
+    }
+    if (active) {
+#pragma unroll
+        for (int i = 0; i < NN; ++i) {
+            const int n = nidx(i, la, lb);
+            const double r = su[(0 * EPC + el) * NP + n];
+            const double mx = su[(1 * EPC + el) * NP + n], my = su[(2 * EPC + el) * NP + n];
+            const double mz = su[(3 * EPC + el) * NP + n], en = su[(4 * EPC + el) * NP + n];
+            const double ir = 1.0 / r;
+            const double prd = k.km1 * (en - 0.5 * ir * (mx * mx + my * my + mz * mz));
+            qr[i] = (float)r;
+            qp[i] = (float)prd;
+            if (need_lam) {
+                const float c = sqrtf((float)(k.kappa * prd * ir));
+                lx = fmaxf(lx, fabsf((float)(mx * ir)) + c);
+                ly = fmaxf(ly, fabsf((float)(my * ir)) + c);
+                lz = fmaxf(lz, fabsf((float)(mz * ir)) + c);
+            }
+        }
+    }
+    if (a.alpha_out) {
+        const bool learned = a.mlp32 != nullptr;
+        const bool want_feat = learned || a.feat_out != nullptr;
+        float* t1 = scratch;             // [EPC][64]
+        float* t2 = scratch + EPC * NP;  // [EPC][64]
+        float tot[3] = {0.f, 0.f, 0.f}, cl1 = 0.f, cl2 = 0.f, Eo[2][6];
+#pragma unroll
+        for (int w = 0; w < 2; ++w)
+#pragma unroll
+            for (int i = 0; i < 6; ++i) Eo[w][i] = 0.f;
+        const int nq = want_feat ? 3 : 1;   // rho*p, then rho and p
+        for (int w = 0; w < nq; ++w) {
+            if (active) {
+#pragma unroll
+                for (int o = 0; o < NN; ++o) {
+                    float s = 0.f;
+#pragma unroll
+                    for (int i = 0; i < NN; ++i) {
+                        const float qv = w == 0 ? qr[i] * qp[i] : (w == 1 ? qr[i] : qp[i]);
+                        s += (float)k.Vinv[o * NN + i] * qv;
+                    }
+                    t1[el * NP + nidx(o, la, lb)] = s;
+                }
+            }
+            __syncthreads();
+            if (active) {
+#pragma unroll
+                for (int o = 0; o < NN; ++o) {
+                    float s = 0.f;
+#pragma unroll
+                    for (int j = 0; j < NN; ++j) s += (float)k.Vinv[o * NN + j] * t1[el * NP + nidx(la, j, lb)];
+                    t2[el * NP + nidx(la, o, lb)] = s;
+                }
+            }
+            __syncthreads();
+            if (active) {
+#pragma unroll
+                for (int o = 0; o < NN; ++o) {
+                    float s = 0.f;
+#pragma unroll
+                    for (int kk = 0; kk < NN; ++kk) s += (float)k.Vinv[o * NN + kk] * t2[el * NP + nidx(la, lb, kk)];
+                    const float e2 = s * s;
+                    tot[w] += e2;
+                    if (w == 0) {
+                        if (la < NN - 1 && lb < NN - 1 && o < NN - 1) cl1 += e2;
+                        if (la < NN - 2 && lb < NN - 2 && o < NN - 2) cl2 += e2;
+                    } else {
+                        const int ord[3] = {la, lb, o};
+#pragma unroll
+                        for (int d = 0; d < 3; ++d) {
+                            if (ord[d] == NN - 1) Eo[w - 1][2 * d] += e2;
+                            if (ord[d] == NN - 2) Eo[w - 1][2 * d + 1] += e2;
+                        }
+                    }
+                }
+            }
+            __syncthreads();
+        }
+        const float t0 = hsum16(tot[0]), c1 = hsum16(cl1), c2 = hsum16(cl2);
+        float am;
+        {
+            const float energy = fmaxf((t0 - c1) / t0, (c1 - c2) / c1);
+            float al = 1.0f / (1.0f + __expf((float)k.ind_k * (energy - (float)k.ind_T)));
+            if (al < (float)k.alpha_min) al = 0.0f;
+            else if (al > (float)k.one_m_alpha_min) al = 1.0f;
+            am = fminf((float)k.alpha_max, al);
+        }
+        float alpha = am;
+        if (a.feat_out) {
+#pragma unroll
+            for (int w = 0; w < 2; ++w) {
+                const float tw = hsum16(tot[1 + w]);
+#pragma unroll
+                for (int i = 0; i < 6; ++i) {
+                    const float f = __logf(hsum16(Eo[w][i]) / tw + 1e-12f);
+                    if (active && ab == 0) a.feat_out[e * 12 + 6 * w + i] = f;
+                }
+            }
+            if (active && ab == 0 && a.alpha_modal_out) a.alpha_modal_out[e] = (double)am;
+        }
+        if (learned) {
+            const float* W = a.mlp32;
+            const float* lo = W + MLP_NW;
+            const float* hi = lo + 12;
+            // positivity-risk check and the 12 features
+            float rs = 0.f, ps = 0.f, rmn = 3.4e38f, pmn = 3.4e38f;
+#pragma unroll
+            for (int i = 0; i < NN; ++i) {
+                rs += qr[i];
+                ps += qp[i];
+                rmn = fminf(rmn, qr[i]);
+                pmn = fminf(pmn, qp[i]);
+            }
+            rs = hsum16(rs);
+            ps = hsum16(ps);
+            rmn = hmin16(rmn);
+            pmn = hmin16(pmn);
+            bool fb = rmn < 0.1f * (rs / 64.0f) || pmn < 0.1f * (ps / 64.0f);
+            float x[12];
+#pragma unroll
+            for (int w = 0; w < 2; ++w) {
+                const float tw = hsum16(tot[1 + w]);
+#pragma unroll
+                for (int i = 0; i < 6; ++i) {
+                    const float f = __logf(hsum16(Eo[w][i]) / tw + 1e-12f);
+                    x[6 * w + i] = f * 0.1f + 1.0f;
+                    fb = fb || x[6 * w + i] < lo[6 * w + i] || x[6 * w + i] > hi[6 * w + i];
+                }
+            }
+            const float* W1 = W;
+            const float* b1 = W1 + 32 * 12;
+            const float* W2 = b1 + 32;
+            const float* b2 = W2 + 32 * 32;
+            const float* W3 = b2 + 32;
+            const int j0 = 2 * ab, j1 = 2 * ab + 1;
+            float s0 = b1[j0], s1 = b1[j1];
+#pragma unroll
+            for (int i = 0; i < 12; ++i) {
+                s0 += W1[j0 * 12 + i] * x[i];
+                s1 += W1[j1 * 12 + i] * x[i];
+            }
+            const float h0 = s0 / (1.0f + __expf(-s0)), h1v = s1 / (1.0f + __expf(-s1));
+            float u0 = b2[j0], u1 = b2[j1];
+#pragma unroll
+            for (int src = 0; src < 16; ++src) {
+                const float he = __shfl_sync(0xffffffffu, h0, src, 16);
+                const float ho = __shfl_sync(0xffffffffu, h1v, src, 16);
+                u0 += W2[j0 * 32 + 2 * src] * he + W2[j0 * 32 + 2 * src + 1] * ho;
+                u1 += W2[j1 * 32 + 2 * src] * he + W2[j1 * 32 + 2 * src + 1] * ho;
+            }
+            const float g0 = u0 / (1.0f + __expf(-u0)), g1 = u1 / (1.0f + __expf(-u1));
+            const float z = hsum16(W3[j0] * g0 + W3[j1] * g1) + W3[32];
+            float al = (float)k.alpha_max / (1.0f + __expf(-z));
+            if (al < (float)k.alpha_min) al = 0.0f;
+            if (fb) {
+                alpha = am;
+                if (active && ab == 0) atomicAdd(&ctrl->fallback, 1ull);
+            } else {
+                alpha = al;
+                if (active && ab == 0) {
+                    atomicAdd(&ctrl->judge_sum, (double)fabsf(al - am));
+                    atomicAdd(&ctrl->judge_n, 1ull);
+                }
+            }
+        }
+        if (active && ab == 0) a.alpha_out[e] = (double)alpha;
+    }
+    if (need_lam) {
+        lx = hmax16(lx);
+        ly = hmax16(ly);
+        lz = hmax16(lz);
+        if (active && ab == 0) {
+            const double dte = fmin(fmin(a.delta[e * 3 + 0] / (double)lx, a.delta[e * 3 + 1] / (double)ly),
+                                    a.delta[e * 3 + 2] / (double)lz);
+            const int g = a.group ? a.group[e] : 0;
+            atomicMin(&ctrl->dtmin_bits[g], (unsigned long long)__double_as_longlong(dte));
+            atomicMax(&ctrl->lmax_bits[g], (unsigned long long)__double_as_longlong((double)fmaxf(fmaxf(lx, ly), lz)));
+        }
+    }
+}
+
 }  // namespace
 
 // One CTA = EPC elements x 16 threads; thread (a,b) of an element owns the x-, y- and z-lines
@@ -246,13 +458,17 @@ __global__ void __launch_bounds__(NT, 3) k_stage_euler32(StageArgs a) {
         }
         s_alpha[tid] = al;
     }
-    const bool load_reg = !RHS_ONLY && a.stage > 0;
+    const bool load_reg = !RHS_ONLY && !a.prep_only && a.stage > 0;
     tile_issue32(su, a.u_in, sg, load_reg ? a.reg : nullptr, E, e0, nel, &bar);
     if (!tile_wait32(&bar, ctrl)) return;
 
     const int el = tid >> 4, ab = tid & 15, la = ab & 3, lb = ab >> 2;
     const bool active = el < nel;
     const int64_t e = e0 + el;
+    if (a.prep_only) {
+        epilogue32(a, su, sq, el, ab, la, lb, active, e, k);
+        return;
+    }
     auto SQ = [&](int q, int elx, int n) -> float& { return sq[(q * EPC + elx) * NP + n]; };
 
     // per-node primitives of the thread's x-line nodes: recovered in FP64, stored in FP32
@@ -476,101 +692,7 @@ __global__ void __launch_bounds__(NT, 3) k_stage_euler32(StageArgs a) {
         ctrl->steps += 1;
     }
 
-    // ---- epilogue on the new state: modal indicator (FP32) and CFL bound (FP32 speeds, FP64 min)
-    const bool need_lam = a.epi_dt != 0;
-    if (!a.alpha_out && !need_lam) {
-        if (tid == 0) tile_store_wait32();
-        return;
-    }
-    float qx[NN];
-    float lx = 0.f, ly = 0.f, lz = 0.f;
-    if (active) {
-#pragma unroll
-        for (int i = 0; i < NN; ++i) {
-            const int n = nidx(i, la, lb);
-            const double r = su[(0 * EPC + el) * NP + n];
-            const double mx = su[(1 * EPC + el) * NP + n], my = su[(2 * EPC + el) * NP + n];
-            const double mz = su[(3 * EPC + el) * NP + n], en = su[(4 * EPC + el) * NP + n];
-            const double ir = 1.0 / r;
-            const double prd = k.km1 * (en - 0.5 * ir * (mx * mx + my * my + mz * mz));
-            qx[i] = (float)(r * prd);
-            if (need_lam) {
-                const float c = sqrtf((float)(k.kappa * prd * ir));
-                lx = fmaxf(lx, fabsf((float)(mx * ir)) + c);
-                ly = fmaxf(ly, fabsf((float)(my * ir)) + c);
-                lz = fmaxf(lz, fabsf((float)(mz * ir)) + c);
-            }
-        }
-    } else {
-#pragma unroll
-        for (int i = 0; i < NN; ++i) qx[i] = 0.f;
-    }
-    if (a.alpha_out) {
-        float* t1 = sq;               // [EPC][64], the node data is dead now
-        float* t2 = sq + EPC * NP;
-        // x transform of the thread's own line, in registers
-        if (active) {
-#pragma unroll
-            for (int o = 0; o < NN; ++o) {
-                float s = 0.f;
-#pragma unroll
-                for (int i = 0; i < NN; ++i) s += (float)k.Vinv[o * NN + i] * qx[i];
-                t1[el * NP + nidx(o, la, lb)] = s;
-            }
-        }
-        __syncthreads();
-        if (active) {   // y transform of the line (la, ., lb)
-#pragma unroll
-            for (int o = 0; o < NN; ++o) {
-                float s = 0.f;
-#pragma unroll
-                for (int j = 0; j < NN; ++j) s += (float)k.Vinv[o * NN + j] * t1[el * NP + nidx(la, j, lb)];
-                t2[el * NP + nidx(la, o, lb)] = s;
-            }
-        }
-        __syncthreads();
-        float tot = 0.f, cl1 = 0.f, cl2 = 0.f;
-        if (active) {   // z transform of the line (la, lb, .), energies of its 4 modes
-#pragma unroll
-            for (int o = 0; o < NN; ++o) {
-                float s = 0.f;
-#pragma unroll
-                for (int kk = 0; kk < NN; ++kk) s += (float)k.Vinv[o * NN + kk] * t2[el * NP + nidx(la, lb, kk)];
-                const float e2 = s * s;
-                tot += e2;
-                if (la < NN - 1 && lb < NN - 1 && o < NN - 1) cl1 += e2;
-                if (la < NN - 2 && lb < NN - 2 && o < NN - 2) cl2 += e2;
-            }
-        }
-#pragma unroll
-        for (int o = 8; o > 0; o >>= 1) {
-            tot += __shfl_xor_sync(0xffffffffu, tot, o);
-            cl1 += __shfl_xor_sync(0xffffffffu, cl1, o);
-            cl2 += __shfl_xor_sync(0xffffffffu, cl2, o);
-        }
-        if (active && ab == 0) {
-            const float energy = fmaxf((tot - cl1) / tot, (cl1 - cl2) / cl1);
-            float al = 1.0f / (1.0f + __expf((float)k.ind_k * (energy - (float)k.ind_T)));
-            if (al < (float)k.alpha_min) al = 0.0f;
-            else if (al > (float)k.one_m_alpha_min) al = 1.0f;
-            a.alpha_out[e] = (double)fminf((float)k.alpha_max, al);
-        }
-    }
-    if (need_lam) {
-#pragma unroll
-        for (int o = 8; o > 0; o >>= 1) {
-            lx = fmaxf(lx, __shfl_xor_sync(0xffffffffu, lx, o));
-            ly = fmaxf(ly, __shfl_xor_sync(0xffffffffu, ly, o));
-            lz = fmaxf(lz, __shfl_xor_sync(0xffffffffu, lz, o));
-        }
-        if (active && ab == 0) {
-            const double dte = fmin(fmin(a.delta[e * 3 + 0] / (double)lx, a.delta[e * 3 + 1] / (double)ly),
-                                    a.delta[e * 3 + 2] / (double)lz);
-            const int g = a.group ? a.group[e] : 0;
-            atomicMin(&ctrl->dtmin_bits[g], (unsigned long long)__double_as_longlong(dte));
-            atomicMax(&ctrl->lmax_bits[g], (unsigned long long)__double_as_longlong((double)fmaxf(fmaxf(lx, ly), lz)));
-        }
-    }
+    epilogue32(a, su, sq, el, ab, la, lb, active, e, k);
     if (tid == 0) tile_store_wait32();
 }
 

@@ -83,6 +83,198 @@ __device__ __forceinline__ bool tile_load(double* su, const double* __restrict__
     return ok;
 }
 
+
+// Epilogue on a state held in smem (the new state of a stage, or the uploaded state of a prepare
+// launch): the blending coefficient for the next stage (modal indicator, or learned indicator with
+// the modal one as fallback and judge) and, if requested, the per-element CFL bound.
+__device__ __forceinline__ double silu64(double x) { return x / (1.0 + pexp64(-x)); }
+
+__device__ void epilogue64(const StageArgs& a, const double* su, double* sp, unsigned long long (*s_lam)[3],
+                           int nel, int64_t e0, int tid, const OpConsts& k) {
+    __shared__ double s_am[EPC];
+    __shared__ int s_fb[EPC];
+    Control* ctrl = a.ctrl;
+    const int64_t E = a.E;
+    (void)E;
+    if (a.alpha_out) {
+        const bool learned = a.mlp64 != nullptr;
+        double* q = sp;
+        double* t1 = sp + EPC * NP;
+        double* t2 = sp + 2 * EPC * NP;
+        const int nq = learned ? 3 : 1;   // modal coefficients of rho*p, then rho and p
+        for (int w = 0; w < nq; ++w) {
+            double* cm = sp + (3 + w) * EPC * NP;
+            for (int p = tid; p < nel * NP; p += NT) {
+                const int pel = p / NP, n = p % NP;
+                double uu[V];
+#pragma unroll
+                for (int v = 0; v < V; ++v) uu[v] = su[(v * EPC + pel) * NP + n];
+                q[pel * NP + n] = w == 0 ? uu[0] * pressure64(uu, k) : (w == 1 ? uu[0] : pressure64(uu, k));
+            }
+            __syncthreads();
+            for (int p = tid; p < nel * NP; p += NT) {
+                const int pel = p / NP, n = p % NP;
+                const int ai = n % NN, j = (n / NN) % NN, kk = n / NF;
+                double s = 0.0;
+#pragma unroll
+                for (int i = 0; i < NN; ++i) s = s + k.Vinv[ai * NN + i] * q[pel * NP + nidx(i, j, kk)];
+                t1[pel * NP + n] = s;
+            }
+            __syncthreads();
+            for (int p = tid; p < nel * NP; p += NT) {
+                const int pel = p / NP, n = p % NP;
+                const int ai = n % NN, bj = (n / NN) % NN, kk = n / NF;
+                double s = 0.0;
+#pragma unroll
+                for (int j = 0; j < NN; ++j) s = s + k.Vinv[bj * NN + j] * t1[pel * NP + nidx(ai, j, kk)];
+                t2[pel * NP + n] = s;
+            }
+            __syncthreads();
+            for (int p = tid; p < nel * NP; p += NT) {
+                const int pel = p / NP, n = p % NP;
+                const int ai = n % NN, bj = (n / NN) % NN, cc = n / NF;
+                double s = 0.0;
+#pragma unroll
+                for (int kk = 0; kk < NN; ++kk) s = s + k.Vinv[cc * NN + kk] * t2[pel * NP + nidx(ai, bj, kk)];
+                cm[pel * NP + n] = s;
+            }
+            __syncthreads();
+        }
+        double* feat = q;   // [EPC][12], the nodal scratch is dead now
+        if (tid < nel) {
+            const double* m = sp + 3 * EPC * NP + tid * NP;
+            double total = 0.0, clip1 = 0.0, clip2 = 0.0;
+            for (int cc = 0; cc < NN; ++cc)
+                for (int bj = 0; bj < NN; ++bj)
+                    for (int ai = 0; ai < NN; ++ai) {
+                        const double mv = m[nidx(ai, bj, cc)];
+                        const double e2 = mv * mv;
+                        total = total + e2;
+                        if (ai < NN - 1 && bj < NN - 1 && cc < NN - 1) clip1 = clip1 + e2;
+                        if (ai < NN - 2 && bj < NN - 2 && cc < NN - 2) clip2 = clip2 + e2;
+                    }
+            const double e1 = (total - clip1) / total;
+            const double e2 = (clip1 - clip2) / clip1;
+            const double energy = fmax(e1, e2);
+            double al = 1.0 / (1.0 + pexp64(k.ind_k * (energy - k.ind_T)));
+            if (al < k.alpha_min) al = 0.0;
+            else if (al > k.one_m_alpha_min) al = 1.0;
+            s_am[tid] = fmin(k.alpha_max, al);
+            int fb = 0;
+            if (learned) {
+                // positivity-risk check: min nodal rho or p below a tenth of the element mean
+                double rs = 0.0, ps = 0.0, rmin = 1e300, pmin = 1e300;
+                for (int n = 0; n < NP; ++n) {
+                    double uu[V];
+#pragma unroll
+                    for (int v = 0; v < V; ++v) uu[v] = su[(v * EPC + tid) * NP + n];
+                    const double pr = pressure64(uu, k);
+                    rs = rs + uu[0];
+                    ps = ps + pr;
+                    rmin = fmin(rmin, uu[0]);
+                    pmin = fmin(pmin, pr);
+                }
+                if (rmin < 0.1 * (rs / 64.0) || pmin < 0.1 * (ps / 64.0)) fb = 1;
+                for (int w = 0; w < 2; ++w) {
+                    const double* mw = sp + (4 + w) * EPC * NP + tid * NP;
+                    double tot = 0.0, Eo[6] = {0, 0, 0, 0, 0, 0};
+                    for (int cc = 0; cc < NN; ++cc)
+                        for (int bj = 0; bj < NN; ++bj)
+                            for (int ai = 0; ai < NN; ++ai) {
+                                const double mv = mw[nidx(ai, bj, cc)];
+                                const double ee = mv * mv;
+                                tot = tot + ee;
+                                const int ord[3] = {ai, bj, cc};
+#pragma unroll
+                                for (int d = 0; d < 3; ++d) {
+                                    if (ord[d] == NN - 1) Eo[2 * d] = Eo[2 * d] + ee;
+                                    if (ord[d] == NN - 2) Eo[2 * d + 1] = Eo[2 * d + 1] + ee;
+                                }
+                            }
+                    for (int i = 0; i < 6; ++i) {
+                        const double f = plog64(Eo[i] / tot + 1e-12);
+                        feat[tid * 12 + 6 * w + i] = f;
+                        const double x = f / 10.0 + 1.0;
+                        if (x < a.mlp64[MLP_NW + 6 * w + i] || x > a.mlp64[MLP_NW + 12 + 6 * w + i]) fb = 1;
+                    }
+                }
+            }
+            s_fb[tid] = fb;
+        }
+        __syncthreads();
+        if (learned) {
+            const double* W1 = a.mlp64;
+            const double* b1 = W1 + 32 * 12;
+            const double* W2 = b1 + 32;
+            const double* b2 = W2 + 32 * 32;
+            const double* W3 = b2 + 32;
+            double* h1 = t1;   // [EPC][32]
+            double* h2 = t2;
+            for (int p = tid; p < nel * 32; p += NT) {
+                const int pel = p / 32, j = p % 32;
+                double s = b1[j];
+                for (int i = 0; i < 12; ++i) s = s + W1[j * 12 + i] * (feat[pel * 12 + i] / 10.0 + 1.0);
+                h1[pel * 32 + j] = silu64(s);
+            }
+            __syncthreads();
+            for (int p = tid; p < nel * 32; p += NT) {
+                const int pel = p / 32, j = p % 32;
+                double s = b2[j];
+                for (int i = 0; i < 32; ++i) s = s + W2[j * 32 + i] * h1[pel * 32 + i];
+                h2[pel * 32 + j] = silu64(s);
+            }
+            __syncthreads();
+            if (tid < nel) {
+                double z = W3[32];
+                for (int j = 0; j < 32; ++j) z = z + W3[j] * h2[tid * 32 + j];
+                double al = k.alpha_max / (1.0 + pexp64(-z));
+                if (al < k.alpha_min) al = 0.0;
+                const double am = s_am[tid];
+                if (s_fb[tid]) {
+                    atomicAdd(&ctrl->fallback, 1ull);
+                    al = am;
+                } else {
+                    atomicAdd(&ctrl->judge_sum, fabs(al - am));
+                    atomicAdd(&ctrl->judge_n, 1ull);
+                }
+                a.alpha_out[e0 + tid] = al;
+            }
+        } else if (tid < nel) {
+            a.alpha_out[e0 + tid] = s_am[tid];
+        }
+    }
+    if (a.epi_dt) {
+        for (int p = tid; p < nel * NP; p += NT) {
+            const int pel = p / NP, n = p % NP;
+            double uu[V];
+#pragma unroll
+            for (int v = 0; v < V; ++v) uu[v] = su[(v * EPC + pel) * NP + n];
+            double rr[V];
+#pragma unroll
+            for (int dd = 0; dd < 3; ++dd) {
+                rr[0] = uu[0];
+                rr[1] = uu[1 + dd];
+                rr[2] = uu[1 + (dd + 1) % 3];
+                rr[3] = uu[1 + (dd + 2) % 3];
+                rr[4] = uu[4];
+                const double lam = xlambda64(rr, k);
+                atomicMax(&s_lam[pel][dd], (unsigned long long)__double_as_longlong(lam));
+            }
+        }
+        __syncthreads();
+        if (tid < nel) {
+            const int64_t pe = e0 + tid;
+            const double lf = __longlong_as_double((long long)s_lam[tid][0]);
+            const double lg = __longlong_as_double((long long)s_lam[tid][1]);
+            const double lh = __longlong_as_double((long long)s_lam[tid][2]);
+            const double dte = fmin(fmin(a.delta[pe * 3 + 0] / lf, a.delta[pe * 3 + 1] / lg), a.delta[pe * 3 + 2] / lh);
+            const int g = a.group ? a.group[pe] : 0;
+            atomicMin(&ctrl->dtmin_bits[g], (unsigned long long)__double_as_longlong(dte));
+            atomicMax(&ctrl->lmax_bits[g], (unsigned long long)__double_as_longlong(fmax(fmax(lf, lg), lh)));
+        }
+    }
+}
+
 }  // namespace
 
 template <bool BLEND, bool IND, bool RHS_ONLY>
@@ -124,6 +316,10 @@ __global__ void __launch_bounds__(NT, 1) k_stage_euler64(StageArgs a) {
         s_alpha[tid] = al;
     }
     if (!tile_load(su, a.u_in, E, e0, nel, &bar, ctrl)) return;
+    if (a.prep_only) {
+        epilogue64(a, su, smem + V * EPC * NP, s_lam, nel, e0, tid, k);
+        return;
+    }
 
     // per-node primitives: velocities and, per direction d, beta_d = rho/(2 p_d) where p_d is the
     // pressure of the state rotated into direction d (the reference evaluates the two-point flux on
@@ -349,187 +545,7 @@ __global__ void __launch_bounds__(NT, 1) k_stage_euler64(StageArgs a) {
         ctrl->steps += 1;
     }
 
-    // ---- epilogue: indicator of the new state (for the next stage)
-    if (a.alpha_out) {
-        double* q = sp;                    // [EPC][64] rho*p
-        double* t1 = sp + EPC * NP;        // [EPC][64]
-        double* t2 = sp + 2 * EPC * NP;    // [EPC][64]
-        for (int p = tid; p < nel * NP; p += NT) {
-            const int pel = p / NP, n = p % NP;
-            double uu[V];
-#pragma unroll
-            for (int v = 0; v < V; ++v) uu[v] = su[(v * EPC + pel) * NP + n];
-            q[pel * NP + n] = uu[0] * pressure64(uu, k);
-        }
-        __syncthreads();
-        // 1D transforms, one output per thread (x, then y, then z)
-        for (int p = tid; p < nel * NP; p += NT) {
-            const int pel = p / NP, n = p % NP;
-            const int ai = n % NN, j = (n / NN) % NN, kk = n / NF;
-            double s = 0.0;
-#pragma unroll
-            for (int i = 0; i < NN; ++i) s = s + k.Vinv[ai * NN + i] * q[pel * NP + nidx(i, j, kk)];
-            t1[pel * NP + n] = s;
-        }
-        __syncthreads();
-        for (int p = tid; p < nel * NP; p += NT) {
-            const int pel = p / NP, n = p % NP;
-            const int ai = n % NN, bj = (n / NN) % NN, kk = n / NF;
-            double s = 0.0;
-#pragma unroll
-            for (int j = 0; j < NN; ++j) s = s + k.Vinv[bj * NN + j] * t1[pel * NP + nidx(ai, j, kk)];
-            t2[pel * NP + n] = s;
-        }
-        __syncthreads();
-        for (int p = tid; p < nel * NP; p += NT) {
-            const int pel = p / NP, n = p % NP;
-            const int ai = n % NN, bj = (n / NN) % NN, cc = n / NF;
-            double s = 0.0;
-#pragma unroll
-            for (int kk = 0; kk < NN; ++kk) s = s + k.Vinv[cc * NN + kk] * t2[pel * NP + nidx(ai, bj, kk)];
-            q[pel * NP + n] = s;  // modal coefficients
-        }
-        __syncthreads();
-        if (tid < nel) {
-            const double* m = q + tid * NP;
-            double total = 0.0, clip1 = 0.0, clip2 = 0.0;
-            for (int cc = 0; cc < NN; ++cc)
-                for (int bj = 0; bj < NN; ++bj)
-                    for (int ai = 0; ai < NN; ++ai) {
-                        const double mv = m[nidx(ai, bj, cc)];
-                        const double e2 = mv * mv;
-                        total = total + e2;
-                        if (ai < NN - 1 && bj < NN - 1 && cc < NN - 1) clip1 = clip1 + e2;
-                        if (ai < NN - 2 && bj < NN - 2 && cc < NN - 2) clip2 = clip2 + e2;
-                    }
-            const double e1 = (total - clip1) / total;
-            const double e2 = (clip1 - clip2) / clip1;
-            const double energy = fmax(e1, e2);
-            double al = 1.0 / (1.0 + pexp64(k.ind_k * (energy - k.ind_T)));
-            if (al < k.alpha_min) al = 0.0;
-            else if (al > k.one_m_alpha_min) al = 1.0;
-            a.alpha_out[e0 + tid] = fmin(k.alpha_max, al);
-        }
-    }
-
-    // ---- epilogue: CFL bound of the new state (last stage only)
-    if (a.epi_dt) {
-        for (int p = tid; p < nel * NP; p += NT) {
-            const int pel = p / NP, n = p % NP;
-            double uu[V];
-#pragma unroll
-            for (int v = 0; v < V; ++v) uu[v] = su[(v * EPC + pel) * NP + n];
-            double rr[V];
-#pragma unroll
-            for (int dd = 0; dd < 3; ++dd) {
-                rr[0] = uu[0];
-                rr[1] = uu[1 + dd];
-                rr[2] = uu[1 + (dd + 1) % 3];
-                rr[3] = uu[1 + (dd + 2) % 3];
-                rr[4] = uu[4];
-                const double lam = xlambda64(rr, k);
-                atomicMax(&s_lam[pel][dd], (unsigned long long)__double_as_longlong(lam));
-            }
-        }
-        __syncthreads();
-        if (tid < nel) {
-            const int64_t pe = e0 + tid;
-            const double lf = __longlong_as_double((long long)s_lam[tid][0]);
-            const double lg = __longlong_as_double((long long)s_lam[tid][1]);
-            const double lh = __longlong_as_double((long long)s_lam[tid][2]);
-            const double dte = fmin(fmin(a.delta[pe * 3 + 0] / lf, a.delta[pe * 3 + 1] / lg), a.delta[pe * 3 + 2] / lh);
-            const int g = a.group ? a.group[pe] : 0;
-            atomicMin(&ctrl->dtmin_bits[g], (unsigned long long)__double_as_longlong(dte));
-            atomicMax(&ctrl->lmax_bits[g], (unsigned long long)__double_as_longlong(fmax(fmax(lf, lg), lh)));
-        }
-    }
-}
-
-// ---------------------------------------------------------------------------------------------
-// Per-element preparation from a state: raw indicator and CFL bound (used before the first
-// stage and by nemo_gpu_calc_timestep).  One CTA per 4 elements, one thread per node.
-
-__global__ void __launch_bounds__(256) k_prepare_euler64(PrepArgs a) {
-    __shared__ double q[4][NP], t1[4][NP], t2[4][NP];
-    __shared__ unsigned long long s_lam[4][3];
-    const OpConsts& k = c_ops64;
-    const int el = threadIdx.x / NP, n = threadIdx.x % NP;
-    const int64_t e = (int64_t)blockIdx.x * 4 + el;
-    const bool act = e < a.E;
-    if (n < 3) s_lam[el][n] = 0ull;
-    double uu[V];
-    if (act) {
-#pragma unroll
-        for (int v = 0; v < V; ++v) uu[v] = a.u[((int64_t)v * a.E + e) * NP + n];
-        q[el][n] = uu[0] * pressure64(uu, k);
-    }
-    __syncthreads();
-    if (act && a.dt_candidates) {
-        double rr[V];
-#pragma unroll
-        for (int dd = 0; dd < 3; ++dd) {
-            rr[0] = uu[0];
-            rr[1] = uu[1 + dd];
-            rr[2] = uu[1 + (dd + 1) % 3];
-            rr[3] = uu[1 + (dd + 2) % 3];
-            rr[4] = uu[4];
-            atomicMax(&s_lam[el][dd], (unsigned long long)__double_as_longlong(xlambda64(rr, k)));
-        }
-    }
-    if (a.alpha_out) {
-        const int ai = n % NN, j = (n / NN) % NN, kk = n / NF;
-        double s = 0.0;
-        if (act) {
-#pragma unroll
-            for (int i = 0; i < NN; ++i) s = s + k.Vinv[ai * NN + i] * q[el][nidx(i, j, kk)];
-        }
-        t1[el][n] = s;
-        __syncthreads();
-        s = 0.0;
-        if (act) {
-#pragma unroll
-            for (int jj = 0; jj < NN; ++jj) s = s + k.Vinv[j * NN + jj] * t1[el][nidx(ai, jj, kk)];
-        }
-        t2[el][n] = s;
-        __syncthreads();
-        s = 0.0;
-        if (act) {
-#pragma unroll
-            for (int kx = 0; kx < NN; ++kx) s = s + k.Vinv[kk * NN + kx] * t2[el][nidx(ai, j, kx)];
-        }
-        q[el][n] = s;
-    }
-    __syncthreads();
-    if (!act || n != 0) return;
-    if (a.alpha_out) {
-        const double* m = q[el];
-        double total = 0.0, clip1 = 0.0, clip2 = 0.0;
-        for (int cc = 0; cc < NN; ++cc)
-            for (int bj = 0; bj < NN; ++bj)
-                for (int ai = 0; ai < NN; ++ai) {
-                    const double mv = m[nidx(ai, bj, cc)];
-                    const double e2 = mv * mv;
-                    total = total + e2;
-                    if (ai < NN - 1 && bj < NN - 1 && cc < NN - 1) clip1 = clip1 + e2;
-                    if (ai < NN - 2 && bj < NN - 2 && cc < NN - 2) clip2 = clip2 + e2;
-                }
-        const double e1 = (total - clip1) / total;
-        const double e2 = (clip1 - clip2) / clip1;
-        const double energy = fmax(e1, e2);
-        double al = 1.0 / (1.0 + pexp64(k.ind_k * (energy - k.ind_T)));
-        if (al < k.alpha_min) al = 0.0;
-        else if (al > k.one_m_alpha_min) al = 1.0;
-        a.alpha_out[e] = fmin(k.alpha_max, al);
-    }
-    if (a.dt_candidates) {
-        const double lf = __longlong_as_double((long long)s_lam[el][0]);
-        const double lg = __longlong_as_double((long long)s_lam[el][1]);
-        const double lh = __longlong_as_double((long long)s_lam[el][2]);
-        const double dte = fmin(fmin(a.delta[e * 3 + 0] / lf, a.delta[e * 3 + 1] / lg), a.delta[e * 3 + 2] / lh);
-        const int g = a.group ? a.group[e] : 0;
-        atomicMin(&a.ctrl->dtmin_bits[g], (unsigned long long)__double_as_longlong(dte));
-        atomicMax(&a.ctrl->lmax_bits[g], (unsigned long long)__double_as_longlong(fmax(fmax(lf, lg), lh)));
-    }
+    epilogue64(a, su, sp, s_lam, nel, e0, tid, k);
 }
 
 // Conserved totals: per-element weighted sums in the oracle's order, then a serial sum per
@@ -589,12 +605,6 @@ cudaError_t setup_stage_euler64(const OpConsts& ops) {
     err = cudaFuncSetAttribute(k_stage_euler64<false, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (err != cudaSuccess) return err;
     return cudaMemcpyToSymbol(c_ops64, &ops, sizeof(OpConsts));
-}
-
-cudaError_t launch_prepare_euler64(const PrepArgs& a, cudaStream_t s) {
-    const int grid = (int)((a.E + 3) / 4);
-    k_prepare_euler64<<<grid, 256, 0, s>>>(a);
-    return cudaGetLastError();
 }
 
 cudaError_t launch_totals64(const double* u, const double* delta, int64_t E, int nv, double* part, double* out,

@@ -471,6 +471,117 @@ double indicator_alpha(const Ctx& c, const double (*ue)[VMAX]) {
     return std::min(c.cfg.alpha_max, alpha);
 }
 
+// 3D modal coefficients of nodal values q (transform along x, then y, then z).
+void modal3(const Ops& op, const double* q, double* m) {
+    double t1[NP], t2[NP];
+    for (int k = 0; k < NN; ++k)
+        for (int j = 0; j < NN; ++j)
+            for (int a = 0; a < NN; ++a) {
+                double s = 0.0;
+                for (int i = 0; i < NN; ++i) s = s + op.Vinv[a * NN + i] * q[nidx(i, j, k)];
+                t1[nidx(a, j, k)] = s;
+            }
+    for (int k = 0; k < NN; ++k)
+        for (int b = 0; b < NN; ++b)
+            for (int a = 0; a < NN; ++a) {
+                double s = 0.0;
+                for (int j = 0; j < NN; ++j) s = s + op.Vinv[b * NN + j] * t1[nidx(a, j, k)];
+                t2[nidx(a, b, k)] = s;
+            }
+    for (int cc = 0; cc < NN; ++cc)
+        for (int b = 0; b < NN; ++b)
+            for (int a = 0; a < NN; ++a) {
+                double s = 0.0;
+                for (int k = 0; k < NN; ++k) s = s + op.Vinv[cc * NN + k] * t2[nidx(a, b, k)];
+                m[nidx(a, b, cc)] = s;
+            }
+}
+
+// Learned-indicator features of one element: for q in (rho, p), direction d in (x, y, z) and
+// polynomial order o in (N, N-1): log(E_{q,d,o} / E_q + 1e-12), E_{q,d,o} the energy of the modes
+// whose order in direction d is o, E_q the total modal energy.  Sums run over modes in the order
+// (z, y, x) as the indicator's.
+void element_features(const Ctx& c, const double (*ue)[VMAX], double* feat) {
+    double q[2][NP], m[NP];
+    for (int p = 0; p < NP; ++p) {
+        q[0][p] = ue[p][0];
+        q[1][p] = e_pressure(ue[p], c.cfg.kappa);
+    }
+    for (int w = 0; w < 2; ++w) {
+        modal3(c.op, q[w], m);
+        double tot = 0.0, E[6] = {0, 0, 0, 0, 0, 0};
+        for (int cc = 0; cc < NN; ++cc)
+            for (int b = 0; b < NN; ++b)
+                for (int a = 0; a < NN; ++a) {
+                    const double e2 = m[nidx(a, b, cc)] * m[nidx(a, b, cc)];
+                    tot = tot + e2;
+                    const int ord[3] = {a, b, cc};
+                    for (int d = 0; d < 3; ++d) {
+                        if (ord[d] == NN - 1) E[2 * d] = E[2 * d] + e2;
+                        if (ord[d] == NN - 2) E[2 * d + 1] = E[2 * d + 1] + e2;
+                    }
+                }
+        for (int i = 0; i < 6; ++i) feat[6 * w + i] = own_log(E[i] / tot + 1e-12);
+    }
+}
+
+// MLP of the learned indicator: 12 -> 32 (SiLU) -> 32 (SiLU) -> 1, alpha = alpha_max * sigmoid.
+// Packed weights: W1[32][12], b1[32], W2[32][32], b2[32], W3[32], b3 (1505 values); input
+// x_i = feat_i / 10 + 1.  Each sum starts from the bias and runs over the inputs in order.
+constexpr int MLP_NW = 32 * 12 + 32 + 32 * 32 + 32 + 32 + 1;
+struct Mlp {
+    bool set = false;
+    double w[MLP_NW];
+    double lo[12], hi[12];   // feature bounds of the training data (normalised inputs)
+};
+Mlp g_mlp;
+
+inline double silu(double x) { return x / (1.0 + own_exp(-x)); }
+
+// Positivity-risk check of the learned indicator: an element whose minimum nodal density or
+// pressure is below a tenth of its mean is handed to the modal indicator.
+bool positivity_risk(const Ctx& c, const double (*ue)[VMAX]) {
+    double rs = 0.0, ps = 0.0, rmin = HUGE_VAL, pmin = HUGE_VAL;
+    for (int p = 0; p < NP; ++p) {
+        const double r = ue[p][0], pr = e_pressure(ue[p], c.cfg.kappa);
+        rs = rs + r;
+        ps = ps + pr;
+        rmin = std::min(rmin, r);
+        pmin = std::min(pmin, pr);
+    }
+    return rmin < 0.1 * (rs / 64.0) || pmin < 0.1 * (ps / 64.0);
+}
+
+// Returns the learned alpha, or -1 when an input lies outside the training bounds (fallback).
+double mlp_alpha(const Ctx& c, const double* feat) {
+    const double* W1 = g_mlp.w;
+    const double* b1 = W1 + 32 * 12;
+    const double* W2 = b1 + 32;
+    const double* b2 = W2 + 32 * 32;
+    const double* W3 = b2 + 32;
+    const double b3 = W3[32];
+    double x[12], h1[32], h2[32];
+    for (int i = 0; i < 12; ++i) {
+        x[i] = feat[i] / 10.0 + 1.0;
+        if (x[i] < g_mlp.lo[i] || x[i] > g_mlp.hi[i]) return -1.0;
+    }
+    for (int j = 0; j < 32; ++j) {
+        double s = b1[j];
+        for (int i = 0; i < 12; ++i) s = s + W1[j * 12 + i] * x[i];
+        h1[j] = silu(s);
+    }
+    for (int j = 0; j < 32; ++j) {
+        double s = b2[j];
+        for (int i = 0; i < 32; ++i) s = s + W2[j * 32 + i] * h1[i];
+        h2[j] = silu(s);
+    }
+    double z = b3;
+    for (int j = 0; j < 32; ++j) z = z + W3[j] * h2[j];
+    double al = c.cfg.alpha_max / (1.0 + own_exp(-z));
+    if (al < c.cfg.alpha_min) al = 0.0;
+    return al;
+}
+
 // rhs of one element: split-form DG volume + surface lift, blended with FV subcells.
 void element_rhs(const Ctx& c, const Mesh& M, const double* u, int64_t e, double alpha, double* rhs) {
     const Ops& op = c.op;
@@ -664,7 +775,13 @@ void compute_alpha(const Ctx& c, const Mesh& M, const double* u, double* alpha, 
     for (int64_t e = 0; e < M.E; ++e) {
         double ue[NP][VMAX];
         gather(c, M.E, u, e, ue);
-        raw[e] = indicator_alpha(c, ue);
+        double a = -1.0;
+        if (c.cfg.indicator == NEMO_IND_LEARNED && g_mlp.set && !positivity_risk(c, ue)) {
+            double f[12];
+            element_features(c, ue, f);
+            a = mlp_alpha(c, f);
+        }
+        raw[e] = a >= 0.0 ? a : indicator_alpha(c, ue);
     }
     for (int64_t e = 0; e < M.E; ++e) {
         double a = raw[e];
@@ -845,6 +962,32 @@ int or_repair(const nemo_cfg* cfg, double* st) {
     for (int v = 0; v < c.V; ++v)
         for (int p = 0; p < NP; ++p) st[v * NP + p] = s[p][v];
     return ok ? 1 : 0;
+}
+
+// Learned indicator weights (1505 values, see mlp_alpha) and normalised-input bounds (12 + 12).
+void or_set_mlp(const double* w, const double* lo, const double* hi) {
+    std::memcpy(g_mlp.w, w, sizeof g_mlp.w);
+    std::memcpy(g_mlp.lo, lo, sizeof g_mlp.lo);
+    std::memcpy(g_mlp.hi, hi, sizeof g_mlp.hi);
+    g_mlp.set = true;
+}
+
+// Features [E][12] and the modal (Hennemann) raw alpha [E] of a state.
+void or_features(const nemo_cfg* cfg, int64_t E, const double* u, double* feat, double* alpha_modal, int nthreads) {
+    Ctx c = make_ctx(cfg);
+#pragma omp parallel for schedule(dynamic, 16) num_threads(nthreads)
+    for (int64_t e = 0; e < E; ++e) {
+        double ue[NP][VMAX];
+        gather(c, E, u, e, ue);
+        element_features(c, ue, feat + 12 * e);
+        if (alpha_modal) alpha_modal[e] = indicator_alpha(c, ue);
+    }
+}
+
+// Learned alpha of given features (-1 = outside the training bounds).
+double or_mlp_alpha(const nemo_cfg* cfg, const double* feat) {
+    Ctx c = make_ctx(cfg);
+    return mlp_alpha(c, feat);
 }
 
 double or_log(double x) { return own_log(x); }

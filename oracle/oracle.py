@@ -60,6 +60,10 @@ def lib():
         L.or_log.argtypes = [ctypes.c_double]
         L.or_exp.restype = ctypes.c_double
         L.or_exp.argtypes = [ctypes.c_double]
+        L.or_set_mlp.argtypes = [_dp, _dp, _dp]
+        L.or_features.argtypes = [ctypes.c_void_p, ctypes.c_int64, _dp, _dp, ctypes.c_void_p, ctypes.c_int]
+        L.or_mlp_alpha.restype = ctypes.c_double
+        L.or_mlp_alpha.argtypes = [ctypes.c_void_p, _dp]
         L.or_repair.restype = ctypes.c_int
         L.or_repair.argtypes = [ctypes.c_void_p, _dp]
         _LIB = L
@@ -96,6 +100,26 @@ def rk_coeffs():
     a, b, c = np.zeros(5), np.zeros(5), np.zeros(5)
     lib().or_rk_coeffs(_p(a), _p(b), _p(c))
     return a, b, c
+
+
+def set_mlp(w, lo, hi):
+    """Weights (1505, FP64 values of the BF16-rounded weights the GPU uses) and input bounds."""
+    w, lo, hi = _f64(w), _f64(lo), _f64(hi)
+    lib().or_set_mlp(_p(w), _p(lo), _p(hi))
+
+
+def features(cfg, u):
+    u = _f64(u)
+    E = u.shape[1]
+    f = np.zeros((E, 12))
+    a = np.zeros(E)
+    lib().or_features(ctypes.byref(cfg), E, _p(u), _p(f), a.ctypes.data, nthreads_default())
+    return f, a
+
+
+def mlp_alpha(cfg, feat):
+    feat = _f64(feat)
+    return lib().or_mlp_alpha(ctypes.byref(cfg), _p(feat))
 
 
 def repair(cfg, st):
