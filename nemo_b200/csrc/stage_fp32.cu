@@ -224,8 +224,9 @@ __device__ __forceinline__ float hmin16(float v) {
     return v;
 }
 
-__device__ __forceinline__ void epilogue32(const StageArgs& a, const double* su, float* scratch, int el, int ab, int la,
-                                           int lb, bool active, int64_t e, const OpConsts& k) {
+__device__ __forceinline__ void epilogue32(const StageArgs& a, const double* su, float* scratch, const float* sw,
+                                           int el, int ab, int la, int lb, bool active, int64_t e,
+                                           const OpConsts& k) {
     Control* ctrl = a.ctrl;
     const bool need_lam = a.epi_dt != 0;
     if (!a.alpha_out && !need_lam) return;
@@ -258,16 +259,18 @@ __device__ __forceinline__ void epilogue32(const StageArgs& a, const double* su,
     if (a.alpha_out) {
         const bool learned = a.mlp32 != nullptr;
         const bool want_feat = learned || a.feat_out != nullptr;
-        float* t1 = scratch;             // [EPC][64]
-        float* t2 = scratch + EPC * NP;  // [EPC][64]
+        // modal transforms of rho*p (and, for the features, rho and p) fused over the quantities:
+        // x in registers, y and z through shared memory [3][EPC][64] each
+        float* t1 = scratch;                 // [3][EPC][64]
+        float* t2 = scratch + 3 * EPC * NP;  // [3][EPC][64]
         float tot[3] = {0.f, 0.f, 0.f}, cl1 = 0.f, cl2 = 0.f, Eo[2][6];
 #pragma unroll
         for (int w = 0; w < 2; ++w)
 #pragma unroll
             for (int i = 0; i < 6; ++i) Eo[w][i] = 0.f;
         const int nq = want_feat ? 3 : 1;   // rho*p, then rho and p
-        for (int w = 0; w < nq; ++w) {
-            if (active) {
+        if (active) {
+            for (int w = 0; w < nq; ++w) {
 #pragma unroll
                 for (int o = 0; o < NN; ++o) {
                     float s = 0.f;
@@ -276,26 +279,31 @@ __device__ __forceinline__ void epilogue32(const StageArgs& a, const double* su,
                         const float qv = w == 0 ? qr[i] * qp[i] : (w == 1 ? qr[i] : qp[i]);
                         s += (float)k.Vinv[o * NN + i] * qv;
                     }
-                    t1[el * NP + nidx(o, la, lb)] = s;
+                    t1[(w * EPC + el) * NP + nidx(o, la, lb)] = s;
                 }
             }
-            __syncthreads();
-            if (active) {
+        }
+        __syncthreads();
+        if (active) {
+            for (int w = 0; w < nq; ++w) {
 #pragma unroll
                 for (int o = 0; o < NN; ++o) {
                     float s = 0.f;
 #pragma unroll
-                    for (int j = 0; j < NN; ++j) s += (float)k.Vinv[o * NN + j] * t1[el * NP + nidx(la, j, lb)];
-                    t2[el * NP + nidx(la, o, lb)] = s;
+                    for (int j = 0; j < NN; ++j) s += (float)k.Vinv[o * NN + j] * t1[(w * EPC + el) * NP + nidx(la, j, lb)];
+                    t2[(w * EPC + el) * NP + nidx(la, o, lb)] = s;
                 }
             }
-            __syncthreads();
-            if (active) {
+        }
+        __syncthreads();
+        if (active) {
+            for (int w = 0; w < nq; ++w) {
 #pragma unroll
                 for (int o = 0; o < NN; ++o) {
                     float s = 0.f;
 #pragma unroll
-                    for (int kk = 0; kk < NN; ++kk) s += (float)k.Vinv[o * NN + kk] * t2[el * NP + nidx(la, lb, kk)];
+                    for (int kk = 0; kk < NN; ++kk)
+                        s += (float)k.Vinv[o * NN + kk] * t2[(w * EPC + el) * NP + nidx(la, lb, kk)];
                     const float e2 = s * s;
                     tot[w] += e2;
                     if (w == 0) {
@@ -311,7 +319,6 @@ __device__ __forceinline__ void epilogue32(const StageArgs& a, const double* su,
                     }
                 }
             }
-            __syncthreads();
         }
         const float t0 = hsum16(tot[0]), c1 = hsum16(cl1), c2 = hsum16(cl2);
         float am;
@@ -364,29 +371,33 @@ __device__ __forceinline__ void epilogue32(const StageArgs& a, const double* su,
                     fb = fb || x[6 * w + i] < lo[6 * w + i] || x[6 * w + i] > hi[6 * w + i];
                 }
             }
-            const float* W1 = W;
-            const float* b1 = W1 + 32 * 12;
-            const float* W2 = b1 + 32;
-            const float* b2 = W2 + 32 * 32;
+            // sw: W1 transposed [12][32], b1[32], W2 transposed [32][32], b2[32], W3[32], b3
+            const float* W1T = sw;
+            const float* b1 = W1T + 12 * 32;
+            const float* W2T = b1 + 32;
+            const float* b2 = W2T + 32 * 32;
             const float* W3 = b2 + 32;
-            const int j0 = 2 * ab, j1 = 2 * ab + 1;
-            float s0 = b1[j0], s1 = b1[j1];
+            const int j0 = 2 * ab;
+            float2 sacc = *reinterpret_cast<const float2*>(b1 + j0);
 #pragma unroll
             for (int i = 0; i < 12; ++i) {
-                s0 += W1[j0 * 12 + i] * x[i];
-                s1 += W1[j1 * 12 + i] * x[i];
+                const float2 wv = *reinterpret_cast<const float2*>(W1T + i * 32 + j0);
+                sacc.x += wv.x * x[i];
+                sacc.y += wv.y * x[i];
             }
-            const float h0 = s0 / (1.0f + __expf(-s0)), h1v = s1 / (1.0f + __expf(-s1));
-            float u0 = b2[j0], u1 = b2[j1];
+            const float h0 = sacc.x / (1.0f + __expf(-sacc.x)), h1v = sacc.y / (1.0f + __expf(-sacc.y));
+            float2 uacc = *reinterpret_cast<const float2*>(b2 + j0);
 #pragma unroll
             for (int src = 0; src < 16; ++src) {
                 const float he = __shfl_sync(0xffffffffu, h0, src, 16);
                 const float ho = __shfl_sync(0xffffffffu, h1v, src, 16);
-                u0 += W2[j0 * 32 + 2 * src] * he + W2[j0 * 32 + 2 * src + 1] * ho;
-                u1 += W2[j1 * 32 + 2 * src] * he + W2[j1 * 32 + 2 * src + 1] * ho;
+                const float2 we = *reinterpret_cast<const float2*>(W2T + (2 * src) * 32 + j0);
+                const float2 wo = *reinterpret_cast<const float2*>(W2T + (2 * src + 1) * 32 + j0);
+                uacc.x += we.x * he + wo.x * ho;
+                uacc.y += we.y * he + wo.y * ho;
             }
-            const float g0 = u0 / (1.0f + __expf(-u0)), g1 = u1 / (1.0f + __expf(-u1));
-            const float z = hsum16(W3[j0] * g0 + W3[j1] * g1) + W3[32];
+            const float g0 = uacc.x / (1.0f + __expf(-uacc.x)), g1 = uacc.y / (1.0f + __expf(-uacc.y));
+            const float z = hsum16(W3[j0] * g0 + W3[j0 + 1] * g1) + W3[32];
             float al = (float)k.alpha_max / (1.0f + __expf(-z));
             if (al < (float)k.alpha_min) al = 0.0f;
             if (fb) {
@@ -431,6 +442,7 @@ __global__ void __launch_bounds__(NT, 3) k_stage_euler32(StageArgs a) {
     __shared__ uint64_t bar;
     __shared__ float s_alpha[EPC];
     __shared__ int s_bad[EPC];
+    __shared__ __align__(16) float s_w[MLP_NW];   // learned indicator, transposed layout
 
     const OpConsts& k = c_ops32;
     Control* ctrl = a.ctrl;
@@ -439,6 +451,18 @@ __global__ void __launch_bounds__(NT, 3) k_stage_euler32(StageArgs a) {
     const int64_t E = a.E;
     const int64_t e0 = (int64_t)blockIdx.x * EPC;
     const int nel = (int)min((int64_t)EPC, E - e0);
+    if (a.mlp32) {  // visible to the epilogue after the barriers of the stage
+        for (int i = tid; i < MLP_NW; i += NT) {
+            float v;
+            if (i < 12 * 32) v = a.mlp32[(i % 32) * 12 + i / 32];                           // W1T[i/32][i%32]
+            else if (i < 12 * 32 + 32) v = a.mlp32[i];                                        // b1
+            else if (i < 12 * 32 + 32 + 32 * 32) {
+                const int r = i - (12 * 32 + 32);
+                v = a.mlp32[12 * 32 + 32 + (r % 32) * 32 + r / 32];                           // W2T[r/32][r%32]
+            } else v = a.mlp32[i];                                                            // b2, W3, b3
+            s_w[i] = v;
+        }
+    }
 
     if (tid < EPC) {
         s_bad[tid] = 0;
@@ -466,7 +490,8 @@ __global__ void __launch_bounds__(NT, 3) k_stage_euler32(StageArgs a) {
     const bool active = el < nel;
     const int64_t e = e0 + el;
     if (a.prep_only) {
-        epilogue32(a, su, sq, el, ab, la, lb, active, e, k);
+        __syncthreads();
+        epilogue32(a, su, sq, s_w, el, ab, la, lb, active, e, k);
         return;
     }
     auto SQ = [&](int q, int elx, int n) -> float& { return sq[(q * EPC + elx) * NP + n]; };
@@ -692,7 +717,7 @@ __global__ void __launch_bounds__(NT, 3) k_stage_euler32(StageArgs a) {
         ctrl->steps += 1;
     }
 
-    epilogue32(a, su, sq, el, ab, la, lb, active, e, k);
+    epilogue32(a, su, sq, s_w, el, ab, la, lb, active, e, k);
     if (tid == 0) tile_store_wait32();
 }
 
