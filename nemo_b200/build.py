@@ -17,7 +17,7 @@ COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-ffp-contract=o
 # per-source extra flags
 SOURCES = {
     "nemo_gpu.cu": [],
-    "control.cu": [],
+    "control.cu": ["-fmad=false"],
     "stage_fp64.cu": ["-fmad=false"],
     "stage_fp32.cu": ["--use_fast_math"],
     "noalloc.cu": ["-fmad=false"],

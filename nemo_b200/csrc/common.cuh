@@ -31,6 +31,11 @@ struct Control {
     unsigned long long fallback;              // elements that used the modal fallback (learned indicator)
     double judge_sum;                         // sum |alpha_learned - alpha_modal| over judged elements
     unsigned long long judge_n;               // number of judged elements
+    double glm_ch;                            // GLM cleaning speed of the current step (MHD)
+    double glm_alpha;                         // GLM damping of the current step (MHD)
+    unsigned long long vmax_bits;             // max |velocity component| (positive double bits, MHD)
+    int32_t mhd;                              // 1: update glm_ch/glm_alpha from lmax/vmax each step
+    int32_t pad2;
 };
 
 // Learned indicator: packed MLP weights (W1[32][12], b1[32], W2[32][32], b2[32], W3[32], b3)

@@ -13,6 +13,7 @@ __global__ void k_ctrl_reset(Control* c) {
         c->dtmin_bits[g] = POS_INF_BITS;
         c->lmax_bits[g] = 0ull;
     }
+    if (g == 0) c->vmax_bits = 0ull;
 }
 
 __global__ void k_ctrl_set_dt(Control* c, double dt) {
@@ -25,7 +26,16 @@ __global__ void k_ctrl_set_dt(Control* c, double dt) {
 // step's last stage (or by a prepare launch): dt = factor * min(delta/lambda), clamped to t_end.
 __global__ void k_ctrl_step(Control* c) {
     __shared__ int s_live;
-    if (threadIdx.x == 0) s_live = 0;
+    if (threadIdx.x == 0) {
+        s_live = 0;
+        if (c->mhd) {  // GLM cleaning speed and damping of this step (kernel_timestep_mod.f90:338-344)
+            const double lmax = __longlong_as_double((long long)c->lmax_bits[0]);
+            const double vmax = __longlong_as_double((long long)c->vmax_bits);
+            c->glm_ch = 2.0 * fabs(lmax - vmax);
+            c->glm_alpha = c->glm_ch / 0.18;
+            c->vmax_bits = 0ull;
+        }
+    }
     __syncthreads();
     for (int g = threadIdx.x; g < c->ngroups; g += blockDim.x) {
         const double dtmin = __longlong_as_double((long long)c->dtmin_bits[g]);

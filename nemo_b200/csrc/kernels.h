@@ -48,6 +48,12 @@ cudaError_t setup_stage_euler32(const OpConsts& ops);
 cudaError_t launch_stage_euler32(const StageArgs& a, bool blend, bool rhs_only, cudaStream_t s);
 int stage_smem_bytes32();
 
+// GLM-MHD stages (stage_mhd.cuh instantiated in stage_fp64.cu / stage_fp32.cu)
+cudaError_t setup_stage_mhd64();
+cudaError_t setup_stage_mhd32();
+cudaError_t launch_stage_mhd64(const StageArgs& a, bool blend, bool rhs_only, cudaStream_t s);
+cudaError_t launch_stage_mhd32(const StageArgs& a, bool blend, bool rhs_only, cudaStream_t s);
+
 // learned-indicator training (mlp.cu)
 cudaError_t mlp_grad_launch(const float* feat, const float* target, const int32_t* idx, int64_t n, const float* W,
                             float amax, float* grad, float* loss, cudaStream_t s);

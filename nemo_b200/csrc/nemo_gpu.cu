@@ -265,7 +265,13 @@ StageArgs stage_args(int st, bool rhs_only) {
     return a;
 }
 
+bool is_mhd() { return g.cfg.eqn == NEMO_EQN_MHD; }
+
 cudaError_t launch_stage_any(const StageArgs& a, bool rhs_only, cudaStream_t s) {
+    if (is_mhd()) {
+        if (g.cfg.precision == NEMO_PREC_FP32) return launch_stage_mhd32(a, blended(), rhs_only, s);
+        return launch_stage_mhd64(a, blended(), rhs_only, s);
+    }
     if (g.cfg.precision == NEMO_PREC_FP32) return launch_stage_euler32(a, blended(), rhs_only, s);
     return launch_stage_euler64(a, blended(), blended(), rhs_only, s);
 }
@@ -378,12 +384,22 @@ int nemo_gpu_operators(int32_t n, double* nodes, double* weights, double* dmat, 
 int nemo_gpu_init(const nemo_cfg* cfg) {
     if (!cfg) return fail(NEMO_ERR_ARG, "cfg is NULL");
     if (cfg->n_nodes != NN) return fail(NEMO_ERR_ARG, "n_nodes must be %d", NN);
-    if (cfg->eqn != NEMO_EQN_EULER || cfg->n_vars != 5)
-        return fail(NEMO_ERR_ARG, "only the Euler equations (n_vars 5) are supported by this build");
-    if (cfg->volume_flux != NEMO_VOLFLUX_CHANDRASHEKAR && cfg->volume_flux != NEMO_VOLFLUX_CENTRAL)
-        return fail(NEMO_ERR_ARG, "unsupported volume flux %d", cfg->volume_flux);
-    if (cfg->surface_flux != NEMO_SURFFLUX_HLLC && cfg->surface_flux != NEMO_SURFFLUX_RUSANOV)
-        return fail(NEMO_ERR_ARG, "unsupported surface flux %d", cfg->surface_flux);
+    if (cfg->eqn == NEMO_EQN_EULER) {
+        if (cfg->n_vars != 5) return fail(NEMO_ERR_ARG, "the Euler equations have n_vars 5");
+        if (cfg->volume_flux != NEMO_VOLFLUX_CHANDRASHEKAR && cfg->volume_flux != NEMO_VOLFLUX_CENTRAL)
+            return fail(NEMO_ERR_ARG, "unsupported Euler volume flux %d", cfg->volume_flux);
+        if (cfg->surface_flux != NEMO_SURFFLUX_HLLC && cfg->surface_flux != NEMO_SURFFLUX_RUSANOV)
+            return fail(NEMO_ERR_ARG, "unsupported Euler surface flux %d", cfg->surface_flux);
+    } else if (cfg->eqn == NEMO_EQN_MHD) {
+        if (cfg->n_vars != 9) return fail(NEMO_ERR_ARG, "GLM-MHD has n_vars 9");
+        if (cfg->volume_flux != NEMO_VOLFLUX_EC_MHD && cfg->volume_flux != NEMO_VOLFLUX_CENTRAL)
+            return fail(NEMO_ERR_ARG, "unsupported MHD volume flux %d", cfg->volume_flux);
+        if (cfg->surface_flux != NEMO_SURFFLUX_RUSANOV)
+            return fail(NEMO_ERR_ARG, "MHD surface flux %d is not available in this build (Rusanov only)", cfg->surface_flux);
+        if (!(cfg->mu0 > 0.0)) return fail(NEMO_ERR_ARG, "mu0 must be positive");
+    } else {
+        return fail(NEMO_ERR_ARG, "unknown equation system %d", cfg->eqn);
+    }
     if (cfg->precision != NEMO_PREC_FP64 && cfg->precision != NEMO_PREC_FP32)
         return fail(NEMO_ERR_ARG, "unsupported precision %d", cfg->precision);
     if (cfg->indicator != NEMO_IND_NONE && cfg->indicator != NEMO_IND_MODAL && cfg->indicator != NEMO_IND_LEARNED)
@@ -416,6 +432,8 @@ int nemo_gpu_init(const nemo_cfg* cfg) {
     CK(cudaStreamCreateWithFlags(&g.stream, cudaStreamNonBlocking));
     CK(setup_stage_euler64(o));
     CK(setup_stage_euler32(o));
+    CK(setup_stage_mhd64());
+    CK(setup_stage_mhd32());
     CK(cudaMalloc(&g.ctrl, sizeof(Control)));
     CK(cudaMemset(g.ctrl, 0, sizeof(Control)));
     CK(cudaMalloc(&g.tot, 16 * sizeof(double)));
@@ -485,6 +503,9 @@ int nemo_gpu_set_mesh(int64_t nelems, const double* delta, const double* center,
     Control c{};
     c.ngroups = 1;
     c.dt_factor = 0.25 * g.cfg.cfl / (double)(2 * NN - 1);
+    c.glm_ch = g.cfg.glm_ch;
+    c.glm_alpha = g.cfg.glm_alpha;
+    c.mhd = is_mhd() ? 1 : 0;
     CK(cudaMemcpy(g.ctrl, &c, sizeof c, cudaMemcpyHostToDevice));
     g.has_mesh = true;
     return NEMO_OK;
@@ -522,6 +543,9 @@ int nemo_gpu_upload_state(const double* host, int64_t stride) {
     Control c{};
     c.ngroups = g.ngroups;
     c.dt_factor = 0.25 * g.cfg.cfl / (double)(2 * NN - 1);
+    c.glm_ch = g.cfg.glm_ch;
+    c.glm_alpha = g.cfg.glm_alpha;
+    c.mhd = is_mhd() ? 1 : 0;
     CK(cudaMemcpyAsync(g.ctrl, &c, sizeof c, cudaMemcpyHostToDevice, g.stream));
     CK(cudaStreamSynchronize(g.stream));
     g.has_state = true;
@@ -557,6 +581,16 @@ int nemo_gpu_calc_timestep(double cfl, double* dt_out, double* lmax_out) {
     std::memcpy(&lmax, &bits[1], 8);
     const double dt = 0.25 * cfl / (double)(2 * NN - 1) * dtmin;
     if (!std::isfinite(dt) || !(dt > 0.0)) return fail(NEMO_ERR_NONFINITE, "time step %g is not positive and finite", dt);
+    if (is_mhd()) {  // GLM cleaning speed and damping for the coming step (kernel_timestep_mod.f90:338-344)
+        unsigned long long vb = 0;
+        CK(cudaMemcpy(&vb, &g.ctrl->vmax_bits, 8, cudaMemcpyDeviceToHost));
+        double vmax;
+        std::memcpy(&vmax, &vb, 8);
+        const double gch = 2.0 * std::fabs(lmax - vmax);
+        const double gal = gch / 0.18;
+        CK(cudaMemcpy(&g.ctrl->glm_ch, &gch, 8, cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(&g.ctrl->glm_alpha, &gal, 8, cudaMemcpyHostToDevice));
+    }
     if (dt_out) *dt_out = dt;
     if (lmax_out) *lmax_out = lmax;
     g.prepared = true;

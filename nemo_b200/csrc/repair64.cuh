@@ -3,6 +3,7 @@
 
 #include "common.cuh"
 #include "euler_fp64.cuh"
+#include "mhd_phys.cuh"
 
 namespace nemo {
 
@@ -59,6 +60,73 @@ __device__ __noinline__ bool repair_elem(double* su, int el, const OpConsts& k) 
                             for (int v = 0; v < V; ++v) tiles[t][v] = means[v] + squeeze * hiles[t][v];
                         bool tv2 = true;
                         for (int t = 0; t < 8; ++t) tv2 = tv2 && isvalid64(tiles[t], k);
+                        if (tv2) break;
+                    }
+                    for (int v = 0; v < V; ++v)
+                        for (int kx = 2 * r * nn; kx < (2 * r + 2) * nn; ++kx)
+                            for (int jx = 2 * pp * nn; jx < (2 * pp + 2) * nn; ++jx)
+                                for (int ix = 2 * q * nn; ix < (2 * q + 2) * nn; ++ix) {
+                                    int p = nidx(ix, jx, kx);
+                                    at(v, p) = means[v] + squeeze * (at(v, p) - means[v]);
+                                }
+                }
+    }
+    ok = true;
+    for (int p = 0; p < NP; ++p) ok = ok && node_ok(p);
+    return ok;
+}
+
+
+// The same repair for the 9 GLM-MHD variables (MHD pressure in the admissibility check).
+template <int EPC>
+__device__ __noinline__ bool repair_elem_mhd(double* su, int el, const OpConsts& k) {
+    constexpr int V = 9;
+    auto at = [&](int v, int p) -> double& { return su[(v * EPC + el) * NP + p]; };
+    auto node_ok = [&](int p) {
+        double q[9];
+        for (int v = 0; v < V; ++v) q[v] = at(v, p);
+        return m_isvalid(q, k.kappa, k.mu0);
+    };
+    bool ok = true;
+    for (int p = 0; p < NP; ++p) ok = ok && node_ok(p);
+    if (ok) return true;
+    for (int level = 1; level <= 2; ++level) {
+        int mm = 1 << (level - 1), nn = 1 << (2 - level);
+        double ws = 1.0 / (double)(nn * nn * nn);
+        for (int r = 0; r < mm; ++r)
+            for (int pp = 0; pp < mm; ++pp)
+                for (int q = 0; q < mm; ++q) {
+                    double tiles[8][V], means[V];
+                    for (int t = 0; t < 8; ++t)
+                        for (int v = 0; v < V; ++v) tiles[t][v] = 0.0;
+                    for (int v = 0; v < V; ++v)
+                        for (int kk = 0; kk < 2; ++kk)
+                            for (int jj = 0; jj < 2; ++jj)
+                                for (int ii = 0; ii < 2; ++ii)
+                                    for (int kx = (2 * r + kk) * nn; kx < (2 * r + kk + 1) * nn; ++kx)
+                                        for (int jx = (2 * pp + jj) * nn; jx < (2 * pp + jj + 1) * nn; ++jx)
+                                            for (int ix = (2 * q + ii) * nn; ix < (2 * q + ii + 1) * nn; ++ix) {
+                                                int t = ii + 2 * (jj + 2 * kk);
+                                                tiles[t][v] = tiles[t][v] + ws * at(v, nidx(ix, jx, kx));
+                                            }
+                    bool tv = true;
+                    for (int t = 0; t < 8; ++t) tv = tv && m_isvalid(tiles[t], k.kappa, k.mu0);
+                    if (tv) continue;
+                    for (int v = 0; v < V; ++v) {
+                        double s = 0.0;
+                        for (int t = 0; t < 8; ++t) s = s + tiles[t][v];
+                        means[v] = 0.125 * s;
+                    }
+                    double hiles[8][V];
+                    for (int t = 0; t < 8; ++t)
+                        for (int v = 0; v < V; ++v) hiles[t][v] = tiles[t][v] - means[v];
+                    double squeeze = 1.0;
+                    while (squeeze > 0.0) {
+                        squeeze = fmax(0.0, squeeze - k.repair_decr);
+                        for (int t = 0; t < 8; ++t)
+                            for (int v = 0; v < V; ++v) tiles[t][v] = means[v] + squeeze * hiles[t][v];
+                        bool tv2 = true;
+                        for (int t = 0; t < 8; ++t) tv2 = tv2 && m_isvalid(tiles[t], k.kappa, k.mu0);
                         if (tv2) break;
                     }
                     for (int v = 0; v < V; ++v)

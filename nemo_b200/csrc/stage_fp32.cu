@@ -755,4 +755,36 @@ cudaError_t setup_stage_euler32(const OpConsts& ops) {
     return cudaMemcpyToSymbol(c_ops32, &ops, sizeof(OpConsts));
 }
 
+
+// ---- GLM-MHD stage (float flux arithmetic)
+#define NEMO_MHD_OPS c_ops32
+}  // namespace nemo
+#include "stage_mhd.cuh"
+namespace nemo {
+#undef NEMO_MHD_OPS
+
+int stage_smem_bytes_mhd32() { return mhd::V * mhd::EPC * NP * (int)(sizeof(double) + sizeof(float)); }
+
+cudaError_t setup_stage_mhd32() {
+    const int smem = stage_smem_bytes_mhd32();
+    cudaError_t err;
+    if ((err = cudaFuncSetAttribute(k_stage_mhd<float, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem))) return err;
+    if ((err = cudaFuncSetAttribute(k_stage_mhd<float, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem))) return err;
+    if ((err = cudaFuncSetAttribute(k_stage_mhd<float, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem))) return err;
+    return cudaFuncSetAttribute(k_stage_mhd<float, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+}
+
+cudaError_t launch_stage_mhd32(const StageArgs& a, bool blend, bool rhs_only, cudaStream_t s) {
+    const int grid = (int)((a.E + mhd::EPC - 1) / mhd::EPC);
+    const int smem = stage_smem_bytes_mhd32();
+    if (rhs_only) {
+        if (blend) k_stage_mhd<float, true, true><<<grid, mhd::NT, smem, s>>>(a);
+        else k_stage_mhd<float, false, true><<<grid, mhd::NT, smem, s>>>(a);
+    } else {
+        if (blend) k_stage_mhd<float, true, false><<<grid, mhd::NT, smem, s>>>(a);
+        else k_stage_mhd<float, false, false><<<grid, mhd::NT, smem, s>>>(a);
+    }
+    return cudaGetLastError();
+}
+
 }  // namespace nemo

@@ -614,4 +614,36 @@ cudaError_t launch_totals64(const double* u, const double* delta, int64_t E, int
     return cudaGetLastError();
 }
 
+
+// ---- GLM-MHD stage (double flux arithmetic)
+#define NEMO_MHD_OPS c_ops64
+}  // namespace nemo
+#include "stage_mhd.cuh"
+namespace nemo {
+#undef NEMO_MHD_OPS
+
+int stage_smem_bytes_mhd64() { return mhd::V * mhd::EPC * NP * (int)(sizeof(double) + sizeof(double)); }
+
+cudaError_t setup_stage_mhd64() {
+    const int smem = stage_smem_bytes_mhd64();
+    cudaError_t err;
+    if ((err = cudaFuncSetAttribute(k_stage_mhd<double, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem))) return err;
+    if ((err = cudaFuncSetAttribute(k_stage_mhd<double, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem))) return err;
+    if ((err = cudaFuncSetAttribute(k_stage_mhd<double, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem))) return err;
+    return cudaFuncSetAttribute(k_stage_mhd<double, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+}
+
+cudaError_t launch_stage_mhd64(const StageArgs& a, bool blend, bool rhs_only, cudaStream_t s) {
+    const int grid = (int)((a.E + mhd::EPC - 1) / mhd::EPC);
+    const int smem = stage_smem_bytes_mhd64();
+    if (rhs_only) {
+        if (blend) k_stage_mhd<double, true, true><<<grid, mhd::NT, smem, s>>>(a);
+        else k_stage_mhd<double, false, true><<<grid, mhd::NT, smem, s>>>(a);
+    } else {
+        if (blend) k_stage_mhd<double, true, false><<<grid, mhd::NT, smem, s>>>(a);
+        else k_stage_mhd<double, false, false><<<grid, mhd::NT, smem, s>>>(a);
+    }
+    return cudaGetLastError();
+}
+
 }  // namespace nemo

@@ -1,0 +1,525 @@
+// stage_mhd.cuh -- fused LSRK stage for GLM-MHD (9 variables), templated on the flux arithmetic.
+//
+// Included by stage_fp64.cu (R = double, -fmad=false: bit-identical to the oracle) and by
+// stage_fp32.cu (R = float, fast math; state, register, update, repair and reductions stay FP64).
+// One CTA = 8 elements, 16 threads per element; thread (a,b) owns the x-, y- and z-lines through
+// (a,b) and adds its direction terms into one shared rhs array (x, then y, then z), which keeps the
+// oracle's summation order.  Per line: surface flux (Rusanov) + the element's own-side
+// non-conservative Powell/GLM term at both ends, 6 node pairs of EC flux (Derigs) + non-conservative
+// term in flux-differencing form, the lift, and (alpha > 0) FV subcells with the same interface
+// terms; then the GLM damping -glm_alpha psi, the RK register/state update (FP64) and the
+// positivity repair.  The epilogue computes the blending coefficient for the next stage (modal
+// indicator, or the learned one with the modal fallback) and, on the last stage, the CFL bound,
+// the maximum wave speed and the maximum velocity for the GLM cleaning speed.
+#pragma once
+
+#include "common.cuh"
+#include "kernels.h"
+#include "mhd_phys.cuh"
+#include "pmath64.cuh"
+#include "repair64.cuh"
+
+namespace nemo {
+namespace mhd {
+
+constexpr int EPC = 8;
+constexpr int NT = 128;
+constexpr int V = 9;
+
+__device__ __forceinline__ unsigned su32(const void* p) { return static_cast<unsigned>(__cvta_generic_to_shared(p)); }
+
+__device__ __forceinline__ bool mbar_wait_m(uint64_t* bar, unsigned phase) {
+    const unsigned addr = su32(bar);
+    for (int it = 0; it < (1 << 24); ++it) {
+        unsigned ok;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(ok) : "r"(addr), "r"(phase) : "memory");
+        if (ok) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ bool tile_load_m(double* su, const double* __restrict__ u, int64_t E, int64_t e0, int nel,
+                                            uint64_t* bar, Control* ctrl) {
+    if (threadIdx.x == 0) {
+        const unsigned b = su32(bar);
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(b) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const unsigned b = su32(bar);
+        const unsigned bytes = (unsigned)(nel * NP * 8);
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(b), "r"(bytes * V) : "memory");
+        for (int v = 0; v < V; ++v)
+            asm volatile(
+                "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                    su32(su + v * EPC * NP)),
+                "l"(u + ((int64_t)v * E + e0) * NP), "r"(bytes), "r"(b)
+                : "memory");
+    }
+    bool ok = mbar_wait_m(bar, 0);
+    if (!ok) {
+        atomicOr(&ctrl->error, 1);
+        mbar_wait_m(bar, 0);
+    }
+    return ok;
+}
+
+// rotated state of node n of element el (momentum and field cyclically into direction d)
+template <typename R>
+__device__ __forceinline__ void load_rot(const double* su, int el, int n, int d, R* r) {
+    r[0] = (R)su[(0 * EPC + el) * NP + n];
+    r[4] = (R)su[(4 * EPC + el) * NP + n];
+    r[8] = (R)su[(8 * EPC + el) * NP + n];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        r[1 + c] = (R)su[((1 + (d + c) % 3) * EPC + el) * NP + n];
+        r[5 + c] = (R)su[((5 + (d + c) % 3) * EPC + el) * NP + n];
+    }
+}
+
+template <typename R>
+__device__ __forceinline__ void load_rot_global(const double* __restrict__ g, int64_t E, int64_t ne, int n, int d, R* r) {
+    r[0] = (R)__ldg(g + ((int64_t)0 * E + ne) * NP + n);
+    r[4] = (R)__ldg(g + ((int64_t)4 * E + ne) * NP + n);
+    r[8] = (R)__ldg(g + ((int64_t)8 * E + ne) * NP + n);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        r[1 + c] = (R)__ldg(g + ((int64_t)(1 + (d + c) % 3) * E + ne) * NP + n);
+        r[5 + c] = (R)__ldg(g + ((int64_t)(5 + (d + c) % 3) * E + ne) * NP + n);
+    }
+}
+
+// variable index of rotated component c in direction d
+__device__ __forceinline__ int unrot(int d, int c) {
+    if (c == 0 || c == 4 || c == 8) return c;
+    if (c < 4) return 1 + (d + c - 1) % 3;
+    return 5 + (d + c - 5) % 3;
+}
+
+__device__ __forceinline__ double silu_m(double x) { return x / (1.0 + pexp64(-x)); }
+__device__ __forceinline__ float silu_m(float x) { return x / (1.0f + __expf(-x)); }
+__device__ __forceinline__ double expneg(double x) { return pexp64(x); }
+__device__ __forceinline__ float expneg(float x) { return __expf(x); }
+
+// Epilogue: modal (or learned) blending coefficient of the state in su and the CFL bound; sums in
+// the oracle's serial order (one thread per element), MLP layers over 32 threads per element.
+template <typename R>
+__device__ void epilogue_mhd(const StageArgs& a, const double* su, R* scr, unsigned long long (*s_lam)[3],
+                             unsigned long long* s_vmax, int nel, int64_t e0, int tid, const OpConsts& k) {
+    __shared__ R s_am[EPC];
+    __shared__ int s_fb[EPC];
+    Control* ctrl = a.ctrl;
+    const R kap = (R)k.kappa, mu0 = (R)k.mu0;
+    if (a.alpha_out) {
+        const R* W = nullptr;
+        if (sizeof(R) == 8) W = reinterpret_cast<const R*>(a.mlp64);
+        else W = reinterpret_cast<const R*>(a.mlp32);
+        const bool learned = W != nullptr;
+        R* q = scr;
+        R* t1 = scr + EPC * NP;
+        R* t2 = scr + 2 * EPC * NP;
+        const int nq = learned ? 3 : 1;
+        for (int w = 0; w < nq; ++w) {
+            R* cm = scr + (3 + w) * EPC * NP;
+            for (int p = tid; p < nel * NP; p += NT) {
+                const int pel = p / NP, n = p % NP;
+                R uu[V];
+#pragma unroll
+                for (int v = 0; v < V; ++v) uu[v] = (R)su[(v * EPC + pel) * NP + n];
+                const R pr = m_pressure(uu, kap, mu0);
+                q[pel * NP + n] = w == 0 ? uu[0] * pr : (w == 1 ? uu[0] : pr);
+            }
+            __syncthreads();
+            for (int p = tid; p < nel * NP; p += NT) {
+                const int pel = p / NP, n = p % NP;
+                const int ai = n % NN, j = (n / NN) % NN, kk = n / NF;
+                R s = R(0.0);
+#pragma unroll
+                for (int i = 0; i < NN; ++i) s = s + (R)k.Vinv[ai * NN + i] * q[pel * NP + nidx(i, j, kk)];
+                t1[pel * NP + n] = s;
+            }
+            __syncthreads();
+            for (int p = tid; p < nel * NP; p += NT) {
+                const int pel = p / NP, n = p % NP;
+                const int ai = n % NN, bj = (n / NN) % NN, kk = n / NF;
+                R s = R(0.0);
+#pragma unroll
+                for (int j = 0; j < NN; ++j) s = s + (R)k.Vinv[bj * NN + j] * t1[pel * NP + nidx(ai, j, kk)];
+                t2[pel * NP + n] = s;
+            }
+            __syncthreads();
+            for (int p = tid; p < nel * NP; p += NT) {
+                const int pel = p / NP, n = p % NP;
+                const int ai = n % NN, bj = (n / NN) % NN, cc = n / NF;
+                R s = R(0.0);
+#pragma unroll
+                for (int kk = 0; kk < NN; ++kk) s = s + (R)k.Vinv[cc * NN + kk] * t2[pel * NP + nidx(ai, bj, kk)];
+                cm[pel * NP + n] = s;
+            }
+            __syncthreads();
+        }
+        R* feat = q;
+        if (tid < nel) {
+            const R* m = scr + 3 * EPC * NP + tid * NP;
+            R total = R(0.0), clip1 = R(0.0), clip2 = R(0.0);
+            for (int cc = 0; cc < NN; ++cc)
+                for (int bj = 0; bj < NN; ++bj)
+                    for (int ai = 0; ai < NN; ++ai) {
+                        const R mv = m[nidx(ai, bj, cc)];
+                        const R e2 = mv * mv;
+                        total = total + e2;
+                        if (ai < NN - 1 && bj < NN - 1 && cc < NN - 1) clip1 = clip1 + e2;
+                        if (ai < NN - 2 && bj < NN - 2 && cc < NN - 2) clip2 = clip2 + e2;
+                    }
+            const R e1 = (total - clip1) / total;
+            const R e2 = (clip1 - clip2) / clip1;
+            const R energy = fmax(e1, e2);
+            R al = R(1.0) / (R(1.0) + expneg((R)k.ind_k * (energy - (R)k.ind_T)));
+            if (al < (R)k.alpha_min) al = R(0.0);
+            else if (al > (R)k.one_m_alpha_min) al = R(1.0);
+            s_am[tid] = fmin((R)k.alpha_max, al);
+            int fb = 0;
+            if (learned) {
+                R rs = R(0.0), ps = R(0.0), rmin = R(1e30), pmin = R(1e30);
+                for (int n = 0; n < NP; ++n) {
+                    R uu[V];
+#pragma unroll
+                    for (int v = 0; v < V; ++v) uu[v] = (R)su[(v * EPC + tid) * NP + n];
+                    const R pr = m_pressure(uu, kap, mu0);
+                    rs = rs + uu[0];
+                    ps = ps + pr;
+                    rmin = fmin(rmin, uu[0]);
+                    pmin = fmin(pmin, pr);
+                }
+                if (rmin < R(0.1) * (rs / R(64.0)) || pmin < R(0.1) * (ps / R(64.0))) fb = 1;
+                for (int w = 0; w < 2; ++w) {
+                    const R* mw = scr + (4 + w) * EPC * NP + tid * NP;
+                    R tot = R(0.0), Eo[6] = {R(0), R(0), R(0), R(0), R(0), R(0)};
+                    for (int cc = 0; cc < NN; ++cc)
+                        for (int bj = 0; bj < NN; ++bj)
+                            for (int ai = 0; ai < NN; ++ai) {
+                                const R mv = mw[nidx(ai, bj, cc)];
+                                const R ee = mv * mv;
+                                tot = tot + ee;
+                                const int ord[3] = {ai, bj, cc};
+#pragma unroll
+                                for (int d = 0; d < 3; ++d) {
+                                    if (ord[d] == NN - 1) Eo[2 * d] = Eo[2 * d] + ee;
+                                    if (ord[d] == NN - 2) Eo[2 * d + 1] = Eo[2 * d + 1] + ee;
+                                }
+                            }
+                    for (int i = 0; i < 6; ++i) {
+                        const R f = mlog(Eo[i] / tot + R(1e-12));
+                        feat[tid * 12 + 6 * w + i] = f;
+                        const R x = f / R(10.0) + R(1.0);
+                        if (x < W[MLP_NW + 6 * w + i] || x > W[MLP_NW + 12 + 6 * w + i]) fb = 1;
+                    }
+                }
+            }
+            s_fb[tid] = fb;
+        }
+        __syncthreads();
+        if (learned) {
+            const R* W1 = W;
+            const R* b1 = W1 + 32 * 12;
+            const R* W2 = b1 + 32;
+            const R* b2 = W2 + 32 * 32;
+            const R* W3 = b2 + 32;
+            R* h1 = t1;
+            R* h2 = t2;
+            for (int p = tid; p < nel * 32; p += NT) {
+                const int pel = p / 32, j = p % 32;
+                R s = b1[j];
+                for (int i = 0; i < 12; ++i) s = s + W1[j * 12 + i] * (feat[pel * 12 + i] / R(10.0) + R(1.0));
+                h1[pel * 32 + j] = silu_m(s);
+            }
+            __syncthreads();
+            for (int p = tid; p < nel * 32; p += NT) {
+                const int pel = p / 32, j = p % 32;
+                R s = b2[j];
+                for (int i = 0; i < 32; ++i) s = s + W2[j * 32 + i] * h1[pel * 32 + i];
+                h2[pel * 32 + j] = silu_m(s);
+            }
+            __syncthreads();
+            if (tid < nel) {
+                R z = W3[32];
+                for (int j = 0; j < 32; ++j) z = z + W3[j] * h2[tid * 32 + j];
+                R al = (R)k.alpha_max / (R(1.0) + expneg(-z));
+                if (al < (R)k.alpha_min) al = R(0.0);
+                const R am = s_am[tid];
+                if (s_fb[tid]) {
+                    atomicAdd(&ctrl->fallback, 1ull);
+                    al = am;
+                } else {
+                    atomicAdd(&ctrl->judge_sum, (double)fabs(al - am));
+                    atomicAdd(&ctrl->judge_n, 1ull);
+                }
+                a.alpha_out[e0 + tid] = (double)al;
+            }
+        } else if (tid < nel) {
+            a.alpha_out[e0 + tid] = (double)s_am[tid];
+        }
+    }
+    if (a.epi_dt) {
+        for (int p = tid; p < nel * NP; p += NT) {
+            const int pel = p / NP, n = p % NP;
+            double uu[V];
+#pragma unroll
+            for (int v = 0; v < V; ++v) uu[v] = su[(v * EPC + pel) * NP + n];
+            double rr[V];
+#pragma unroll
+            for (int dd = 0; dd < 3; ++dd) {
+                rr[0] = uu[0];
+                rr[4] = uu[4];
+                rr[8] = uu[8];
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    rr[1 + c] = uu[1 + (dd + c) % 3];
+                    rr[5 + c] = uu[5 + (dd + c) % 3];
+                }
+                const double lam = m_xlambda(rr, k.kappa, k.mu0);
+                atomicMax(&s_lam[pel][dd], (unsigned long long)__double_as_longlong(lam));
+            }
+            const double vm = fmax(fmax(fabs(uu[1] / uu[0]), fabs(uu[2] / uu[0])), fabs(uu[3] / uu[0]));
+            atomicMax(s_vmax, (unsigned long long)__double_as_longlong(vm));
+        }
+        __syncthreads();
+        if (tid < nel) {
+            const int64_t pe = e0 + tid;
+            const double lf = __longlong_as_double((long long)s_lam[tid][0]);
+            const double lg = __longlong_as_double((long long)s_lam[tid][1]);
+            const double lh = __longlong_as_double((long long)s_lam[tid][2]);
+            const double dte = fmin(fmin(a.delta[pe * 3 + 0] / lf, a.delta[pe * 3 + 1] / lg), a.delta[pe * 3 + 2] / lh);
+            const int g = a.group ? a.group[pe] : 0;
+            atomicMin(&ctrl->dtmin_bits[g], (unsigned long long)__double_as_longlong(dte));
+            atomicMax(&ctrl->lmax_bits[g], (unsigned long long)__double_as_longlong(fmax(fmax(lf, lg), lh)));
+        }
+        if (tid == 0) atomicMax(&ctrl->vmax_bits, *s_vmax);
+    }
+}
+
+}  // namespace mhd
+
+template <typename R, bool BLEND, bool RHS_ONLY>
+__global__ void __launch_bounds__(mhd::NT, 1) k_stage_mhd(StageArgs a) {
+    constexpr int MEPC = mhd::EPC, MV = mhd::V;
+    using mhd::load_rot;
+    using mhd::load_rot_global;
+    using mhd::unrot;
+    extern __shared__ __align__(128) double smem_m[];
+    double* su = smem_m;                                    // [9][MEPC][64] FP64 state
+    R* sR = reinterpret_cast<R*>(su + MV * MEPC * NP);        // [9][MEPC][64] rhs terms
+    __shared__ uint64_t bar;
+    __shared__ R s_alpha[MEPC];
+    __shared__ int s_bad[MEPC];
+    __shared__ unsigned long long s_lam[MEPC][3];
+    __shared__ unsigned long long s_vmax;
+
+    const OpConsts& k = NEMO_MHD_OPS;
+    Control* ctrl = a.ctrl;
+    if (!RHS_ONLY && !a.prep_only && ctrl->done) return;
+    const int tid = threadIdx.x;
+    const int64_t E = a.E;
+    const int64_t e0 = (int64_t)blockIdx.x * MEPC;
+    const int nel = (int)min((int64_t)MEPC, E - e0);
+    const R kap = (R)k.kappa, mu0 = (R)k.mu0;
+    const R ch = (R)ctrl->glm_ch;
+
+    if (tid < MEPC) {
+        s_bad[tid] = 0;
+        s_lam[tid][0] = s_lam[tid][1] = s_lam[tid][2] = 0ull;
+        R al = R(0.0);
+        if (BLEND && tid < nel) {
+            const int64_t e = e0 + tid;
+            double ad = a.alpha_in[e];
+            if (a.smooth)
+                for (int f = 0; f < 6; ++f) {
+                    const int32_t ne = a.nbr[e * 6 + f];
+                    if (ne >= 0) ad = fmax(ad, 0.5 * a.alpha_in[ne]);
+                }
+            if (a.alpha_used) a.alpha_used[e] = ad;
+            al = (R)ad;
+        }
+        s_alpha[tid] = al;
+    }
+    if (tid == 0) s_vmax = 0ull;
+    if (!mhd::tile_load_m(su, a.u_in, E, e0, nel, &bar, ctrl)) return;
+    if (a.prep_only) {
+        mhd::epilogue_mhd<R>(a, su, sR, s_lam, &s_vmax, nel, e0, tid, k);
+        return;
+    }
+
+    const int el = tid >> 4, ab = tid & 15, la = ab & 3, lb = ab >> 2;
+    const bool active = el < nel;
+    const int64_t e = e0 + el;
+    for (int d = 0; d < 3; ++d) {
+        if (active) {
+            int idx[NN];
+#pragma unroll
+            for (int i = 0; i < NN; ++i) idx[i] = line_node(d, la, lb, i);
+            // ---- surface flux + own-side non-conservative term at both ends
+            R Fs[2][MV];
+#pragma unroll
+            for (int side = 0; side < 2; ++side) {
+                const int f = 2 * d + side;
+                R uo[MV], un[MV], F[MV], G[MV];
+                load_rot(su, el, idx[side ? NN - 1 : 0], d, uo);
+                const int32_t ne = a.nbr[e * 6 + f];
+                if (ne >= 0) {
+                    const int nn = line_node(d, la, lb, side ? 0 : NN - 1);
+                    const int64_t nl = (int64_t)ne - e0;
+                    if (nl >= 0 && nl < nel) load_rot(su, (int)nl, nn, d, un);
+                    else load_rot_global(a.u_in, E, ne, nn, d, un);
+                } else {
+#pragma unroll
+                    for (int v = 0; v < MV; ++v) un[v] = uo[v];
+                }
+                if (side) {
+                    m_rusanov_x(uo, un, F, kap, mu0, ch);
+                    m_nc_x(uo, uo, un, G, mu0);
+                } else {
+                    m_rusanov_x(un, uo, F, kap, mu0, ch);
+                    m_nc_x(uo, un, uo, G, mu0);
+                }
+#pragma unroll
+                for (int v = 0; v < MV; ++v) Fs[side][v] = F[v] + G[v];
+            }
+            // ---- volume: EC flux + non-conservative term, 6 pairs in the oracle's order
+            R t[NN][MV];
+#pragma unroll
+            for (int i = 0; i < NN; ++i)
+#pragma unroll
+                for (int v = 0; v < MV; ++v) t[i][v] = R(0.0);
+#pragma unroll
+            for (int i = 0; i < NN - 1; ++i)
+#pragma unroll
+                for (int m = i + 1; m < NN; ++m) {
+                    R ui[MV], um[MV], F[MV], Gi[MV], Gm[MV];
+                    load_rot(su, el, idx[i], d, ui);
+                    load_rot(su, el, idx[m], d, um);
+                    if (a.volume_flux == NEMO_VOLFLUX_CENTRAL) m_central_x(ui, um, F, kap, mu0, ch);
+                    else m_ec_x(ui, um, F, kap, mu0, ch);
+                    m_nc_x(ui, ui, um, Gi, mu0);
+                    m_nc_x(um, ui, um, Gm, mu0);
+                    const R sim = (R)k.S[i * NN + m], smi = (R)k.S[m * NN + i];
+#pragma unroll
+                    for (int v = 0; v < MV; ++v) {
+                        t[i][v] = t[i][v] + sim * (F[v] + Gi[v]);
+                        t[m][v] = t[m][v] + smi * (F[v] + Gm[v]);
+                    }
+                }
+            // ---- lift
+#pragma unroll
+            for (int v = 0; v < MV; ++v) {
+                t[0][v] = t[0][v] + (R)k.winv[0] * (-Fs[0][v]);
+                t[NN - 1][v] = t[NN - 1][v] + (R)k.winv[NN - 1] * Fs[1][v];
+            }
+            // ---- FV subcells and blend
+            if (BLEND) {
+                const R al = s_alpha[el];
+                if (al > R(0.0)) {
+                    R Fh[MV];   // Riemann flux of the interface to the left of node i (i > 0)
+#pragma unroll
+                    for (int i = 0; i < NN; ++i) {
+                        R ui[MV], FR[MV], FL[MV], G[MV];
+                        load_rot(su, el, idx[i], d, ui);
+                        if (i > 0) {
+                            R ul[MV];
+                            load_rot(su, el, idx[i - 1], d, ul);
+                            m_nc_x(ui, ul, ui, G, mu0);
+#pragma unroll
+                            for (int v = 0; v < MV; ++v) FL[v] = Fh[v] + G[v];
+                        } else {
+#pragma unroll
+                            for (int v = 0; v < MV; ++v) FL[v] = Fs[0][v];
+                        }
+                        if (i < NN - 1) {
+                            R ur[MV];
+                            load_rot(su, el, idx[i + 1], d, ur);
+                            m_rusanov_x(ui, ur, Fh, kap, mu0, ch);
+                            m_nc_x(ui, ui, ur, G, mu0);
+#pragma unroll
+                            for (int v = 0; v < MV; ++v) FR[v] = Fh[v] + G[v];
+                        } else {
+#pragma unroll
+                            for (int v = 0; v < MV; ++v) FR[v] = Fs[1][v];
+                        }
+                        const R wi = (R)k.winv[i];
+#pragma unroll
+                        for (int v = 0; v < MV; ++v) t[i][v] = (R(1.0) - al) * t[i][v] + al * (wi * (FR[v] - FL[v]));
+                    }
+                }
+            }
+            // ---- accumulate c_d * t (x writes, y and z add)
+            const R cd = (R)a.cdel[e * 3 + d];
+#pragma unroll
+            for (int i = 0; i < NN; ++i)
+#pragma unroll
+                for (int c = 0; c < MV; ++c) {
+                    R& Rv = sR[(unrot(d, c) * MEPC + el) * NP + idx[i]];
+                    Rv = (d == 0 ? cd * t[i][c] : Rv + cd * t[i][c]);
+                }
+        }
+        __syncthreads();
+    }
+
+    // ---- FP64 register/state update and GLM damping
+    const int st = a.stage;
+    const double A = rk_a(st);
+    const double cdt = rk_c(st) * ctrl->dt[0];
+    const double galpha = ctrl->glm_alpha;
+    if (active) {
+        bool ok = true;
+#pragma unroll
+        for (int i = 0; i < NN; ++i) {
+            const int n = nidx(i, la, lb);
+            double uu[MV];
+#pragma unroll
+            for (int v = 0; v < MV; ++v) {
+                const int s = (v * MEPC + el) * NP + n;
+                double rhs = -(double)sR[s];
+                if (v == 8) rhs = rhs - galpha * su[s];
+                const int64_t g = ((int64_t)v * E + e) * NP + n;
+                if (RHS_ONLY) {
+                    a.rhs_out[g] = rhs;
+                } else {
+                    const double r2 = st == 0 ? rhs : A * a.reg[g] + rhs;
+                    a.reg[g] = r2;
+                    su[s] = su[s] + cdt * r2;
+                }
+                uu[v] = su[s];
+            }
+            if (!RHS_ONLY && a.positivity) ok = ok && m_isvalid(uu, k.kappa, k.mu0);
+        }
+        if (!ok) s_bad[el] = 1;
+    }
+    if (RHS_ONLY) return;
+    __syncthreads();
+    if (a.positivity && active && ab == 0 && s_bad[el]) {
+        if (!repair_elem_mhd<mhd::EPC>(su, el, k)) atomicAdd(&ctrl->nbad, 1ull);
+    }
+    __syncthreads();
+    if (active) {
+#pragma unroll
+        for (int v = 0; v < MV; ++v)
+#pragma unroll
+            for (int i = 0; i < NN; ++i) {
+                const int n = nidx(i, la, lb);
+                a.u_out[((int64_t)v * E + e) * NP + n] = su[(v * MEPC + el) * NP + n];
+            }
+    }
+    if (st == 4 && blockIdx.x == 0 && tid == 0) {
+        for (int g = 0; g < ctrl->ngroups; ++g) ctrl->t[g] = ctrl->t[g] + ctrl->dt[g];
+        ctrl->steps += 1;
+    }
+    __syncthreads();
+    mhd::epilogue_mhd<R>(a, su, sR, s_lam, &s_vmax, nel, e0, tid, k);
+}
+
+}  // namespace nemo

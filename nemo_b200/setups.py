@@ -83,3 +83,41 @@ def smooth_random(m, seed=0, kappa=1.4, nodes=LGL4, amp=0.2):
     vx, vy, vz = 0.5 * wave(1), -0.4 * wave(2), 0.3 * wave(3)
     p = 1.0 + amp * wave(4)
     return np.ascontiguousarray(prim2cons(rho, vx, vy, vz, p, kappa))
+
+
+def mhd_prim2cons(rho, vx, vy, vz, p, bx, by, bz, psi, kappa, mu0=1.0):
+    """Primitive -> conserved GLM-MHD variables (rho, m, E, B, psi) with
+    E = p/(kappa-1) + rho v^2/2 + (B^2 + psi^2)/(2 mu0) (source/setups/mhd/3d/orszag-tang/setup_init_mod.f90)."""
+    ener = p / (kappa - 1.0) + 0.5 * rho * (vx ** 2 + vy ** 2 + vz ** 2) + 0.5 / mu0 * (bx ** 2 + by ** 2 + bz ** 2) \
+        + 0.5 / mu0 * psi ** 2
+    return np.stack([rho, rho * vx, rho * vy, rho * vz, ener, bx, by, bz, psi])
+
+
+def orszag_tang(m, kappa=5.0 / 3.0, eps=0.2, b0=1.0 / np.sqrt(4.0 * np.pi), nodes=LGL4):
+    """3D Orszag-Tang-type vortex on the periodic unit box: rho = 25/(36 pi), p = 5/(12 pi),
+    v = (-(1 + eps sin 2 pi z) sin 2 pi y, (1 + eps sin 2 pi z) sin 2 pi x, eps sin 2 pi z),
+    B = b0 (-sin 2 pi y, sin 4 pi x, 0), psi = 0, mu0 = 1 (the velocity and field pattern of
+    source/setups/mhd/3d/orszag-tang/setup_init_mod.f90 with the classic density/pressure/b0)."""
+    x, y, z = m.node_coords(nodes)
+    tp = 2.0 * np.pi
+    rho = np.full_like(x, 25.0 / (36.0 * np.pi))
+    p = np.full_like(x, 5.0 / (12.0 * np.pi))
+    fz = 1.0 + eps * np.sin(tp * z)
+    vx, vy, vz = -fz * np.sin(tp * y), fz * np.sin(tp * x), eps * np.sin(tp * z)
+    bx, by, bz = -b0 * np.sin(tp * y), b0 * np.sin(2 * tp * x), np.zeros_like(x)
+    return np.ascontiguousarray(mhd_prim2cons(rho, vx, vy, vz, p, bx, by, bz, np.zeros_like(x), kappa))
+
+
+def divergence_b(m, u, dmat, weights):
+    """Discrete div B on the Gauss-Lobatto nodes (D applied along each direction, 2/delta scaling):
+    returns (L2 norm over the domain, max |div B|)."""
+    E = m.E
+    n = dmat.shape[0]
+    B = u[5:8].reshape(3, E, n, n, n)  # [c][e][k][j][i]
+    div = np.einsum("im,ekjm->ekji", dmat, B[0]) * (2.0 / m.delta[:, 0])[:, None, None, None]
+    div += np.einsum("jm,ekmi->ekji", dmat, B[1]) * (2.0 / m.delta[:, 1])[:, None, None, None]
+    div += np.einsum("km,emji->ekji", dmat, B[2]) * (2.0 / m.delta[:, 2])[:, None, None, None]
+    w3 = np.einsum("k,j,i->kji", weights, weights, weights) / 8.0
+    vol = np.prod(m.delta, axis=1)[:, None, None, None]
+    l2 = float(np.sqrt(np.sum(w3[None] * vol * div ** 2)))
+    return l2, float(np.max(np.abs(div)))

@@ -396,6 +396,192 @@ void e_twopoint(int kind, int d, const double* u, const double* v, double* F, do
 }
 
 // ------------------------------------------------------------------------------------------
+// GLM-MHD physics (source/equations/mhd/equations_mod.f90), variables
+// rho, m_x, m_y, m_z, E, B_x, B_y, B_z, psi (source/equations/mhd/equations_const_mod.f90:7-29)
+
+struct MhdPar {
+    double kappa, mu0, ch;
+};
+
+// pressure_elemental, equations_mod.f90:223-234
+inline double m_pressure(const double* u, const MhdPar& P) {
+    return (P.kappa - 1.0) * (u[4] - 0.5 / u[0] * (u[1] * u[1] + u[2] * u[2] + u[3] * u[3]) -
+                              0.5 / P.mu0 * (u[5] * u[5] + u[6] * u[6] + u[7] * u[7] + u[8] * u[8]));
+}
+
+// xflux, equations_mod.f90:64-139
+void m_xflux(const double* U, double* f, const MhdPar& P) {
+    const double smu_0 = 1.0 / P.mu0, s2mu_0 = 0.5 / P.mu0;
+    const double kappaM1 = P.kappa - 1.0, kappaM2 = P.kappa - 2.0;
+    const double Etotal = U[4] - 0.5 * smu_0 * (U[8] * U[8]);
+    const double srho = 1.0 / U[0];
+    const double v1 = U[1] * srho, v2 = U[2] * srho, v3 = U[3] * srho;
+    const double v_2 = v1 * v1 + v2 * v2 + v3 * v3;
+    const double bb2 = U[5] * U[5] + U[6] * U[6] + U[7] * U[7];
+    const double vb = U[5] * v1 + U[6] * v2 + U[7] * v3;
+    const double pt = kappaM1 * (Etotal - 0.5 * U[0] * v_2) - kappaM2 * s2mu_0 * bb2;
+    const double Ep = Etotal + pt;
+    f[0] = U[1];
+    f[1] = U[1] * v1 + pt - smu_0 * U[5] * U[5];
+    f[2] = U[1] * v2 - smu_0 * U[5] * U[6];
+    f[3] = U[1] * v3 - smu_0 * U[5] * U[7];
+    f[4] = Ep * v1 - smu_0 * U[5] * vb;
+    f[5] = 0.0;
+    f[6] = v1 * U[6] - U[5] * v2;
+    f[7] = v1 * U[7] - U[5] * v3;
+    f[4] = f[4] + smu_0 * P.ch * U[5] * U[8];
+    f[5] = f[5] + P.ch * U[8];
+    f[8] = P.ch * U[5];
+}
+
+// Fastest_Signal_Speed, equations_mod.f90:693-714; xlambdaMax :522-531
+inline double m_xlambda(const double* U, const MhdPar& P) {
+    const double pres = m_pressure(U, P);
+    const double cs2 = P.kappa * pres / U[0];
+    const double ca2 = U[5] * U[5] / U[0] / P.mu0;
+    const double va2 = (U[6] * U[6] + U[7] * U[7]) / U[0] / P.mu0 + ca2;
+    const double astar = std::sqrt((cs2 + va2) * (cs2 + va2) - 4.0 * cs2 * ca2);
+    const double c = std::sqrt(0.5 * (cs2 + va2 + astar));
+    return std::fabs(U[1] / U[0]) + c;
+}
+
+inline bool m_isvalid(const double* u, const MhdPar& P) { return (u[0] > 0.0) && (m_pressure(u, P) > 0.0); }
+
+// rotation of momentum and magnetic field into direction d (the reference's y/z wrappers)
+inline void m_rot_in(int d, const double* u, double* r) {
+    r[0] = u[0];
+    r[4] = u[4];
+    r[8] = u[8];
+    for (int c = 0; c < 3; ++c) {
+        r[1 + c] = u[1 + (d + c) % 3];
+        r[5 + c] = u[5 + (d + c) % 3];
+    }
+}
+inline void m_rot_out(int d, const double* r, double* f) {
+    f[0] = r[0];
+    f[4] = r[4];
+    f[8] = r[8];
+    for (int c = 0; c < 3; ++c) {
+        f[1 + (d + c) % 3] = r[1 + c];
+        f[5 + (d + c) % 3] = r[5 + c];
+    }
+}
+
+// Rusanov, source/equations/mhd/riemann/rusanov/riemann_mod.f90:7-24
+void m_rusanov_x(const double* uL, const double* uR, double* F, const MhdPar& P) {
+    double FL[9], FR[9];
+    m_xflux(uL, FL, P);
+    m_xflux(uR, FR, P);
+    const double lmax = std::max(m_xlambda(uL, P), m_xlambda(uR, P));
+    for (int v = 0; v < 9; ++v) F[v] = 0.5 * (FL[v] + FR[v] + lmax * (uL[v] - uR[v]));
+}
+
+// LN_MEAN with the relative switch, source/equations/mhd/two_point/ec/two_point_flux_mod.f90:203-219
+inline double ln_mean_rel(double aL, double aR) {
+    const double Xi = aR / aL;
+    const double u = (Xi * (Xi - 2.0) + 1.0) / (Xi * (Xi + 2.0) + 1.0);
+    if (u < 1.0e-4) return (aL + aR) * 52.5 / (105.0 + u * (35.0 + u * (21.0 + u * 15.0)));
+    return (aR - aL) / own_log(Xi);
+}
+
+// EC (Derigs) flux, source/equations/mhd/two_point/ec/two_point_flux_mod.f90:13-86
+void m_ec_x(const double* UL, const double* UR, double* F, const MhdPar& P) {
+    const double kappaM1 = P.kappa - 1.0, skappaM1 = 1.0 / (P.kappa - 1.0), smu_0 = 1.0 / P.mu0;
+    const double rho_L = UL[0], rho_R = UR[0];
+    const double E_L = UL[4] - 0.5 * smu_0 * (UL[8] * UL[8]), E_R = UR[4] - 0.5 * smu_0 * (UR[8] * UR[8]);
+    const double psi_L = UL[8], psi_R = UR[8];
+    double v_L[3], v_R[3];
+    for (int c = 0; c < 3; ++c) {
+        v_L[c] = UL[1 + c] / rho_L;
+        v_R[c] = UR[1 + c] / rho_R;
+    }
+    const double* B_L = UL + 5;
+    const double* B_R = UR + 5;
+    const double v2_L = v_L[0] * v_L[0] + v_L[1] * v_L[1] + v_L[2] * v_L[2];
+    const double v2_R = v_R[0] * v_R[0] + v_R[1] * v_R[1] + v_R[2] * v_R[2];
+    const double B2_L = B_L[0] * B_L[0] + B_L[1] * B_L[1] + B_L[2] * B_L[2];
+    const double B2_R = B_R[0] * B_R[0] + B_R[1] * B_R[1] + B_R[2] * B_R[2];
+    const double p_L = kappaM1 * (E_L - 0.5 * (rho_L * v2_L + smu_0 * B2_L));
+    const double p_R = kappaM1 * (E_R - 0.5 * (rho_R * v2_R + smu_0 * B2_R));
+    const double beta_L = 0.5 * rho_L / p_L, beta_R = 0.5 * rho_R / p_R;
+    const double rhoLN = ln_mean_rel(rho_L, rho_R);
+    const double betaLN = ln_mean_rel(beta_L, beta_R);
+    double vAvg[3], BAvg[3];
+    for (int c = 0; c < 3; ++c) {
+        vAvg[c] = 0.5 * (v_L[c] + v_R[c]);
+        BAvg[c] = 0.5 * (B_L[c] + B_R[c]);
+    }
+    const double v1_B2Avg = 0.5 * (v_L[0] * B2_L + v_R[0] * B2_R);
+    const double vB_Avg = 0.5 * ((v_L[0] * B_L[0] + v_L[1] * B_L[1] + v_L[2] * B_L[2]) +
+                                 (v_R[0] * B_R[0] + v_R[1] * B_R[1] + v_R[2] * B_R[2]));
+    const double pTilde = 0.5 * ((rho_L + rho_R) / (beta_L + beta_R) + smu_0 * 0.5 * (B2_L + B2_R));
+    const double psiAvg = 0.5 * (psi_L + psi_R);
+    F[0] = rhoLN * vAvg[0];
+    F[1] = F[0] * vAvg[0] - smu_0 * BAvg[0] * BAvg[0] + pTilde;
+    F[2] = F[0] * vAvg[1] - smu_0 * BAvg[0] * BAvg[1];
+    F[3] = F[0] * vAvg[2] - smu_0 * BAvg[0] * BAvg[2];
+    F[6] = vAvg[0] * BAvg[1] - BAvg[0] * vAvg[1];
+    F[7] = vAvg[0] * BAvg[2] - BAvg[0] * vAvg[2];
+    F[5] = P.ch * psiAvg;
+    F[8] = P.ch * BAvg[0];
+    const double s1 = vAvg[0] * F[1] + vAvg[1] * F[2] + vAvg[2] * F[3];
+    const double s2 = BAvg[0] * F[5] + BAvg[1] * F[6] + BAvg[2] * F[7];
+    F[4] = F[0] * 0.5 * (skappaM1 / betaLN - 0.5 * (v2_L + v2_R)) + s1 +
+           smu_0 * (s2 - 0.5 * v1_B2Avg + BAvg[0] * vB_Avg + F[8] * psiAvg -
+                    P.ch * 0.5 * (psi_L * B_L[0] + psi_R * B_R[0]));
+}
+
+// central flux 0.5 (f(u) + f(v)) for MHD
+void m_central_x(const double* u, const double* v, double* F, const MhdPar& P) {
+    double fu[9], fv[9];
+    m_xflux(u, fu, P);
+    m_xflux(v, fv, P);
+    for (int c = 0; c < 9; ++c) F[c] = 0.5 * (fu[c] + fv[c]);
+}
+
+// Non_Conservative_two_point_xFlux (Powell + GLM), source/equations/mhd/non_conservative_flux_mod.f90:10-45
+void m_nc_x(const double* UI, const double* UL, const double* UR, double* F, const MhdPar& P) {
+    const double Bavg = 0.5 * (UL[5] + UR[5]);
+    const double Gavg = 0.5 * (UL[8] + UR[8]);
+    const double v[3] = {UI[1] / UI[0], UI[2] / UI[0], UI[3] / UI[0]};
+    F[0] = 0.0;
+    for (int c = 0; c < 3; ++c) F[1 + c] = Bavg * UI[5 + c] / P.mu0;
+    F[4] = Bavg * (UI[5] * v[0] + UI[6] * v[1] + UI[7] * v[2]) / P.mu0;
+    for (int c = 0; c < 3; ++c) F[5 + c] = Bavg * v[c];
+    F[8] = 0.0;
+    const double gv = Gavg * v[0];
+    F[4] = F[4] + gv * (UI[8] / P.mu0);
+    F[8] = F[8] + gv * 1.0;
+}
+
+void m_riemann(int kind, int d, const double* uL, const double* uR, double* F, const MhdPar& P) {
+    double rL[9], rR[9], rF[9];
+    m_rot_in(d, uL, rL);
+    m_rot_in(d, uR, rR);
+    (void)kind;
+    m_rusanov_x(rL, rR, rF, P);
+    m_rot_out(d, rF, F);
+}
+
+void m_twopoint(int kind, int d, const double* u, const double* v, double* F, const MhdPar& P) {
+    double ru[9], rv[9], rF[9];
+    m_rot_in(d, u, ru);
+    m_rot_in(d, v, rv);
+    if (kind == NEMO_VOLFLUX_CENTRAL) m_central_x(ru, rv, rF, P);
+    else m_ec_x(ru, rv, rF, P);
+    m_rot_out(d, rF, F);
+}
+
+void m_nc(int d, const double* UI, const double* UL, const double* UR, double* F, const MhdPar& P) {
+    double rI[9], rL[9], rR[9], rF[9];
+    m_rot_in(d, UI, rI);
+    m_rot_in(d, UL, rL);
+    m_rot_in(d, UR, rR);
+    m_nc_x(rI, rL, rR, rF, P);
+    m_rot_out(d, rF, F);
+}
+
+// ------------------------------------------------------------------------------------------
 // Element operator
 
 inline int nidx(int i, int j, int k) { return i + NN * (j + NN * k); }
@@ -418,7 +604,17 @@ struct Ctx {
     Ops op;
     nemo_cfg cfg;
     int V;
+    bool mhd() const { return cfg.eqn == NEMO_EQN_MHD; }
+    MhdPar mp() const { return MhdPar{cfg.kappa, cfg.mu0, cfg.glm_ch}; }
 };
+
+// pressure and admissibility of either equation system
+inline double pressure_any(const Ctx& c, const double* u) {
+    return c.mhd() ? m_pressure(u, c.mp()) : e_pressure(u, c.cfg.kappa);
+}
+inline bool isvalid_any(const Ctx& c, const double* u) {
+    return c.mhd() ? m_isvalid(u, c.mp()) : e_isvalid(u, c.cfg.kappa);
+}
 
 void gather(const Ctx& c, int64_t E, const double* u, int64_t e, double (*ue)[VMAX]) {
     for (int v = 0; v < c.V; ++v)
@@ -429,7 +625,7 @@ void gather(const Ctx& c, int64_t E, const double* u, int64_t e, double (*ue)[VM
 double indicator_alpha(const Ctx& c, const double (*ue)[VMAX]) {
     const Ops& op = c.op;
     double q[NP], t1[NP], t2[NP], m[NP];
-    for (int p = 0; p < NP; ++p) q[p] = ue[p][0] * e_pressure(ue[p], c.cfg.kappa);
+    for (int p = 0; p < NP; ++p) q[p] = ue[p][0] * pressure_any(c, ue[p]);
     for (int k = 0; k < NN; ++k)
         for (int j = 0; j < NN; ++j)
             for (int a = 0; a < NN; ++a) {
@@ -505,7 +701,7 @@ void element_features(const Ctx& c, const double (*ue)[VMAX], double* feat) {
     double q[2][NP], m[NP];
     for (int p = 0; p < NP; ++p) {
         q[0][p] = ue[p][0];
-        q[1][p] = e_pressure(ue[p], c.cfg.kappa);
+        q[1][p] = pressure_any(c, ue[p]);
     }
     for (int w = 0; w < 2; ++w) {
         modal3(c.op, q[w], m);
@@ -543,7 +739,7 @@ inline double silu(double x) { return x / (1.0 + own_exp(-x)); }
 bool positivity_risk(const Ctx& c, const double (*ue)[VMAX]) {
     double rs = 0.0, ps = 0.0, rmin = HUGE_VAL, pmin = HUGE_VAL;
     for (int p = 0; p < NP; ++p) {
-        const double r = ue[p][0], pr = e_pressure(ue[p], c.cfg.kappa);
+        const double r = ue[p][0], pr = pressure_any(c, ue[p]);
         rs = rs + r;
         ps = ps + pr;
         rmin = std::min(rmin, r);
@@ -686,18 +882,124 @@ void element_rhs(const Ctx& c, const Mesh& M, const double* u, int64_t e, double
             }
 }
 
+// GLM-MHD element operator: EC volume flux plus the non-conservative Powell/GLM term in flux-
+// differencing form (node i takes S_im (f#(u_i,u_m) + Phi(u_i) avg(B_n, psi)), Bohm et al. 2018
+// with the reference's two-point term, source/equations/mhd/non_conservative_flux_mod.f90), the
+// surface flux plus the element's own-side non-conservative term (the reference's face treatment,
+// source/kernel/mcfv/3d/kernel_flux_mod.f90:230-250), FV subcells with the same interface terms
+// (:478-497), and the GLM damping -glm_alpha psi (:496-497).
+void mhd_element_rhs(const Ctx& c, const Mesh& M, const double* u, int64_t e, double alpha, double* rhs) {
+    const Ops& op = c.op;
+    const int V = 9;
+    const MhdPar P = c.mp();
+    double ue[NP][VMAX];
+    gather(c, M.E, u, e, ue);
+    double fs[6][NN * NN][VMAX];
+    for (int f = 0; f < 6; ++f) {
+        const int d = f >> 1, plus = f & 1;
+        const int64_t ne = M.nbr[e * 6 + f];
+        for (int b = 0; b < NN; ++b)
+            for (int a = 0; a < NN; ++a) {
+                const int own = face_node(f, a, b);
+                double uo[VMAX], unb[VMAX], F[VMAX], G[VMAX];
+                for (int v = 0; v < V; ++v) uo[v] = ue[own][v];
+                if (ne >= 0) {
+                    const int nn = face_node(f ^ 1, a, b);
+                    for (int v = 0; v < V; ++v) unb[v] = u[(v * M.E + ne) * NP + nn];
+                } else {
+                    for (int v = 0; v < V; ++v) unb[v] = uo[v];
+                }
+                if (plus) {
+                    m_riemann(c.cfg.surface_flux, d, uo, unb, F, P);
+                    m_nc(d, uo, uo, unb, G, P);
+                } else {
+                    m_riemann(c.cfg.surface_flux, d, unb, uo, F, P);
+                    m_nc(d, uo, unb, uo, G, P);
+                }
+                for (int v = 0; v < V; ++v) fs[f][a + NN * b][v] = F[v] + G[v];
+            }
+    }
+    static const int PI_[6] = {0, 0, 0, 1, 1, 2};
+    static const int PM_[6] = {1, 2, 3, 2, 3, 3};
+    double vol[3][NP][VMAX], fv[3][NP][VMAX];
+    for (int d = 0; d < 3; ++d)
+        for (int b = 0; b < NN; ++b)
+            for (int a = 0; a < NN; ++a) {
+                int idx[NN];
+                for (int i = 0; i < NN; ++i)
+                    idx[i] = d == 0 ? nidx(i, a, b) : (d == 1 ? nidx(a, i, b) : nidx(a, b, i));
+                double acc[NN][VMAX];
+                for (int i = 0; i < NN; ++i)
+                    for (int v = 0; v < V; ++v) acc[i][v] = 0.0;
+                for (int p = 0; p < 6; ++p) {
+                    const int i = PI_[p], m = PM_[p];
+                    double F[VMAX], Gi[VMAX], Gm[VMAX];
+                    m_twopoint(c.cfg.volume_flux, d, ue[idx[i]], ue[idx[m]], F, P);
+                    m_nc(d, ue[idx[i]], ue[idx[i]], ue[idx[m]], Gi, P);
+                    m_nc(d, ue[idx[m]], ue[idx[i]], ue[idx[m]], Gm, P);
+                    for (int v = 0; v < V; ++v) {
+                        acc[i][v] = acc[i][v] + op.S[i * NN + m] * (F[v] + Gi[v]);
+                        acc[m][v] = acc[m][v] + op.S[m * NN + i] * (F[v] + Gm[v]);
+                    }
+                }
+                for (int i = 0; i < NN; ++i)
+                    for (int v = 0; v < V; ++v) vol[d][idx[i]][v] = acc[i][v];
+                if (alpha > 0.0) {
+                    double Fh[NN + 1][VMAX];
+                    for (int i = 0; i < NN - 1; ++i) m_riemann(c.cfg.surface_flux, d, ue[idx[i]], ue[idx[i + 1]], Fh[i + 1], P);
+                    for (int i = 0; i < NN; ++i) {
+                        double FR[VMAX], FL[VMAX], G[VMAX];
+                        if (i < NN - 1) {
+                            m_nc(d, ue[idx[i]], ue[idx[i]], ue[idx[i + 1]], G, P);
+                            for (int v = 0; v < V; ++v) FR[v] = Fh[i + 1][v] + G[v];
+                        } else {
+                            for (int v = 0; v < V; ++v) FR[v] = fs[2 * d + 1][a + NN * b][v];
+                        }
+                        if (i > 0) {
+                            m_nc(d, ue[idx[i]], ue[idx[i - 1]], ue[idx[i]], G, P);
+                            for (int v = 0; v < V; ++v) FL[v] = Fh[i][v] + G[v];
+                        } else {
+                            for (int v = 0; v < V; ++v) FL[v] = fs[2 * d][a + NN * b][v];
+                        }
+                        for (int v = 0; v < V; ++v) fv[d][idx[i]][v] = op.winv[i] * (FR[v] - FL[v]);
+                    }
+                }
+            }
+    const double cd[3] = {2.0 / M.delta[e * 3 + 0], 2.0 / M.delta[e * 3 + 1], 2.0 / M.delta[e * 3 + 2]};
+    for (int k = 0; k < NN; ++k)
+        for (int j = 0; j < NN; ++j)
+            for (int i = 0; i < NN; ++i) {
+                const int p = nidx(i, j, k);
+                const int ii[3] = {i, j, k};
+                for (int v = 0; v < V; ++v) {
+                    double t[3];
+                    for (int d = 0; d < 3; ++d) {
+                        const int q = ii[d];
+                        double tt = vol[d][p][v];
+                        const int a = d == 0 ? j : i, b = d == 2 ? j : k;
+                        if (q == 0) tt = tt + op.winv[q] * (-fs[2 * d][a + NN * b][v]);
+                        else if (q == NN - 1) tt = tt + op.winv[q] * fs[2 * d + 1][a + NN * b][v];
+                        if (alpha > 0.0) tt = (1.0 - alpha) * tt + alpha * fv[d][p][v];
+                        t[d] = tt;
+                    }
+                    double r = -(cd[0] * t[0] + cd[1] * t[1] + cd[2] * t[2]);
+                    if (v == 8) r = r - c.cfg.glm_alpha * ue[p][8];
+                    rhs[(v * M.E + e) * NP + p] = r;
+                }
+            }
+}
+
 // dgfv_repair_3d, source/kernel/mcfv/3d/kernel_validate_mod.f90:159-272 (N_NODES = 4: 2 levels)
-bool tiles_valid(const double (*t)[VMAX], double kappa) {
+bool tiles_valid(const Ctx& c, const double (*t)[VMAX]) {
     for (int p = 0; p < 8; ++p)
-        if (!e_isvalid(t[p], kappa)) return false;
+        if (!isvalid_any(c, t[p])) return false;
     return true;
 }
 
 bool repair_element(const Ctx& c, double (*st)[VMAX]) {
-    const double kappa = c.cfg.kappa;
     const int V = c.V;
     bool ok = true;
-    for (int p = 0; p < NP; ++p) ok = ok && e_isvalid(st[p], kappa);
+    for (int p = 0; p < NP; ++p) ok = ok && isvalid_any(c, st[p]);
     if (ok) return true;
     const int nlevels = 2;
     for (int level = 1; level <= nlevels; ++level) {
@@ -719,7 +1021,7 @@ bool repair_element(const Ctx& c, double (*st)[VMAX]) {
                                                 int t = ii + 2 * (jj + 2 * kk);
                                                 tiles[t][v] = tiles[t][v] + ws * st[nidx(i, j, k)][v];
                                             }
-                    if (tiles_valid(tiles, kappa)) continue;
+                    if (tiles_valid(c, tiles)) continue;
                     for (int v = 0; v < V; ++v) {
                         double s = 0.0;
                         for (int t = 0; t < 8; ++t) s = s + tiles[t][v];
@@ -732,7 +1034,7 @@ bool repair_element(const Ctx& c, double (*st)[VMAX]) {
                         squeeze = std::max(0.0, squeeze - c.cfg.repair_decr);
                         for (int t = 0; t < 8; ++t)
                             for (int v = 0; v < V; ++v) tiles[t][v] = means[v] + squeeze * hiles[t][v];
-                        if (tiles_valid(tiles, kappa)) break;
+                        if (tiles_valid(c, tiles)) break;
                     }
                     for (int v = 0; v < V; ++v)
                         for (int k = 2 * r * nn; k < (2 * r + 2) * nn; ++k)
@@ -744,7 +1046,7 @@ bool repair_element(const Ctx& c, double (*st)[VMAX]) {
                 }
     }
     ok = true;
-    for (int p = 0; p < NP; ++p) ok = ok && e_isvalid(st[p], kappa);
+    for (int p = 0; p < NP; ++p) ok = ok && isvalid_any(c, st[p]);
     return ok;
 }
 
@@ -853,31 +1155,55 @@ void or_rhs(const nemo_cfg* cfg, int64_t E, const int32_t* nbr, const double* de
     if (alpha_in) std::memcpy(alpha.data(), alpha_in, sizeof(double) * E);
     else compute_alpha(c, M, u, alpha.data(), nthreads);
 #pragma omp parallel for schedule(dynamic, 16) num_threads(nthreads)
-    for (int64_t e = 0; e < E; ++e) element_rhs(c, M, u, e, alpha[e], rhs);
+    for (int64_t e = 0; e < E; ++e) {
+        if (c.mhd()) mhd_element_rhs(c, M, u, e, alpha[e], rhs);
+        else element_rhs(c, M, u, e, alpha[e], rhs);
+    }
 }
 
 // hook_calc_timestep_200 (DG form): dt = 0.5^(D-1)*cfl/(2*n-1)*min(delta/lambda); returns dt.
-double or_timestep(const nemo_cfg* cfg, int64_t E, const double* delta, const double* u, double* lmax_out) {
+// hook_calc_timestep_200 (DG form): dt = 0.5^(D-1)*cfl/(2*n-1)*min(delta/lambda); returns dt.
+// lmax: max wave speed; vmax: max |velocity component| (the GLM cleaning speed uses both,
+// source/kernel/mcfv/3d/kernel_timestep_mod.f90:338-344 and :373-377).
+double or_timestep2(const nemo_cfg* cfg, int64_t E, const double* delta, const double* u, double* lmax_out,
+                    double* vmax_out) {
     const double kappa = cfg->kappa;
     const int V = cfg->n_vars;
-    double dtmin = HUGE_VAL, lmax = 0.0;
+    const bool mhd = cfg->eqn == NEMO_EQN_MHD;
+    const MhdPar P{cfg->kappa, cfg->mu0, cfg->glm_ch};
+    double dtmin = HUGE_VAL, lmax = 0.0, vmax = 0.0;
     for (int64_t e = 0; e < E; ++e) {
         double lf = 0.0, lg = 0.0, lh = 0.0;
         for (int p = 0; p < NP; ++p) {
-            double q[VMAX], r[5];
+            double q[VMAX], r[VMAX];
             for (int v = 0; v < V; ++v) q[v] = u[(v * E + e) * NP + p];
-            lf = std::max(lf, e_xlambda(q, kappa));
-            rot_in(1, q, r);
-            lg = std::max(lg, e_xlambda(r, kappa));
-            rot_in(2, q, r);
-            lh = std::max(lh, e_xlambda(r, kappa));
+            if (mhd) {
+                lf = std::max(lf, m_xlambda(q, P));
+                m_rot_in(1, q, r);
+                lg = std::max(lg, m_xlambda(r, P));
+                m_rot_in(2, q, r);
+                lh = std::max(lh, m_xlambda(r, P));
+                vmax = std::max(vmax, std::max(std::max(std::fabs(q[1] / q[0]), std::fabs(q[2] / q[0])),
+                                               std::fabs(q[3] / q[0])));
+            } else {
+                lf = std::max(lf, e_xlambda(q, kappa));
+                rot_in(1, q, r);
+                lg = std::max(lg, e_xlambda(r, kappa));
+                rot_in(2, q, r);
+                lh = std::max(lh, e_xlambda(r, kappa));
+            }
         }
         double dt = std::min(std::min(delta[e * 3 + 0] / lf, delta[e * 3 + 1] / lg), delta[e * 3 + 2] / lh);
         dtmin = std::min(dtmin, dt);
         lmax = std::max(lmax, std::max(std::max(lf, lg), lh));
     }
     if (lmax_out) *lmax_out = lmax;
+    if (vmax_out) *vmax_out = vmax;
     return 0.25 * cfg->cfl / (double)(2 * NN - 1) * dtmin;
+}
+
+double or_timestep(const nemo_cfg* cfg, int64_t E, const double* delta, const double* u, double* lmax_out) {
+    return or_timestep2(cfg, E, delta, u, lmax_out, nullptr);
 }
 
 // One LSRK stage (0-based stage), in place on u and reg.  Returns #elements whose repair failed.
@@ -889,7 +1215,10 @@ int64_t or_stage(const nemo_cfg* cfg, int64_t E, const int32_t* nbr, const doubl
     std::vector<double> rhs((size_t)V * E * NP), alpha(E);
     compute_alpha(c, M, u, alpha.data(), nthreads);
 #pragma omp parallel for schedule(dynamic, 16) num_threads(nthreads)
-    for (int64_t e = 0; e < E; ++e) element_rhs(c, M, u, e, alpha[e], rhs.data());
+    for (int64_t e = 0; e < E; ++e) {
+        if (c.mhd()) mhd_element_rhs(c, M, u, e, alpha[e], rhs.data());
+        else element_rhs(c, M, u, e, alpha[e], rhs.data());
+    }
     const double A = RK_A[stage], Cdt = RK_C[stage] * dt;
     int64_t nbad = 0;
 #pragma omp parallel for schedule(static) num_threads(nthreads) reduction(+ : nbad)
@@ -916,12 +1245,18 @@ int64_t or_run(const nemo_cfg* cfg, int64_t E, const int32_t* nbr, const double*
     std::vector<double> reg((size_t)V * E * NP, 0.0);
     double t = t_io ? *t_io : 0.0;
     int64_t steps = 0, nbad = 0;
+    nemo_cfg c = *cfg;
     while (true) {
         if (nsteps > 0 && steps >= nsteps) break;
         if (t_end > 0.0 && t >= t_end) break;
-        double dt = or_timestep(cfg, E, delta, u, nullptr);
+        double lmax = 0.0, vmax = 0.0;
+        double dt = or_timestep2(&c, E, delta, u, &lmax, &vmax);
+        if (c.eqn == NEMO_EQN_MHD) {  // GLM cleaning speed and damping of this step
+            c.glm_ch = 2.0 * std::fabs(lmax - vmax);
+            c.glm_alpha = c.glm_ch / 0.18;
+        }
         if (t_end > 0.0 && t + dt > t_end) dt = t_end - t;
-        for (int s = 0; s < 5; ++s) nbad += or_stage(cfg, E, nbr, delta, s, dt, u, reg.data(), nthreads);
+        for (int s = 0; s < 5; ++s) nbad += or_stage(&c, E, nbr, delta, s, dt, u, reg.data(), nthreads);
         t = t + dt;
         steps += 1;
     }
@@ -963,6 +1298,25 @@ int or_repair(const nemo_cfg* cfg, double* st) {
         for (int p = 0; p < NP; ++p) st[v * NP + p] = s[p][v];
     return ok ? 1 : 0;
 }
+
+// MHD unit entry points (9 variables): physical flux, Rusanov, two-point, non-conservative term.
+void or_mhd_flux(int d, const double* u, double* f, double kappa, double mu0, double ch) {
+    MhdPar P{kappa, mu0, ch};
+    double r[9], rf[9];
+    m_rot_in(d, u, r);
+    m_xflux(r, rf, P);
+    m_rot_out(d, rf, f);
+}
+void or_mhd_riemann(int d, const double* uL, const double* uR, double* F, double kappa, double mu0, double ch) {
+    m_riemann(NEMO_SURFFLUX_RUSANOV, d, uL, uR, F, MhdPar{kappa, mu0, ch});
+}
+void or_mhd_twopoint(int kind, int d, const double* u, const double* v, double* F, double kappa, double mu0, double ch) {
+    m_twopoint(kind, d, u, v, F, MhdPar{kappa, mu0, ch});
+}
+void or_mhd_nc(int d, const double* UI, const double* UL, const double* UR, double* F, double kappa, double mu0) {
+    m_nc(d, UI, UL, UR, F, MhdPar{kappa, mu0, 0.0});
+}
+double or_mhd_pressure(const double* u, double kappa, double mu0) { return m_pressure(u, MhdPar{kappa, mu0, 0.0}); }
 
 // Learned indicator weights (1505 values, see mlp_alpha) and normalised-input bounds (12 + 12).
 void or_set_mlp(const double* w, const double* lo, const double* hi) {

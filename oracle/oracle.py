@@ -61,6 +61,15 @@ def lib():
         L.or_exp.restype = ctypes.c_double
         L.or_exp.argtypes = [ctypes.c_double]
         L.or_set_mlp.argtypes = [_dp, _dp, _dp]
+        L.or_mhd_flux.argtypes = [ctypes.c_int, _dp, _dp, ctypes.c_double, ctypes.c_double, ctypes.c_double]
+        L.or_mhd_riemann.argtypes = [ctypes.c_int, _dp, _dp, _dp, ctypes.c_double, ctypes.c_double, ctypes.c_double]
+        L.or_mhd_twopoint.argtypes = [ctypes.c_int, ctypes.c_int, _dp, _dp, _dp, ctypes.c_double, ctypes.c_double,
+                                      ctypes.c_double]
+        L.or_mhd_nc.argtypes = [ctypes.c_int, _dp, _dp, _dp, _dp, ctypes.c_double, ctypes.c_double]
+        L.or_mhd_pressure.restype = ctypes.c_double
+        L.or_mhd_pressure.argtypes = [_dp, ctypes.c_double, ctypes.c_double]
+        L.or_timestep2.restype = ctypes.c_double
+        L.or_timestep2.argtypes = [ctypes.c_void_p, ctypes.c_int64, _dp, _dp, _dp, _dp]
         L.or_features.argtypes = [ctypes.c_void_p, ctypes.c_int64, _dp, _dp, ctypes.c_void_p, ctypes.c_int]
         L.or_mlp_alpha.restype = ctypes.c_double
         L.or_mlp_alpha.argtypes = [ctypes.c_void_p, _dp]
@@ -120,6 +129,34 @@ def features(cfg, u):
 def mlp_alpha(cfg, feat):
     feat = _f64(feat)
     return lib().or_mlp_alpha(ctypes.byref(cfg), _p(feat))
+
+
+def mhd_flux(d, u, kappa=5 / 3, mu0=1.0, ch=0.0):
+    u = _f64(u)
+    f = np.zeros(9)
+    lib().or_mhd_flux(d, _p(u), _p(f), kappa, mu0, ch)
+    return f
+
+
+def mhd_riemann(d, uL, uR, kappa=5 / 3, mu0=1.0, ch=0.0):
+    uL, uR = _f64(uL), _f64(uR)
+    f = np.zeros(9)
+    lib().or_mhd_riemann(d, _p(uL), _p(uR), _p(f), kappa, mu0, ch)
+    return f
+
+
+def mhd_twopoint(kind, d, u, v, kappa=5 / 3, mu0=1.0, ch=0.0):
+    u, v = _f64(u), _f64(v)
+    f = np.zeros(9)
+    lib().or_mhd_twopoint(kind, d, _p(u), _p(v), _p(f), kappa, mu0, ch)
+    return f
+
+
+def mhd_nc(d, ui, ul, ur, kappa=5 / 3, mu0=1.0):
+    ui, ul, ur = _f64(ui), _f64(ul), _f64(ur)
+    f = np.zeros(9)
+    lib().or_mhd_nc(d, _p(ui), _p(ul), _p(ur), _p(f), kappa, mu0)
+    return f
 
 
 def repair(cfg, st):
@@ -194,6 +231,13 @@ class Oracle:
         lm = ctypes.c_double(0)
         dt = lib().or_timestep(self._c(), self.E, _p(self.delta), _p(u), ctypes.byref(lm))
         return dt, lm.value
+
+    def timestep2(self, u):
+        """dt, max wave speed, max velocity component (MHD cleaning speed inputs)."""
+        u = _f64(u)
+        lm, vm = ctypes.c_double(0), ctypes.c_double(0)
+        dt = lib().or_timestep2(self._c(), self.E, _p(self.delta), _p(u), ctypes.byref(lm), ctypes.byref(vm))
+        return dt, lm.value, vm.value
 
     def stage(self, u, reg, stage, dt):
         """In place on u and reg (float64 C-contiguous); stage is 0-based."""
