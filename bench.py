@@ -31,7 +31,14 @@ WORKLOADS = {
                     desc="Sedov blast 32^3 elements N=3 (2.1M nodes), DG/FV blending, FP64"),
     "wave16": dict(nx=16, setup="wave", indicator=0, positivity=0,
                    desc="periodic density wave 16^3 elements N=3 (262k nodes), EC volume + HLLC, FP64"),
+    "ot64": dict(nx=64, setup="orszag_tang", indicator=1, positivity=1, mhd=True, t_end=0.1,
+                 desc="GLM-MHD Orszag-Tang 64^3 elements N=3 (16.8M nodes, 9 variables), gamma 5/3, "
+                      "b0 = 1/sqrt(4 pi), HLLD surface + EC volume, DG/FV blending"),
 }
+
+
+def nvars(wl):
+    return 9 if WORKLOADS[wl].get("mhd") else 5
 
 
 def load_peaks():
@@ -49,6 +56,9 @@ def make_state(wl):
     if w["setup"] == "sedov":
         m = mesh.brick(w["nx"], lo=(-0.5,) * 3, hi=(0.5,) * 3)
         u = setups.sedov(m, sigma=0.05)
+    elif w["setup"] == "orszag_tang":
+        m = mesh.brick(w["nx"])
+        u = setups.orszag_tang(m)
     else:
         m = mesh.brick(w["nx"])
         u = setups.density_wave(m, seed=1234)
@@ -59,6 +69,10 @@ def make_cfg(wl, precision=0, learned=False):
     from nemo_b200 import abi
     w = WORKLOADS[wl]
     ind = abi.IND_LEARNED if (learned and w["indicator"]) else w["indicator"]
+    if w.get("mhd"):
+        return abi.default_cfg(indicator=ind, positivity=w["positivity"], cfl=0.5, precision=precision,
+                               eqn=abi.EQN_MHD, n_vars=9, volume_flux=abi.VOLFLUX_EC_MHD,
+                               surface_flux=abi.SURFFLUX_HLLD, kappa=5.0 / 3.0, mu0=1.0)
     return abi.default_cfg(indicator=ind, positivity=w["positivity"], cfl=0.5, precision=precision)
 
 
@@ -163,7 +177,7 @@ def cpu_baseline(wl, u, m, nthreads=None, sample_stages=5):
                       f"{o.nthreads} OpenMP threads, {el:.2f} s"}
 
 
-def accuracy_check(wl, m, u, abi, Solver, t_end=0.05):
+def accuracy_check(wl, m, u, abi, Solver, t_end=0.05):  # noqa: C901
     """All forms to t_end.  The chosen form (FP32 bulk + learned indicator) against the FP64 form of
     the same method (learned indicator evaluated in FP64 from the same BF16 weights; that plain
     path reproduces the FP64 oracle bit for bit, see tests/test_gpu_learned.py), and both against
@@ -179,8 +193,11 @@ def accuracy_check(wl, m, u, abi, Solver, t_end=0.05):
         el = time.perf_counter() - t0
         fb, jn, mae = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_double()
         abi.call("nemo_gpu_indicator_stats", ctypes.byref(fb), ctypes.byref(jn), ctypes.byref(mae))
-        res[key] = dict(rho=s.download()[0], t=t, steps=n, wall=el, nbad=s.status()[1], fallback=fb.value,
+        uf = s.download()
+        res[key] = dict(rho=uf[0], t=t, steps=n, wall=el, nbad=s.status()[1], fallback=fb.value,
                         judged=jn.value, judge_mae=mae.value)
+        if WORKLOADS[wl].get("mhd"):
+            res[key]["divb"] = divb(m, uf, abi)
         s.finalize()
 
     def l1(a, b):
@@ -196,7 +213,15 @@ def accuracy_check(wl, m, u, abi, Solver, t_end=0.05):
                                     "mean_abs_alpha_learned_minus_modal": v["judge_mae"]}
                                 for k, v in r.items() if k != "fp64_modal"},
             "repair_failures": {k: v["nbad"] for k, v in r.items()},
-            "wall_s_to_t_end": {k: v["wall"] for k, v in r.items()}}
+            "wall_s_to_t_end": {k: v["wall"] for k, v in r.items()},
+            **({"div_b_l2_linf": {"t0": divb(m, u, abi), **{k: v["divb"] for k, v in r.items()}}}
+               if WORKLOADS[wl].get("mhd") else {})}
+
+
+def divb(m, u, abi):
+    from nemo_b200 import setups
+    _, w, D, _, _ = abi.operators()
+    return setups.divergence_b(m, u, D, w)
 
 
 def run_reference(args, rank, world):
@@ -267,6 +292,8 @@ def main():
 
     m, u = make_state(args.workload)
     dof_per_step = m.E * 64 * 5
+    V = nvars(args.workload)
+    mhd = bool(WORKLOADS[args.workload].get("mhd"))
 
     # ---- the plain FP64 form (the comparison point of the metric)
     s = Solver(make_cfg(args.workload, abi.PREC_FP64), m)
@@ -291,7 +318,6 @@ def main():
     value = world * dof_per_step * args.steps / (ms * 1e-3)
 
     # ---- roofline of the stage kernel (HBM): algorithmic bytes per launch / avg launch time
-    V = 5
     bytes_per_launch = sum(m.E * 64 * V * 8 * (3 if st == 0 else 4) for st in range(5)) / 5.0
     avg_stage_s = st_ms_v * 1e-3 / max(st_n_v, 1)
     peak, peak_kind = load_peaks()
@@ -334,8 +360,8 @@ def main():
 
     s.finalize()
     accuracy = None
-    if not args.no_accuracy and WORKLOADS[args.workload]["setup"] == "sedov":
-        accuracy = accuracy_check(args.workload, m, u, abi, Solver)
+    if not args.no_accuracy and WORKLOADS[args.workload]["setup"] in ("sedov", "orszag_tang"):
+        accuracy = accuracy_check(args.workload, m, u, abi, Solver, t_end=WORKLOADS[args.workload].get("t_end", 0.05))
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -359,11 +385,12 @@ def main():
                        "stages_per_step": 5,
                        "form": "chosen: FP32 bulk + FP64 accumulation, learned indicator with modal fallback",
                        "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
-                       "l2": "working set (u in/out + register, 3 x 84 MB) larger than L2"},
+                       "l2": f"working set (u in/out + register, 3 x {u.nbytes / 1e6:.0f} MB) larger than L2"},
             "clocks": clk.summary(),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
-                         "kernel": "k_stage_euler32", "algorithmic_bytes_per_launch": bytes_per_launch,
+                         "kernel": "k_stage_mhd<float>" if mhd else "k_stage_euler32",
+                         "algorithmic_bytes_per_launch": bytes_per_launch,
                          "avg_launch_ms": avg_stage_s * 1e3},
             "e2e": None if e2e_val is None else {
                     "value": e2e_val, "unit": "DOF-updates/s", "h2d_bytes_per_step": nbytes,
@@ -373,7 +400,8 @@ def main():
             "gpu_launches": int(tot_n_v),
             "sim": {"t": t_sim, "steps": nst},
             "plain_fp64": {"value": value64, "unit": "DOF-updates/s", "ms_per_step": ms64 / args.steps,
-                           "avg_stage_ms": st64 / max(n64, 1), "kernel": "k_stage_euler64",
+                           "avg_stage_ms": st64 / max(n64, 1),
+                           "kernel": "k_stage_mhd<double>" if mhd else "k_stage_euler64",
                            "speedup_of_chosen_form": value / value64},
             "accuracy": accuracy,
         }

@@ -84,6 +84,156 @@ __device__ __forceinline__ void m_rusanov_x(const R* uL, const R* uR, R* F, R ka
     for (int v = 0; v < 9; ++v) F[v] = R(0.5) * (FL[v] + FR[v] + lmax * (uL[v] - uR[v]));
 }
 
+// HLLD (Miyoshi & Kusano, J. Comput. Phys. 208 (2005) 315-344) for mu0 = 1: the star and double-star
+// states of source/equations/mhd/riemann/hlld/riemann_mod.f90:114-246 with the wave speeds of :83-97.
+// That file is disabled in the reference (its line 1 is an #error: the GLM pair is not handled) and
+// evaluates the fast speed on primitive variables; here the fast speed is taken from the conserved
+// state, and the GLM pair (B_n, psi) is solved upwind first (characteristics B_n +- psi at speeds
+// +-c_h, Dedner et al., J. Comput. Phys. 175 (2002)): both HLLD states use the upwind B_n*, the
+// energy drops psi^2/2, and the GLM fluxes c_h psi*, c_h B_n*, c_h B_n* psi* are added at the end.
+template <typename R>
+__device__ __forceinline__ void m_hlld_x(const R* uL, const R* uR, R* F, R kappa, R ch) {
+    const R half = R(0.5);
+    // GLM pair: characteristics B_n + psi (speed +c_h) from the left, B_n - psi (speed -c_h) from the right
+    const R bn = half * (uL[5] + uR[5]) - half * (uR[8] - uL[8]);
+    const R psn = half * (uL[8] + uR[8]) - half * (uR[5] - uL[5]);
+    const R bn2 = bn * bn;
+    // primitive states; the pressure keeps the conserved state's own B_n, the energy E' drops psi
+    R rho[2], un[2], vt1[2], vt2[2], bt1[2], bt2[2], pr[2], et[2], pt[2], cf[2];
+#pragma unroll
+    for (int s = 0; s < 2; ++s) {
+        const R* u = s ? uR : uL;
+        rho[s] = u[0];
+        un[s] = u[1] / u[0];
+        vt1[s] = u[2] / u[0];
+        vt2[s] = u[3] / u[0];
+        bt1[s] = u[6];
+        bt2[s] = u[7];
+        pr[s] = (kappa - R(1.0)) * (u[4] - half / u[0] * (u[1] * u[1] + u[2] * u[2] + u[3] * u[3]) -
+                                    half * (u[5] * u[5] + u[6] * u[6] + u[7] * u[7] + u[8] * u[8]));
+        const R bb = bn2 + bt1[s] * bt1[s] + bt2[s] * bt2[s];
+        et[s] = pr[s] / (kappa - R(1.0)) + half * rho[s] * (un[s] * un[s] + vt1[s] * vt1[s] + vt2[s] * vt2[s]) + half * bb;
+        pt[s] = pr[s] + half * bb;
+        const R cs2 = kappa * pr[s] / rho[s];
+        const R ca2 = bn2 / rho[s];
+        const R va2 = bb / rho[s];
+        cf[s] = sqrt(half * (cs2 + va2 + sqrt((cs2 + va2) * (cs2 + va2) - R(4.0) * cs2 * ca2)));
+    }
+    const R cmax = fmax(cf[0], cf[1]);
+    const R SL = fmin(un[0], un[1]) - cmax;
+    const R SR = fmax(un[0], un[1]) + cmax;
+    // ideal-MHD fluxes of both states (GLM parts added at the end) and the states themselves
+    R Fk[2][8], Uk[2][8];
+#pragma unroll
+    for (int s = 0; s < 2; ++s) {
+        const R vb = un[s] * bn + vt1[s] * bt1[s] + vt2[s] * bt2[s];
+        const R m = rho[s] * un[s];
+        Fk[s][0] = m;
+        Fk[s][1] = m * un[s] + pt[s] - bn2;
+        Fk[s][2] = m * vt1[s] - bn * bt1[s];
+        Fk[s][3] = m * vt2[s] - bn * bt2[s];
+        Fk[s][4] = (et[s] + pt[s]) * un[s] - bn * vb;
+        Fk[s][5] = R(0.0);
+        Fk[s][6] = un[s] * bt1[s] - bn * vt1[s];
+        Fk[s][7] = un[s] * bt2[s] - bn * vt2[s];
+        Uk[s][0] = rho[s];
+        Uk[s][1] = m;
+        Uk[s][2] = rho[s] * vt1[s];
+        Uk[s][3] = rho[s] * vt2[s];
+        Uk[s][4] = et[s];
+        Uk[s][5] = bn;
+        Uk[s][6] = bt1[s];
+        Uk[s][7] = bt2[s];
+    }
+    if (SL > R(0.0)) {
+#pragma unroll
+        for (int v = 0; v < 8; ++v) F[v] = Fk[0][v];
+    } else if (SR < R(0.0)) {
+#pragma unroll
+        for (int v = 0; v < 8; ++v) F[v] = Fk[1][v];
+    } else {
+        const R dL = rho[0] * (SL - un[0]), dR = rho[1] * (SR - un[1]);
+        const R SM = (dR * un[1] - dL * un[0] - pt[1] + pt[0]) / (dR - dL);
+        const R ptS = pt[0] + dL * (SM - un[0]);
+        // single-star states
+        R rs[2], ws1[2], ws2[2], cs1[2], cs2[2], es[2];
+#pragma unroll
+        for (int s = 0; s < 2; ++s) {
+            const R S = s ? SR : SL;
+            const R d = s ? dR : dL;
+            rs[s] = d / (S - SM);
+            const R den = d * (S - SM) - bn2;
+            if (fabs(den) < R(1.0e-8)) {
+                ws1[s] = vt1[s];
+                ws2[s] = vt2[s];
+                cs1[s] = bt1[s];
+                cs2[s] = bt2[s];
+            } else {
+                const R fv = bn * (SM - un[s]) / den;
+                const R fb = (d * (S - un[s]) - bn2) / den;
+                ws1[s] = vt1[s] - fv * bt1[s];
+                ws2[s] = vt2[s] - fv * bt2[s];
+                cs1[s] = fb * bt1[s];
+                cs2[s] = fb * bt2[s];
+            }
+            const R vb = un[s] * bn + vt1[s] * bt1[s] + vt2[s] * bt2[s];
+            const R vbs = SM * bn + ws1[s] * cs1[s] + ws2[s] * cs2[s];
+            es[s] = ((S - un[s]) * et[s] - pt[s] * un[s] + ptS * SM + bn * (vb - vbs)) / (S - SM);
+        }
+        const R sqL = sqrt(rs[0]), sqR = sqrt(rs[1]);
+        const R SLs = SM - fabs(bn) / sqL, SRs = SM + fabs(bn) / sqR;
+        const int s = SM >= R(0.0) ? 0 : 1;
+        const R S = s ? SR : SL;
+        R Us[8];
+        Us[0] = rs[s];
+        Us[1] = rs[s] * SM;
+        Us[2] = rs[s] * ws1[s];
+        Us[3] = rs[s] * ws2[s];
+        Us[4] = es[s];
+        Us[5] = bn;
+        Us[6] = cs1[s];
+        Us[7] = cs2[s];
+        const bool outer = s ? (SRs < R(0.0)) : (SLs >= R(0.0));
+        if (outer) {
+#pragma unroll
+            for (int v = 0; v < 8; ++v) F[v] = Fk[s][v] + S * (Us[v] - Uk[s][v]);
+        } else {
+            // double-star state of side s (Alfven waves); it equals the single-star state if B_n = 0
+            R Uss[8];
+#pragma unroll
+            for (int v = 0; v < 8; ++v) Uss[v] = Us[v];
+            if (fabs(bn) >= R(1.0e-12)) {
+                const R sg = bn < R(0.0) ? R(-1.0) : R(1.0);
+                const R sden = R(1.0) / (sqL + sqR);
+                const R w1 = (sqL * ws1[0] + sqR * ws1[1] + sg * (cs1[1] - cs1[0])) * sden;
+                const R w2 = (sqL * ws2[0] + sqR * ws2[1] + sg * (cs2[1] - cs2[0])) * sden;
+                const R c1 = (sqL * cs1[1] + sqR * cs1[0] + sg * sqL * sqR * (ws1[1] - ws1[0])) * sden;
+                const R c2 = (sqL * cs2[1] + sqR * cs2[0] + sg * sqL * sqR * (ws2[1] - ws2[0])) * sden;
+                const R wcs = ws1[s] * cs1[s] + ws2[s] * cs2[s];
+                const R wcss = w1 * c1 + w2 * c2;
+                const R sq = s ? sqR : sqL;
+                Uss[2] = rs[s] * w1;
+                Uss[3] = rs[s] * w2;
+                Uss[4] = s ? es[s] + sg * sq * (wcs - wcss) : es[s] - sg * sq * (wcs - wcss);
+                Uss[6] = c1;
+                Uss[7] = c2;
+            }
+            const R Ss = s ? SRs : SLs;
+#pragma unroll
+            for (int v = 0; v < 8; ++v) F[v] = Fk[s][v] + Ss * Uss[v] - (Ss - S) * Us[v] - S * Uk[s][v];
+        }
+    }
+    F[4] = F[4] + ch * bn * psn;
+    F[5] = ch * psn;
+    F[8] = ch * bn;
+}
+
+template <typename R>
+__device__ __forceinline__ void m_riemann_x(int kind, const R* uL, const R* uR, R* F, R kappa, R mu0, R ch) {
+    if (kind == NEMO_SURFFLUX_HLLD) m_hlld_x(uL, uR, F, kappa, ch);
+    else m_rusanov_x(uL, uR, F, kappa, mu0, ch);
+}
+
 // LN_MEAN, source/equations/mhd/two_point/ec/two_point_flux_mod.f90:203-219 (relative switch)
 template <typename R>
 __device__ __forceinline__ R ln_mean_rel(R aL, R aR) {

@@ -394,9 +394,12 @@ int nemo_gpu_init(const nemo_cfg* cfg) {
         if (cfg->n_vars != 9) return fail(NEMO_ERR_ARG, "GLM-MHD has n_vars 9");
         if (cfg->volume_flux != NEMO_VOLFLUX_EC_MHD && cfg->volume_flux != NEMO_VOLFLUX_CENTRAL)
             return fail(NEMO_ERR_ARG, "unsupported MHD volume flux %d", cfg->volume_flux);
-        if (cfg->surface_flux != NEMO_SURFFLUX_RUSANOV)
-            return fail(NEMO_ERR_ARG, "MHD surface flux %d is not available in this build (Rusanov only)", cfg->surface_flux);
+        if (cfg->surface_flux != NEMO_SURFFLUX_RUSANOV && cfg->surface_flux != NEMO_SURFFLUX_HLLD)
+            return fail(NEMO_ERR_ARG, "unsupported MHD surface flux %d (Rusanov or HLLD)", cfg->surface_flux);
         if (!(cfg->mu0 > 0.0)) return fail(NEMO_ERR_ARG, "mu0 must be positive");
+        // the HLLD star states assume mu0 = 1 (source/equations/mhd/riemann/hlld/riemann_mod.f90:13)
+        if (cfg->surface_flux == NEMO_SURFFLUX_HLLD && cfg->mu0 != 1.0)
+            return fail(NEMO_ERR_ARG, "the HLLD surface flux requires mu0 = 1 (got %g)", cfg->mu0);
     } else {
         return fail(NEMO_ERR_ARG, "unknown equation system %d", cfg->eqn);
     }

@@ -381,10 +381,10 @@ __global__ void __launch_bounds__(mhd::NT, 1) k_stage_mhd(StageArgs a) {
                     for (int v = 0; v < MV; ++v) un[v] = uo[v];
                 }
                 if (side) {
-                    m_rusanov_x(uo, un, F, kap, mu0, ch);
+                    m_riemann_x(a.surface_flux, uo, un, F, kap, mu0, ch);
                     m_nc_x(uo, uo, un, G, mu0);
                 } else {
-                    m_rusanov_x(un, uo, F, kap, mu0, ch);
+                    m_riemann_x(a.surface_flux, un, uo, F, kap, mu0, ch);
                     m_nc_x(uo, un, uo, G, mu0);
                 }
 #pragma unroll
@@ -442,7 +442,7 @@ __global__ void __launch_bounds__(mhd::NT, 1) k_stage_mhd(StageArgs a) {
                         if (i < NN - 1) {
                             R ur[MV];
                             load_rot(su, el, idx[i + 1], d, ur);
-                            m_rusanov_x(ui, ur, Fh, kap, mu0, ch);
+                            m_riemann_x(a.surface_flux, ui, ur, Fh, kap, mu0, ch);
                             m_nc_x(ui, ui, ur, G, mu0);
 #pragma unroll
                             for (int v = 0; v < MV; ++v) FR[v] = Fh[v] + G[v];

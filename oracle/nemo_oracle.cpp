@@ -476,6 +476,140 @@ void m_rusanov_x(const double* uL, const double* uR, double* F, const MhdPar& P)
     for (int v = 0; v < 9; ++v) F[v] = 0.5 * (FL[v] + FR[v] + lmax * (uL[v] - uR[v]));
 }
 
+// HLLD (Miyoshi & Kusano 2005) for mu0 = 1: star and double-star states of
+// source/equations/mhd/riemann/hlld/riemann_mod.f90:114-246, wave speeds of :83-97 with the fast speed
+// taken from the conserved state (the reference passes primitives there, and the file is disabled by the
+// #error on its line 1), and the GLM pair solved upwind first (Dedner et al. 2002): B_n* and psi* from
+// the characteristics B_n +- psi, HLLD on the ideal-MHD part with B_n*, then c_h psi*, c_h B_n* and
+// c_h B_n* psi* as the GLM fluxes.
+void m_hlld_x(const double* uL, const double* uR, double* F, double kappa, double ch) {
+    const double half = 0.5;
+    // GLM pair: characteristics B_n + psi (speed +c_h) from the left, B_n - psi (speed -c_h) from the right
+    const double bn = half * (uL[5] + uR[5]) - half * (uR[8] - uL[8]);
+    const double psn = half * (uL[8] + uR[8]) - half * (uR[5] - uL[5]);
+    const double bn2 = bn * bn;
+    // primitive states; the pressure keeps the conserved state's own B_n, the energy E' drops psi
+    double rho[2], un[2], vt1[2], vt2[2], bt1[2], bt2[2], pr[2], et[2], pt[2], cf[2];
+    for (int s = 0; s < 2; ++s) {
+        const double* u = s ? uR : uL;
+        rho[s] = u[0];
+        un[s] = u[1] / u[0];
+        vt1[s] = u[2] / u[0];
+        vt2[s] = u[3] / u[0];
+        bt1[s] = u[6];
+        bt2[s] = u[7];
+        pr[s] = (kappa - 1.0) * (u[4] - half / u[0] * (u[1] * u[1] + u[2] * u[2] + u[3] * u[3]) -
+                                    half * (u[5] * u[5] + u[6] * u[6] + u[7] * u[7] + u[8] * u[8]));
+        const double bb = bn2 + bt1[s] * bt1[s] + bt2[s] * bt2[s];
+        et[s] = pr[s] / (kappa - 1.0) + half * rho[s] * (un[s] * un[s] + vt1[s] * vt1[s] + vt2[s] * vt2[s]) + half * bb;
+        pt[s] = pr[s] + half * bb;
+        const double cs2 = kappa * pr[s] / rho[s];
+        const double ca2 = bn2 / rho[s];
+        const double va2 = bb / rho[s];
+        cf[s] = std::sqrt(half * (cs2 + va2 + std::sqrt((cs2 + va2) * (cs2 + va2) - 4.0 * cs2 * ca2)));
+    }
+    const double cmax = std::fmax(cf[0], cf[1]);
+    const double SL = std::fmin(un[0], un[1]) - cmax;
+    const double SR = std::fmax(un[0], un[1]) + cmax;
+    // ideal-MHD fluxes of both states (GLM parts added at the end) and the states themselves
+    double Fk[2][8], Uk[2][8];
+    for (int s = 0; s < 2; ++s) {
+        const double vb = un[s] * bn + vt1[s] * bt1[s] + vt2[s] * bt2[s];
+        const double m = rho[s] * un[s];
+        Fk[s][0] = m;
+        Fk[s][1] = m * un[s] + pt[s] - bn2;
+        Fk[s][2] = m * vt1[s] - bn * bt1[s];
+        Fk[s][3] = m * vt2[s] - bn * bt2[s];
+        Fk[s][4] = (et[s] + pt[s]) * un[s] - bn * vb;
+        Fk[s][5] = 0.0;
+        Fk[s][6] = un[s] * bt1[s] - bn * vt1[s];
+        Fk[s][7] = un[s] * bt2[s] - bn * vt2[s];
+        Uk[s][0] = rho[s];
+        Uk[s][1] = m;
+        Uk[s][2] = rho[s] * vt1[s];
+        Uk[s][3] = rho[s] * vt2[s];
+        Uk[s][4] = et[s];
+        Uk[s][5] = bn;
+        Uk[s][6] = bt1[s];
+        Uk[s][7] = bt2[s];
+    }
+    if (SL > 0.0) {
+        for (int v = 0; v < 8; ++v) F[v] = Fk[0][v];
+    } else if (SR < 0.0) {
+        for (int v = 0; v < 8; ++v) F[v] = Fk[1][v];
+    } else {
+        const double dL = rho[0] * (SL - un[0]), dR = rho[1] * (SR - un[1]);
+        const double SM = (dR * un[1] - dL * un[0] - pt[1] + pt[0]) / (dR - dL);
+        const double ptS = pt[0] + dL * (SM - un[0]);
+        // single-star states
+        double rs[2], ws1[2], ws2[2], cs1[2], cs2[2], es[2];
+        for (int s = 0; s < 2; ++s) {
+            const double S = s ? SR : SL;
+            const double d = s ? dR : dL;
+            rs[s] = d / (S - SM);
+            const double den = d * (S - SM) - bn2;
+            if (std::fabs(den) < 1.0e-8) {
+                ws1[s] = vt1[s];
+                ws2[s] = vt2[s];
+                cs1[s] = bt1[s];
+                cs2[s] = bt2[s];
+            } else {
+                const double fv = bn * (SM - un[s]) / den;
+                const double fb = (d * (S - un[s]) - bn2) / den;
+                ws1[s] = vt1[s] - fv * bt1[s];
+                ws2[s] = vt2[s] - fv * bt2[s];
+                cs1[s] = fb * bt1[s];
+                cs2[s] = fb * bt2[s];
+            }
+            const double vb = un[s] * bn + vt1[s] * bt1[s] + vt2[s] * bt2[s];
+            const double vbs = SM * bn + ws1[s] * cs1[s] + ws2[s] * cs2[s];
+            es[s] = ((S - un[s]) * et[s] - pt[s] * un[s] + ptS * SM + bn * (vb - vbs)) / (S - SM);
+        }
+        const double sqL = std::sqrt(rs[0]), sqR = std::sqrt(rs[1]);
+        const double SLs = SM - std::fabs(bn) / sqL, SRs = SM + std::fabs(bn) / sqR;
+        const int s = SM >= 0.0 ? 0 : 1;
+        const double S = s ? SR : SL;
+        double Us[8];
+        Us[0] = rs[s];
+        Us[1] = rs[s] * SM;
+        Us[2] = rs[s] * ws1[s];
+        Us[3] = rs[s] * ws2[s];
+        Us[4] = es[s];
+        Us[5] = bn;
+        Us[6] = cs1[s];
+        Us[7] = cs2[s];
+        const bool outer = s ? (SRs < 0.0) : (SLs >= 0.0);
+        if (outer) {
+            for (int v = 0; v < 8; ++v) F[v] = Fk[s][v] + S * (Us[v] - Uk[s][v]);
+        } else {
+            // double-star state of side s (Alfven waves); it equals the single-star state if B_n = 0
+            double Uss[8];
+            for (int v = 0; v < 8; ++v) Uss[v] = Us[v];
+            if (std::fabs(bn) >= 1.0e-12) {
+                const double sg = bn < 0.0 ? -1.0 : 1.0;
+                const double sden = 1.0 / (sqL + sqR);
+                const double w1 = (sqL * ws1[0] + sqR * ws1[1] + sg * (cs1[1] - cs1[0])) * sden;
+                const double w2 = (sqL * ws2[0] + sqR * ws2[1] + sg * (cs2[1] - cs2[0])) * sden;
+                const double c1 = (sqL * cs1[1] + sqR * cs1[0] + sg * sqL * sqR * (ws1[1] - ws1[0])) * sden;
+                const double c2 = (sqL * cs2[1] + sqR * cs2[0] + sg * sqL * sqR * (ws2[1] - ws2[0])) * sden;
+                const double wcs = ws1[s] * cs1[s] + ws2[s] * cs2[s];
+                const double wcss = w1 * c1 + w2 * c2;
+                const double sq = s ? sqR : sqL;
+                Uss[2] = rs[s] * w1;
+                Uss[3] = rs[s] * w2;
+                Uss[4] = s ? es[s] + sg * sq * (wcs - wcss) : es[s] - sg * sq * (wcs - wcss);
+                Uss[6] = c1;
+                Uss[7] = c2;
+            }
+            const double Ss = s ? SRs : SLs;
+            for (int v = 0; v < 8; ++v) F[v] = Fk[s][v] + Ss * Uss[v] - (Ss - S) * Us[v] - S * Uk[s][v];
+        }
+    }
+    F[4] = F[4] + ch * bn * psn;
+    F[5] = ch * psn;
+    F[8] = ch * bn;
+}
+
 // LN_MEAN with the relative switch, source/equations/mhd/two_point/ec/two_point_flux_mod.f90:203-219
 inline double ln_mean_rel(double aL, double aR) {
     const double Xi = aR / aL;
@@ -558,8 +692,8 @@ void m_riemann(int kind, int d, const double* uL, const double* uR, double* F, c
     double rL[9], rR[9], rF[9];
     m_rot_in(d, uL, rL);
     m_rot_in(d, uR, rR);
-    (void)kind;
-    m_rusanov_x(rL, rR, rF, P);
+    if (kind == NEMO_SURFFLUX_HLLD) m_hlld_x(rL, rR, rF, P.kappa, P.ch);
+    else m_rusanov_x(rL, rR, rF, P);
     m_rot_out(d, rF, F);
 }
 
@@ -1307,8 +1441,9 @@ void or_mhd_flux(int d, const double* u, double* f, double kappa, double mu0, do
     m_xflux(r, rf, P);
     m_rot_out(d, rf, f);
 }
-void or_mhd_riemann(int d, const double* uL, const double* uR, double* F, double kappa, double mu0, double ch) {
-    m_riemann(NEMO_SURFFLUX_RUSANOV, d, uL, uR, F, MhdPar{kappa, mu0, ch});
+void or_mhd_riemann(int kind, int d, const double* uL, const double* uR, double* F, double kappa, double mu0,
+                    double ch) {
+    m_riemann(kind, d, uL, uR, F, MhdPar{kappa, mu0, ch});
 }
 void or_mhd_twopoint(int kind, int d, const double* u, const double* v, double* F, double kappa, double mu0, double ch) {
     m_twopoint(kind, d, u, v, F, MhdPar{kappa, mu0, ch});

@@ -62,7 +62,7 @@ def lib():
         L.or_exp.argtypes = [ctypes.c_double]
         L.or_set_mlp.argtypes = [_dp, _dp, _dp]
         L.or_mhd_flux.argtypes = [ctypes.c_int, _dp, _dp, ctypes.c_double, ctypes.c_double, ctypes.c_double]
-        L.or_mhd_riemann.argtypes = [ctypes.c_int, _dp, _dp, _dp, ctypes.c_double, ctypes.c_double, ctypes.c_double]
+        L.or_mhd_riemann.argtypes = [ctypes.c_int, ctypes.c_int, _dp, _dp, _dp, ctypes.c_double, ctypes.c_double, ctypes.c_double]
         L.or_mhd_twopoint.argtypes = [ctypes.c_int, ctypes.c_int, _dp, _dp, _dp, ctypes.c_double, ctypes.c_double,
                                       ctypes.c_double]
         L.or_mhd_nc.argtypes = [ctypes.c_int, _dp, _dp, _dp, _dp, ctypes.c_double, ctypes.c_double]
@@ -138,10 +138,11 @@ def mhd_flux(d, u, kappa=5 / 3, mu0=1.0, ch=0.0):
     return f
 
 
-def mhd_riemann(d, uL, uR, kappa=5 / 3, mu0=1.0, ch=0.0):
+def mhd_riemann(d, uL, uR, kappa=5 / 3, mu0=1.0, ch=0.0, kind=1):
+    """MHD surface flux in direction d: kind 1 Rusanov, 2 HLLD (mu0 = 1)."""
     uL, uR = _f64(uL), _f64(uR)
     f = np.zeros(9)
-    lib().or_mhd_riemann(d, _p(uL), _p(uR), _p(f), kappa, mu0, ch)
+    lib().or_mhd_riemann(kind, d, _p(uL), _p(uR), _p(f), kappa, mu0, ch)
     return f
 
 

@@ -32,12 +32,13 @@ def rel_linf(a, b):
     return max(np.max(np.abs(a[v] - b[v])) / max(np.max(np.abs(b[v])), 1e-300) for v in range(a.shape[0]))
 
 
-@pytest.mark.parametrize("vf", [abi.VOLFLUX_EC_MHD, abi.VOLFLUX_CENTRAL])
-def test_mhd_rhs_bit_exact(vf):
+@pytest.mark.parametrize("vf,sf", [(abi.VOLFLUX_EC_MHD, abi.SURFFLUX_RUSANOV), (abi.VOLFLUX_CENTRAL, abi.SURFFLUX_RUSANOV),
+                                   (abi.VOLFLUX_EC_MHD, abi.SURFFLUX_HLLD)])
+def test_mhd_rhs_bit_exact(vf, sf):
     m = mesh.brick(4)
     u = setups.orszag_tang(m)
     u[8] = 0.01 * np.sin(3.0 * u[0] * np.arange(m.E)[:, None])     # a nonzero psi field
-    c = mcfg(volume_flux=vf)
+    c = mcfg(volume_flux=vf, surface_flux=sf)
     s = Solver(c, m)
     s.upload(u)
     r = s.rhs()
@@ -57,10 +58,11 @@ def test_mhd_run_bit_exact_with_device_glm():
     assert np.array_equal(s.download(), uc)
 
 
-def test_mhd_blended_run_bit_exact():
+@pytest.mark.parametrize("sf", [abi.SURFFLUX_RUSANOV, abi.SURFFLUX_HLLD])
+def test_mhd_blended_run_bit_exact(sf):
     m = mesh.brick(4)
     u = setups.orszag_tang(m)
-    c = mcfg(indicator=abi.IND_MODAL, positivity=1)
+    c = mcfg(indicator=abi.IND_MODAL, positivity=1, surface_flux=sf)
     s = Solver(c, m)
     s.upload(u)
     o = orc.Oracle(c, m.neighbors(), m.delta)
@@ -70,10 +72,11 @@ def test_mhd_blended_run_bit_exact():
     assert np.array_equal(s.download(), uc)
 
 
-def test_mhd_fp32_form_close_to_oracle():
+@pytest.mark.parametrize("sf", [abi.SURFFLUX_RUSANOV, abi.SURFFLUX_HLLD])
+def test_mhd_fp32_form_close_to_oracle(sf):
     m = mesh.brick(8)
     u = setups.orszag_tang(m)
-    c = mcfg(precision=abi.PREC_FP32)
+    c = mcfg(precision=abi.PREC_FP32, surface_flux=sf)
     s = Solver(c, m)
     s.upload(u)
     o = orc.Oracle(c, m.neighbors(), m.delta)
@@ -85,3 +88,9 @@ def test_mhd_fp32_form_close_to_oracle():
     uc, tc, nc, _ = o.run(u, nsteps=10)
     got = s.download()
     assert np.sum(np.abs(got[0] - uc[0])) / np.sum(np.abs(uc[0])) < 1e-6
+
+
+def test_hlld_requires_unit_mu0():
+    m = mesh.brick(2)
+    with pytest.raises(abi.NemoError, match="mu0"):
+        Solver(mcfg(surface_flux=abi.SURFFLUX_HLLD, mu0=2.0), m)

@@ -96,3 +96,60 @@ def test_orszag_tang_short_run_stable_and_div_b_small():
     assert np.all(np.isfinite(u1)) and nbad == 0 and t > 0
     l2_1, _ = setups.divergence_b(m, u1, D, w)
     assert l2_1 < 0.5, (l2_0, l2_1)   # the GLM cleaning keeps the discrete divergence bounded
+
+
+HLLD = abi.SURFFLUX_HLLD
+
+
+@pytest.mark.parametrize("d", [0, 1, 2])
+def test_hlld_consistency(d):
+    rng = np.random.default_rng(20 + d)
+    for _ in range(50):
+        u = rand_mhd(rng)
+        np.testing.assert_allclose(orc.mhd_riemann(d, u, u, ch=0.7, kind=HLLD), orc.mhd_flux(d, u, ch=0.7),
+                                   rtol=1e-12, atol=1e-12)
+
+
+def test_hlld_mirror_symmetry():
+    """x -> -x maps (m_x, B_x) -> -(m_x, B_x); a symmetric numerical flux obeys
+    F(M uR, M uL) = S F(uL, uR) with S = diag(-1, 1, -1, -1, -1, 1, -1, -1, -1)."""
+    rng = np.random.default_rng(31)
+    M = np.array([1, -1, 1, 1, 1, -1, 1, 1, 1.0])
+    S = np.array([-1, 1, -1, -1, -1, 1, -1, -1, -1.0])
+    for _ in range(200):
+        uL, uR = rand_mhd(rng), rand_mhd(rng)
+        f = orc.mhd_riemann(0, uL, uR, ch=0.7, kind=HLLD)
+        g = orc.mhd_riemann(0, M * uR, M * uL, ch=0.7, kind=HLLD)
+        np.testing.assert_allclose(g, S * f, rtol=1e-11, atol=1e-12)
+
+
+@pytest.mark.parametrize("bx", [0.0, 0.8])
+def test_hlld_resolves_stationary_contact(bx):
+    """An isolated stationary contact (equal p, B, zero velocity, density jump) has zero mass and
+    energy flux under HLLD; Rusanov smears it."""
+    uL = setups.mhd_prim2cons(1.0, 0, 0, 0, 1.0, bx, 0.3, -0.2, 0.0, K, MU0)
+    uR = setups.mhd_prim2cons(0.2, 0, 0, 0, 1.0, bx, 0.3, -0.2, 0.0, K, MU0)
+    f = orc.mhd_riemann(0, uL, uR, kind=HLLD)
+    assert abs(f[0]) < 1e-14 and abs(f[4]) < 1e-14
+    pt = 1.0 + 0.5 * (bx * bx + 0.09 + 0.04)
+    assert abs(f[1] - (pt - bx * bx)) < 1e-13
+    assert abs(orc.mhd_riemann(0, uL, uR, kind=abi.SURFFLUX_RUSANOV)[0]) > 0.1
+
+
+def test_hlld_supersonic_upwinds():
+    """Both states moving right faster than the fast speed: the flux is the left state's flux."""
+    uL = setups.mhd_prim2cons(1.0, 5.0, 0.1, 0, 1.0, 0.3, 0.2, 0.1, 0.0, K, MU0)
+    uR = setups.mhd_prim2cons(0.5, 6.0, 0.0, 0, 0.8, 0.3, 0.1, 0.0, 0.0, K, MU0)
+    np.testing.assert_allclose(orc.mhd_riemann(0, uL, uR, ch=0.0, kind=HLLD), orc.mhd_flux(0, uL, ch=0.0),
+                               rtol=1e-13, atol=1e-13)
+
+
+def test_hlld_orszag_tang_run_stable():
+    m = mesh.brick(4)
+    u = setups.orszag_tang(m)
+    c = mhd_cfg(surface_flux=HLLD)
+    o = orc.Oracle(c, m.neighbors(), m.delta)
+    uc, t, n, _ = o.run(u, nsteps=20)
+    assert np.all(np.isfinite(uc)) and n == 20
+    tot0, tot1 = o.totals(u), o.totals(uc)
+    assert abs(tot1[0] - tot0[0]) < 1e-13 * abs(tot0[0])
