@@ -97,14 +97,26 @@ int nemo_gpu_init(const nemo_cfg* cfg);
 int nemo_gpu_operators(int32_t n, double* nodes, double* weights, double* dmat, double* smat,
                        double* vinv);
 
+/* 2:1 mortar matrices (kernel_operators_interpolationMatrix and _projectionMatrix with Q = 2,
+   source/kernel/dgsem/weakform/2d/kernel_operators_mod.f90:1010-1054, :1056-1100), computed on
+   the host without a GPU: prolong[2][n][n] (lower/upper half, [s][fine node][coarse node]) and
+   project[2][n][n] ([s][coarse node][fine node]); either pointer may be NULL. */
+int nemo_gpu_mortar_operators(int32_t n, double* prolong, double* project);
+
 /* Mesh in the reference's side form (source/mesh/p4est/mesh_types_mod.f90:57-77):
      delta[nelems*3], center[nelems*3]            element sizes and centres
      side_quads[nsides*2*4]                        0-based element ids, [side][iside][iquad]
      side_faceid[nsides*2]                         face id (0..5) of the side as seen by each element
      side_nquads[nsides*2]                         1, or 4 on the fine side of a 2:1 mortar, 0 at a boundary
      boundary[nsides]                              0 = interior, else 1 + face id of the domain face
-   The element order is the order of the state arrays.  Sides with nquads 4 on one side are
-   2:1 mortars; iquad runs over the fine elements in face-local (a,b) Morton order. */
+   The element order is the order of the state arrays.  Sides with nquads 4 on one half are
+   2:1 mortars (kernel_fill_faceflux, source/kernel/mcfv/3d/kernel_flux_mod.f90:100-118, 252-269):
+   iquad k = s + 2t runs over the fine elements, s = lower/upper half along the face's first
+   tangential axis (the lower-numbered of the two axes other than the face normal), t along the
+   second -- the rfaceMat/rfaceTam pairing of source/kernel/mcfv/3d/kernel_share_mod.f90:36-60.
+   All elements are axis-aligned in one frame (no tree rotations).  Each stage then runs a mortar
+   kernel before the stage kernel: coarse trace prolonged to the four sub-faces, Riemann flux on
+   every sub-face node, the fine faces take it and the coarse face takes its L2 projection. */
 int nemo_gpu_set_mesh(int64_t nelems, const double* delta, const double* center, int64_t nsides,
                       const int32_t* side_quads, const int8_t* side_faceid,
                       const int8_t* side_nquads, const int32_t* boundary);

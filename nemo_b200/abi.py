@@ -26,7 +26,7 @@ EXPORTS = [
     "nemo_gpu_alpha", "nemo_gpu_totals", "nemo_gpu_status", "nemo_gpu_finalize",
     "nemo_gpu_last_error", "nemo_gpu_set_timing", "nemo_gpu_kernel_timing", "nemo_gpu_stream",
     "nemo_gpu_totals_noalloc", "nemo_gpu_set_mlp", "nemo_gpu_features", "nemo_gpu_indicator_stats",
-    "nemo_gpu_mlp_train", "nemo_gpu_mlp_grad", "nemo_gpu_mlp_forward",
+    "nemo_gpu_mlp_train", "nemo_gpu_mlp_grad", "nemo_gpu_mlp_forward", "nemo_gpu_mortar_operators",
 ]
 
 
@@ -92,6 +92,7 @@ def load(path=LIB_PATH):
         "nemo_gpu_mlp_train": [vp, vp, i64, vp, ctypes.c_float, i32, i32, ctypes.c_float, ctypes.c_uint64, vp],
         "nemo_gpu_mlp_grad": [vp, vp, i64, vp, ctypes.c_float, vp, vp],
         "nemo_gpu_mlp_forward": [vp, i64, vp, ctypes.c_float, vp],
+        "nemo_gpu_mortar_operators": [i32, vp, vp],
     }
     for name, args in sig.items():
         f = getattr(L, name)
@@ -130,6 +131,13 @@ def operators():
     D, S, Vi = np.zeros((n, n)), np.zeros((n, n)), np.zeros((n, n))
     call("nemo_gpu_operators", n, x.ctypes.data, w.ctypes.data, D.ctypes.data, S.ctypes.data, Vi.ctypes.data)
     return x, w, D, S, Vi
+
+
+def mortar_operators():
+    """(prolongation [2,4,4], projection [2,4,4]) of the 2:1 mortar, lower/upper half."""
+    pro, prj = np.zeros((2, 4, 4)), np.zeros((2, 4, 4))
+    call("nemo_gpu_mortar_operators", 4, pro.ctypes.data, prj.ctypes.data)
+    return pro, prj
 
 
 def ptr(a):

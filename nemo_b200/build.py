@@ -22,6 +22,7 @@ SOURCES = {
     "stage_fp32.cu": ["--use_fast_math"],
     "noalloc.cu": ["-fmad=false"],
     "mlp.cu": ["--use_fast_math"],
+    "mortar.cu": ["-fmad=false"],
 }
 
 

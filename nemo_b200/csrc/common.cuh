@@ -56,6 +56,8 @@ struct OpConsts {
     double alpha_min, alpha_max, one_m_alpha_min;
     double repair_decr;
     double mu0;
+    double pro[2][NN * NN];  // 2:1 mortar prolongation to the lower/upper half, [s][fine i][coarse j]
+    double prj[2][NN * NN];  // 2:1 mortar projection from the lower/upper half, [s][coarse a][fine i]
 };
 
 __host__ __device__ inline int nidx(int i, int j, int k) { return i + NN * (j + NN * k); }

@@ -14,7 +14,7 @@ struct StageArgs {
     const double* u_in;       // [V][E][64]
     double* u_out;            // [V][E][64]
     double* reg;              // [V][E][64] LSRK register (FP64)
-    const int32_t* nbr;       // [E][6] conforming face neighbours, -1 domain boundary
+    const int32_t* nbr;       // [E][6] conforming face neighbours, -1 domain boundary, <= -2 mortar row -2-nbr
     const double* cdel;       // [E][3] 2/delta
     const double* delta;      // [E][3]
     const double* alpha_in;   // raw indicator of u_in [E] (blended runs)
@@ -34,7 +34,24 @@ struct StageArgs {
     const float* mlp32;       // same, FP32
     float* feat_out;          // FP32 form, prepare launches: indicator features [E][12] or null
     double* alpha_modal_out;  // FP32 form, prepare launches: modal alpha [E] or null
+    const double* mflux;      // [5 M][V][16] mortar face fluxes in the face's rotated frame (mortar.cu)
 };
+
+// 2:1 mortars (mortar.cu): per mortar, the coarse face flux (row 5m) and the four fine face fluxes
+// (rows 5m+1+k) of the state u_in, before the stage kernel that reads them.
+struct MortarArgs {
+    int64_t E;
+    int64_t nm;
+    const double* u_in;       // [V][E][64]
+    const int32_t* mortar;    // [nm][6]: coarse quad, coarse face, fine quads k = s + 2t
+    double* mflux;            // [5 nm][V][16]
+    const Control* ctrl;      // GLM cleaning speed (MHD); done flag
+    int32_t mhd;
+    int32_t surface_flux;
+    int32_t skip_if_done;     // stage launches: nothing to do once the run reached t_end
+};
+cudaError_t setup_mortar(const OpConsts& ops);
+cudaError_t launch_mortar(const MortarArgs& a, cudaStream_t s);
 
 // plain FP64 Euler path (stage_fp64.cu)
 cudaError_t setup_stage_euler64(const OpConsts& ops);

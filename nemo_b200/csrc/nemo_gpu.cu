@@ -133,7 +133,16 @@ void lu_inverse(int n, const double* A, double* C) {
 
 struct HostOps {
     double x[NN], w[NN], D[NN * NN], S[NN * NN], V[NN * NN], Vinv[NN * NN];
+    double pro[2][NN * NN], prj[2][NN * NN];
 };
+
+// Lagrange basis polynomial j of the nodes x at xi
+double lagrange_at(int n, const double* x, int j, double xi) {
+    double l = 1.0;
+    for (int m = 0; m < n; ++m)
+        if (m != j) l = l * ((xi - x[m]) / (x[j] - x[m]));
+    return l;
+}
 
 void build_host_ops(HostOps& h) {
     gl_nodes(NN - 1, h.x, h.w);
@@ -144,6 +153,17 @@ void build_host_ops(HostOps& h) {
     for (int i = 0; i < NN; ++i)
         for (int j = 0; j < NN; ++j) h.V[i * NN + j] = leg_norm(j, h.x[i]);
     lu_inverse(NN, h.V, h.Vinv);
+    // 2:1 mortar matrices with Q = 2 sub-faces (kernel_operators_interpolationMatrix and
+    // _projectionMatrix, source/kernel/dgsem/weakform/2d/kernel_operators_mod.f90:1010-1100):
+    // pro[s][i][j] = l_j(mu_s + x_i/2), prj[s][a][i] = l_a(mu_s + x_i/2) w_i / w_a / 2, mu = -+1/2
+    for (int s = 0; s < 2; ++s) {
+        const double mu = s ? 0.5 : -0.5;
+        for (int i = 0; i < NN; ++i)
+            for (int j = 0; j < NN; ++j) {
+                h.pro[s][i * NN + j] = lagrange_at(NN, h.x, j, mu + h.x[i] / 2.0);
+                h.prj[s][j * NN + i] = lagrange_at(NN, h.x, j, mu + h.x[i] / 2.0) * h.w[i] / h.w[j] / 2.0;
+            }
+    }
 }
 
 // ---- library state ----------------------------------------------------------------------------
@@ -167,6 +187,9 @@ struct Lib {
     double* alpha[2] = {nullptr, nullptr};
     double* alpha_used = nullptr;
     int32_t* nbr = nullptr;
+    int64_t nm = 0;               // 2:1 mortars
+    int32_t* mortar = nullptr;    // [nm][6]
+    double* mflux = nullptr;      // [5 nm][V][16]
     double* cdel = nullptr;
     double* delta = nullptr;
     int32_t* group = nullptr;
@@ -223,6 +246,8 @@ void release_mesh() {
     free_dev(g.u[0]); free_dev(g.u[1]); free_dev(g.reg); free_dev(g.stagebuf);
     free_dev(g.alpha[0]); free_dev(g.alpha[1]); free_dev(g.alpha_used);
     free_dev(g.nbr); free_dev(g.cdel); free_dev(g.delta); free_dev(g.group);
+    free_dev(g.mortar); free_dev(g.mflux);
+    g.mortar = nullptr; g.mflux = nullptr; g.nm = 0;
     free_dev(g.part);
     free_dev(g.feat_dev);
     g.feat_dev = nullptr;
@@ -262,12 +287,27 @@ StageArgs stage_args(int st, bool rhs_only) {
     a.mlp32 = learned ? g.mlp32 : nullptr;
     a.feat_out = nullptr;
     a.alpha_modal_out = nullptr;
+    a.mflux = g.mflux;
     return a;
 }
 
 bool is_mhd() { return g.cfg.eqn == NEMO_EQN_MHD; }
 
 cudaError_t launch_stage_any(const StageArgs& a, bool rhs_only, cudaStream_t s) {
+    if (g.nm > 0 && !a.prep_only) {  // fluxes of the 2:1 faces of u_in first
+        MortarArgs m{};
+        m.E = a.E;
+        m.nm = g.nm;
+        m.u_in = a.u_in;
+        m.mortar = g.mortar;
+        m.mflux = g.mflux;
+        m.ctrl = g.ctrl;
+        m.mhd = is_mhd() ? 1 : 0;
+        m.surface_flux = g.cfg.surface_flux;
+        m.skip_if_done = rhs_only ? 0 : 1;
+        cudaError_t e = launch_mortar(m, s);
+        if (e != cudaSuccess) return e;
+    }
     if (is_mhd()) {
         if (g.cfg.precision == NEMO_PREC_FP32) return launch_stage_mhd32(a, blended(), rhs_only, s);
         return launch_stage_mhd64(a, blended(), rhs_only, s);
@@ -369,6 +409,15 @@ int nemo_gpu_default_cfg(nemo_cfg* cfg) {
     return NEMO_OK;
 }
 
+int nemo_gpu_mortar_operators(int32_t n, double* prolong, double* project) {
+    if (n != NN) return fail(NEMO_ERR_ARG, "only n = %d Gauss-Lobatto nodes are compiled (got %d)", NN, n);
+    HostOps h;
+    build_host_ops(h);
+    if (prolong) std::memcpy(prolong, h.pro, sizeof h.pro);
+    if (project) std::memcpy(project, h.prj, sizeof h.prj);
+    return NEMO_OK;
+}
+
 int nemo_gpu_operators(int32_t n, double* nodes, double* weights, double* dmat, double* smat, double* vinv) {
     if (n != NN) return fail(NEMO_ERR_ARG, "only n = %d Gauss-Lobatto nodes are compiled (got %d)", NN, n);
     HostOps h;
@@ -432,11 +481,14 @@ int nemo_gpu_init(const nemo_cfg* cfg) {
     o.one_m_alpha_min = 1.0 - cfg->alpha_min;
     o.repair_decr = cfg->repair_decr;
     o.mu0 = cfg->mu0;
+    std::memcpy(o.pro, g.hops.pro, sizeof o.pro);
+    std::memcpy(o.prj, g.hops.prj, sizeof o.prj);
     CK(cudaStreamCreateWithFlags(&g.stream, cudaStreamNonBlocking));
     CK(setup_stage_euler64(o));
     CK(setup_stage_euler32(o));
     CK(setup_stage_mhd64());
     CK(setup_stage_mhd32());
+    CK(setup_mortar(o));
     CK(cudaMalloc(&g.ctrl, sizeof(Control)));
     CK(cudaMemset(g.ctrl, 0, sizeof(Control)));
     CK(cudaMalloc(&g.tot, 16 * sizeof(double)));
@@ -457,26 +509,52 @@ int nemo_gpu_set_mesh(int64_t nelems, const double* delta, const double* center,
         return fail(NEMO_ERR_ARG, "NULL mesh array");
     (void)center;
     const int64_t E = nelems;
-    std::vector<int32_t> nbr(E * 6, -2);
+    constexpr int32_t UNSET = INT32_MIN;
+    std::vector<int32_t> nbr(E * 6, UNSET);
+    std::vector<int32_t> mort;
     for (int64_t s = 0; s < nsides; ++s) {
         const int n0 = side_nquads[s * 2 + 0], n1 = side_nquads[s * 2 + 1];
         const int f0 = side_faceid[s * 2 + 0], f1 = side_faceid[s * 2 + 1];
-        const int32_t q0 = side_quads[s * 8 + 0], q1 = side_quads[s * 8 + 4];
-        if (n0 > 1 || n1 > 1) return fail(NEMO_ERR_ARG, "side %lld: 2:1 mortar sides are not supported by this build", (long long)s);
+        const int32_t* q0 = side_quads + s * 8;
+        const int32_t* q1 = side_quads + s * 8 + 4;
+        auto bad_quad = [&](int32_t q, int f) { return f < 0 || f > 5 || q < 0 || q >= E; };
+        if (n0 == 4 || n1 == 4) {  // 2:1 mortar: one coarse quad, four fine quads
+            if (!((n0 == 1 && n1 == 4) || (n0 == 4 && n1 == 1)) || boundary[s] > 0)
+                return fail(NEMO_ERR_ARG, "side %lld: a mortar side joins 1 and 4 quads in the interior", (long long)s);
+            const bool c0 = n0 == 1;
+            const int32_t* qc = c0 ? q0 : q1;
+            const int32_t* qf = c0 ? q1 : q0;
+            const int fc = c0 ? f0 : f1, ff = c0 ? f1 : f0;
+            if ((fc >> 1) != (ff >> 1) || fc == ff)
+                return fail(NEMO_ERR_ARG, "side %lld: faces %d/%d are not opposite faces of one direction", (long long)s, fc, ff);
+            if (bad_quad(qc[0], fc)) return fail(NEMO_ERR_ARG, "side %lld: bad coarse quad", (long long)s);
+            const int32_t m = (int32_t)(mort.size() / 6);
+            if ((int64_t)m * 5 + 5 > (int64_t)INT32_MAX - 2) return fail(NEMO_ERR_ARG, "too many mortars");
+            mort.push_back(qc[0]);
+            mort.push_back(fc);
+            nbr[qc[0] * 6 + fc] = -2 - 5 * m;
+            for (int k = 0; k < 4; ++k) {
+                if (bad_quad(qf[k], ff)) return fail(NEMO_ERR_ARG, "side %lld: bad fine quad %d", (long long)s, k);
+                mort.push_back(qf[k]);
+                nbr[qf[k] * 6 + ff] = -2 - (5 * m + 1 + k);
+            }
+            continue;
+        }
         if (n0 != 1) return fail(NEMO_ERR_ARG, "side %lld: first half must hold one element", (long long)s);
-        if (f0 < 0 || f0 > 5 || q0 < 0 || q0 >= E) return fail(NEMO_ERR_ARG, "side %lld: bad element/face", (long long)s);
+        if (bad_quad(q0[0], f0)) return fail(NEMO_ERR_ARG, "side %lld: bad element/face", (long long)s);
         if (n1 == 0 || boundary[s] > 0) {
-            nbr[q0 * 6 + f0] = -1;
+            nbr[q0[0] * 6 + f0] = -1;
         } else {
-            if (f1 < 0 || f1 > 5 || q1 < 0 || q1 >= E) return fail(NEMO_ERR_ARG, "side %lld: bad element/face", (long long)s);
+            if (n1 != 1 || bad_quad(q1[0], f1)) return fail(NEMO_ERR_ARG, "side %lld: bad element/face", (long long)s);
             if ((f0 >> 1) != (f1 >> 1) || f0 == f1)
                 return fail(NEMO_ERR_ARG, "side %lld: faces %d/%d are not opposite faces of one direction", (long long)s, f0, f1);
-            nbr[q0 * 6 + f0] = q1;
-            nbr[q1 * 6 + f1] = q0;
+            nbr[q0[0] * 6 + f0] = q1[0];
+            nbr[q1[0] * 6 + f1] = q0[0];
         }
     }
     for (int64_t i = 0; i < E * 6; ++i)
-        if (nbr[i] == -2) return fail(NEMO_ERR_ARG, "element %lld face %d has no side", (long long)(i / 6), (int)(i % 6));
+        if (nbr[i] == UNSET) return fail(NEMO_ERR_ARG, "element %lld face %d has no side", (long long)(i / 6), (int)(i % 6));
+    const int64_t nm = (int64_t)(mort.size() / 6);
     std::vector<double> cd(E * 3);
     for (int64_t i = 0; i < E * 3; ++i) {
         if (!(delta[i] > 0.0)) return fail(NEMO_ERR_ARG, "element %lld has non-positive size", (long long)(i / 3));
@@ -502,6 +580,13 @@ int nemo_gpu_set_mesh(int64_t nelems, const double* delta, const double* center,
     CK(cudaMemcpy(g.nbr, nbr.data(), sizeof(int32_t) * E * 6, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(g.cdel, cd.data(), sizeof(double) * E * 3, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(g.delta, delta, sizeof(double) * E * 3, cudaMemcpyHostToDevice));
+    g.nm = nm;
+    if (nm > 0) {
+        CK(cudaMalloc(&g.mortar, sizeof(int32_t) * 6 * nm));
+        CK(cudaMemcpy(g.mortar, mort.data(), sizeof(int32_t) * 6 * nm, cudaMemcpyHostToDevice));
+        CK(cudaMalloc(&g.mflux, sizeof(double) * 5 * nm * g.V * NF));
+        CK(cudaMemset(g.mflux, 0, sizeof(double) * 5 * nm * g.V * NF));
+    }
     g.ngroups = 1;
     Control c{};
     c.ngroups = 1;
@@ -676,6 +761,7 @@ int nemo_gpu_run(int64_t nsteps, double t_end, double* t_out, int64_t* steps_out
             g.n_total += 1;
         }
         for (auto& ev : evs) cudaEventDestroy(ev);
+        if (g.nm > 0) g.n_total += 5 * nsteps;  // mortar launches, timed inside their stage interval
         issued = nsteps;
     } else {
         for (int s = 0; s < 2; ++s)

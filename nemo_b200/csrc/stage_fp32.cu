@@ -553,6 +553,12 @@ __global__ void __launch_bounds__(NT, 3) k_stage_euler32(StageArgs a) {
                 const P32 qo = prim(side ? NN - 1 : 0);
                 P32 qn = qo;
                 const int32_t ne = a.nbr[e * 6 + f];
+                if (ne <= -2) {  // 2:1 mortar face: flux row of the mortar kernel (FP64)
+                    const double* mf = a.mflux + (int64_t)(-2 - ne) * V * NF + ab;
+#pragma unroll
+                    for (int v = 0; v < V; ++v) Fs[side][v] = (float)mf[v * NF];
+                    continue;
+                }
                 if (ne >= 0) {
                     const int nn = line_node(d, la, lb, side ? 0 : NN - 1);
                     const int64_t nl = (int64_t)ne - e0;

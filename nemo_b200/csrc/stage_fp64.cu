@@ -365,6 +365,12 @@ __global__ void __launch_bounds__(NT, 1) k_stage_euler64(StageArgs a) {
             uo[3] = su[((1 + c2) * EPC + el) * NP + own];
             uo[4] = su[(4 * EPC + el) * NP + own];
             const int32_t ne = a.nbr[e * 6 + f];
+            if (ne <= -2) {  // 2:1 mortar face: flux row of the mortar kernel
+                const double* mf = a.mflux + (int64_t)(-2 - ne) * V * NF + ab;
+#pragma unroll
+                for (int v = 0; v < V; ++v) Fs[side][v] = mf[v * NF];
+                continue;
+            }
             if (ne >= 0) {
                 const int nn = line_node(d, la, lb, side ? 0 : NN - 1);
                 const int64_t nl = (int64_t)ne - e0;

@@ -371,6 +371,12 @@ __global__ void __launch_bounds__(mhd::NT, 1) k_stage_mhd(StageArgs a) {
                 R uo[MV], un[MV], F[MV], G[MV];
                 load_rot(su, el, idx[side ? NN - 1 : 0], d, uo);
                 const int32_t ne = a.nbr[e * 6 + f];
+                if (ne <= -2) {  // 2:1 mortar face: flux row (incl. the own-side NC term) of the mortar kernel
+                    const double* mf = a.mflux + (int64_t)(-2 - ne) * MV * NF + ab;
+#pragma unroll
+                    for (int v = 0; v < MV; ++v) Fs[side][v] = (R)mf[v * NF];
+                    continue;
+                }
                 if (ne >= 0) {
                     const int nn = line_node(d, la, lb, side ? 0 : NN - 1);
                     const int64_t nl = (int64_t)ne - e0;

@@ -41,21 +41,39 @@ class Mesh:
         self.S = self.side_quads.shape[0]
         self.level = level if level is not None else np.zeros(self.E, dtype=np.int8)
 
+    def _mortar_sides(self):
+        return np.nonzero((self.side_nquads == 4).any(axis=1))[0]
+
+    def mortars(self):
+        """2:1 mortars [M,6] = (coarse quad, coarse face, fine quads 0..3) in side order; fine quad
+        k = s + 2 t sits at half s of the face's first tangential axis and half t of the second."""
+        sel = self._mortar_sides()
+        out = np.empty((len(sel), 6), dtype=np.int32)
+        for m, s in enumerate(sel):
+            c = 0 if self.side_nquads[s, 0] == 1 else 1
+            out[m, 0] = self.side_quads[s, c, 0]
+            out[m, 1] = self.side_faceid[s, c]
+            out[m, 2:] = self.side_quads[s, 1 - c, :]
+        return out
+
     def neighbors(self):
-        """Conforming face neighbours [E,6] (-1 at a domain boundary); raises on mortars."""
-        nbr = np.full((self.E, 6), -2, dtype=np.int32)
-        for s in range(self.S):
-            nq = self.side_nquads[s]
-            if nq[0] > 1 or nq[1] > 1:
-                raise ValueError("neighbors(): mesh has non-conforming sides")
-            q0, q1 = self.side_quads[s, 0, 0], self.side_quads[s, 1, 0]
-            f0, f1 = int(self.side_faceid[s, 0]), int(self.side_faceid[s, 1])
-            if nq[1] == 0:
-                nbr[q0, f0] = -1
-            else:
-                nbr[q0, f0] = q1
-                nbr[q1, f1] = q0
-        if (nbr == -2).any():
+        """Face neighbours [E,6]: the conforming neighbour, -1 at a domain boundary, and for a face on
+        a 2:1 mortar -2 - slot, where slot = 5 m for the coarse face of mortar m (in side order) and
+        5 m + 1 + k for its fine quad k -- the row of that face's flux in the mortar flux buffer."""
+        nbr = np.full((self.E, 6), np.iinfo(np.int32).min, dtype=np.int32)
+        conf = (self.side_nquads[:, 0] == 1) & (self.side_nquads[:, 1] == 1) & (self.boundary == 0)
+        q0, q1 = self.side_quads[conf, 0, 0], self.side_quads[conf, 1, 0]
+        f0, f1 = self.side_faceid[conf, 0].astype(np.int64), self.side_faceid[conf, 1].astype(np.int64)
+        nbr[q0, f0] = q1
+        nbr[q1, f1] = q0
+        bnd = (self.side_nquads[:, 1] == 0) | ((self.boundary > 0) & (self.side_nquads[:, 0] == 1))
+        nbr[self.side_quads[bnd, 0, 0], self.side_faceid[bnd, 0].astype(np.int64)] = -1
+        for m, s in enumerate(self._mortar_sides()):
+            c = 0 if self.side_nquads[s, 0] == 1 else 1
+            nbr[self.side_quads[s, c, 0], self.side_faceid[s, c]] = -2 - 5 * m
+            for k in range(4):
+                nbr[self.side_quads[s, 1 - c, k], self.side_faceid[s, 1 - c]] = -2 - (5 * m + 1 + k)
+        if (nbr == np.iinfo(np.int32).min).any():
             raise ValueError("neighbors(): element face without a side")
         return nbr
 
@@ -125,3 +143,140 @@ def ensemble(members, nx):
                 np.tile(one.boundary, members))
     groups = np.repeat(np.arange(members, dtype=np.int32), E1)
     return mesh, groups
+
+
+def forest(nb, refine, max_level=2, lo=(0.0, 0.0, 0.0), hi=(1.0, 1.0, 1.0)):
+    """Statically refined periodic forest on an nb^3 base brick (one octree per base element).
+
+    refine(level, center[n,3], size[n]) -> bool[n] marks leaves of that level to split into 8; it is
+    called for level 0, 1, ..., max_level-1 in turn.  The forest is then 2:1 face-balanced (a leaf whose
+    face neighbour is two or more levels finer is split, repeatedly), the leaves are put in Morton order
+    of their anchors on the finest grid (the p4est order), and the sides are built: conforming sides as
+    in brick(), and one side per 2:1 non-conforming face with the coarse quad on one half and the four
+    fine quads (k = s + 2 t over the face's two tangential axes, lower axis first) on the other."""
+    lo, hi = np.asarray(lo, float), np.asarray(hi, float)
+    nf = nb << max_level
+    g = np.stack(np.meshgrid(np.arange(nb), np.arange(nb), np.arange(nb), indexing="ij"), -1).reshape(-1, 3)
+    lev = np.zeros(len(g), dtype=np.int64)
+    crd = g.astype(np.int64)
+
+    def split(mask):
+        nonlocal lev, crd
+        kids = np.stack(np.meshgrid([0, 1], [0, 1], [0, 1], indexing="ij"), -1).reshape(8, 3)
+        c2 = (2 * crd[mask][:, None, :] + kids[None]).reshape(-1, 3)
+        l2 = np.repeat(lev[mask] + 1, 8)
+        lev = np.concatenate([lev[~mask], l2])
+        crd = np.concatenate([crd[~mask], c2])
+
+    def geometry():
+        size = (hi - lo)[None, :] / (nb << lev)[:, None]
+        return lo + (crd + 0.5) * size, size
+
+    for level in range(max_level):
+        at = lev == level
+        if not at.any():
+            continue
+        cen, size = geometry()
+        mask = np.zeros(len(lev), dtype=bool)
+        mask[at] = np.asarray(refine(level, cen[at], size[at]), dtype=bool)
+        if mask.any():
+            split(mask)
+
+    # 2:1 face balance on the finest grid: owner level per finest cell, neighbour maximum per leaf
+    while True:
+        span = 1 << (max_level - lev)
+        levgrid = np.empty((nf, nf, nf), dtype=np.int64)
+        owner = np.empty((nf, nf, nf), dtype=np.int64)
+        for i in range(len(lev)):
+            a = crd[i] * span[i]
+            levgrid[a[0]:a[0] + span[i], a[1]:a[1] + span[i], a[2]:a[2] + span[i]] = lev[i]
+            owner[a[0]:a[0] + span[i], a[1]:a[1] + span[i], a[2]:a[2] + span[i]] = i
+        nbmax = levgrid.copy()
+        for d in range(3):
+            for sh in (1, -1):
+                nbmax = np.maximum(nbmax, np.roll(levgrid, sh, axis=d))
+        leafmax = np.zeros(len(lev), dtype=np.int64)
+        np.maximum.at(leafmax, owner.ravel(), nbmax.ravel())
+        bad = leafmax > lev + 1
+        if not bad.any():
+            break
+        split(bad)
+
+    anchor = crd << (max_level - lev)[:, None]
+    order = np.argsort(morton3(anchor[:, 0], anchor[:, 1], anchor[:, 2]), kind="stable")
+    lev, crd = lev[order], crd[order]
+    E = len(lev)
+    cen, size = geometry()
+
+    key_scale = np.int64(nf)
+    def key(l, c):
+        return ((l * key_scale + c[:, 0]) * key_scale + c[:, 1]) * key_scale + c[:, 2]
+
+    keys = key(lev, crd)
+    srt = np.argsort(keys)
+    skeys = keys[srt]
+
+    def find(l, c):
+        n_l = nb << l
+        c = np.mod(c, n_l[:, None])
+        k = key(l, c)
+        pos = np.searchsorted(skeys, k)
+        pos = np.minimum(pos, len(skeys) - 1)
+        hit = skeys[pos] == k
+        return np.where(hit, srt[pos], -1)
+
+    Q, F, NQ = [], [], []
+    eidx = np.arange(E)
+    for d in range(3):
+        t1, t2 = [a for a in range(3) if a != d]
+        unit = np.zeros(3, dtype=np.int64)
+        unit[d] = 1
+        # + side: conforming or finer neighbour
+        nbc = find(lev, crd + unit)
+        conf = nbc >= 0
+        q = np.full((conf.sum(), 2, 4), -1, dtype=np.int32)
+        q[:, 0, 0], q[:, 1, 0] = eidx[conf], nbc[conf]
+        Q.append(q); F.append(np.tile([2 * d + 1, 2 * d], (len(q), 1))); NQ.append(np.tile([1, 1], (len(q), 1)))
+        for sign in (1, -1):
+            base = 2 * (crd + sign * unit)
+            if sign == -1:
+                base[:, d] += 1
+            kids = []
+            for k in range(4):
+                off = np.zeros(3, dtype=np.int64)
+                off[t1], off[t2] = k & 1, k >> 1
+                kids.append(find(lev + 1, base + off))
+            kids = np.stack(kids, 1)
+            fine = (kids >= 0).all(axis=1) & (lev < max_level)
+            if sign == 1:
+                fine &= ~conf
+            sel = np.nonzero(fine)[0]
+            q = np.full((len(sel), 2, 4), -1, dtype=np.int32)
+            if sign == 1:   # coarse on the minus half, fine quads see their minus face
+                q[:, 0, 0] = sel
+                q[:, 1, :] = kids[sel]
+                F.append(np.tile([2 * d + 1, 2 * d], (len(sel), 1))); NQ.append(np.tile([1, 4], (len(sel), 1)))
+            else:           # fine quads on the minus half, coarse sees its minus face
+                q[:, 0, :] = kids[sel]
+                q[:, 1, 0] = sel
+                F.append(np.tile([2 * d + 1, 2 * d], (len(sel), 1))); NQ.append(np.tile([4, 1], (len(sel), 1)))
+            Q.append(q)
+    quads, fids, nqs = np.concatenate(Q), np.concatenate(F), np.concatenate(NQ)
+    mesh = Mesh(size, cen, quads, fids, nqs, np.zeros(len(quads), dtype=np.int32), level=lev.astype(np.int8))
+    return mesh
+
+
+def kh_forest(nb=24, max_level=2, seed=7, band=(0.06, 0.05)):
+    """Forest for the Kelvin-Helmholtz layer on [-1,1]^3 (shear interfaces at y = +-0.25): leaves
+    whose centre lies within band[level] of the seeded, sinusoidally displaced interface are split --
+    the finite-difference |grad rho| of the layer exceeds the threshold there."""
+    rng = np.random.default_rng(seed)
+    kx, kz = rng.integers(1, 4, size=2)
+    ph = rng.uniform(0, 2 * np.pi, size=2)
+
+    def refine(level, c, size):
+        shift = 0.02 * np.sin(np.pi * kx * c[:, 0] + ph[0]) * np.sin(np.pi * kz * c[:, 2] + ph[1])
+        dist = np.abs(np.abs(c[:, 1] - shift) - 0.25)
+        return dist < band[min(level, len(band) - 1)] + 0.5 * size[:, 1]
+
+    return forest(nb, refine, max_level=max_level, lo=(-1.0,) * 3, hi=(1.0,) * 3)

@@ -40,6 +40,7 @@ namespace {
 
 constexpr int NN = 4;            // nodes per direction (N = 3)
 constexpr int NP = NN * NN * NN; // nodes per element
+constexpr int NF = NN * NN;
 constexpr int VMAX = 9;
 
 // ------------------------------------------------------------------------------------------
@@ -159,7 +160,17 @@ void invert_lu(int n, const double* A /*row-major*/, double* C) {
 struct Ops {
     double x[NN], w[NN], winv[NN];
     double D[NN * NN], S[NN * NN], V[NN * NN], Vinv[NN * NN];
+    double pro[2][NN * NN];  // mortar prolongation to the lower/upper half: pro[s][i][j] = l_j(x_i/2 -+ 1/2)
+    double prj[2][NN * NN];  // mortar projection from the lower/upper half: prj[s][a][i] = l_a(..) w_i/w_a/2
 };
+
+// Lagrange basis polynomial j of the nodes x at xi
+double lagrange(int n, const double* x, int j, double xi) {
+    double l = 1.0;
+    for (int m = 0; m < n; ++m)
+        if (m != j) l = l * ((xi - x[m]) / (x[j] - x[m]));
+    return l;
+}
 
 void build_ops(Ops& op) {
     lgl_nodes(NN - 1, op.x, op.w);
@@ -174,6 +185,16 @@ void build_ops(Ops& op) {
     for (int i = 0; i < NN; ++i)
         for (int j = 0; j < NN; ++j) op.V[i * NN + j] = legendre_normalised(j, op.x[i]);
     invert_lu(NN, op.V, op.Vinv);
+    // kernel_operators_interpolationMatrix / _projectionMatrix with Q = 2 sub-elements,
+    // source/kernel/dgsem/weakform/2d/kernel_operators_mod.f90:1010-1054, :1056-1100
+    for (int s = 0; s < 2; ++s) {
+        const double mu = s ? 0.5 : -0.5;
+        for (int i = 0; i < NN; ++i)
+            for (int j = 0; j < NN; ++j) {
+                op.pro[s][i * NN + j] = lagrange(NN, op.x, j, mu + op.x[i] / 2.0);
+                op.prj[s][j * NN + i] = lagrange(NN, op.x, j, mu + op.x[i] / 2.0) * op.w[i] / op.w[j] / 2.0;
+            }
+    }
 }
 
 
@@ -730,9 +751,14 @@ inline int face_node(int f, int a, int b) {
 
 struct Mesh {
     int64_t E;
-    const int32_t* nbr;    // [E][6], -1 = domain boundary (mirrored state)
+    const int32_t* nbr;    // [E][6], -1 = domain boundary (mirrored state), <= -2: mortar flux row -2-nbr
     const double* delta;   // [E][3]
+    int64_t nm = 0;                  // 2:1 mortars
+    const int32_t* mortar = nullptr; // [nm][6]: coarse quad, coarse face, fine quads k = s + 2t
+    double* mflux = nullptr;         // [5 nm][NN*NN][VMAX] face fluxes (coarse row 5m, fine k row 5m+1+k)
 };
+
+std::vector<int32_t> g_mortar;  // mortar table of the current mesh (or_set_mortars)
 
 struct Ctx {
     Ops op;
@@ -925,6 +951,12 @@ void element_rhs(const Ctx& c, const Mesh& M, const double* u, int64_t e, double
     for (int f = 0; f < 6; ++f) {
         int d = f >> 1, plus = f & 1;
         int64_t ne = M.nbr[e * 6 + f];
+        if (ne <= -2) {  // 2:1 mortar face: flux of mortar_fluxes
+            const double* mf = M.mflux + (size_t)(-2 - ne) * NF * VMAX;
+            for (int ab = 0; ab < NF; ++ab)
+                for (int v = 0; v < V; ++v) fs[f][ab][v] = mf[ab * VMAX + v];
+            continue;
+        }
         for (int b = 0; b < NN; ++b)
             for (int a = 0; a < NN; ++a) {
                 int own = face_node(f, a, b);
@@ -1032,6 +1064,12 @@ void mhd_element_rhs(const Ctx& c, const Mesh& M, const double* u, int64_t e, do
     for (int f = 0; f < 6; ++f) {
         const int d = f >> 1, plus = f & 1;
         const int64_t ne = M.nbr[e * 6 + f];
+        if (ne <= -2) {  // 2:1 mortar face: flux (incl. the non-conservative term) of mortar_fluxes
+            const double* mf = M.mflux + (size_t)(-2 - ne) * NF * VMAX;
+            for (int ab = 0; ab < NF; ++ab)
+                for (int v = 0; v < V; ++v) fs[f][ab][v] = mf[ab * VMAX + v];
+            continue;
+        }
         for (int b = 0; b < NN; ++b)
             for (int a = 0; a < NN; ++a) {
                 const int own = face_node(f, a, b);
@@ -1201,6 +1239,86 @@ Ctx make_ctx(const nemo_cfg* cfg) {
     return c;
 }
 
+// 2:1 mortar fluxes (the mortar part of kernel_fill_faceflux, source/kernel/mcfv/3d/kernel_flux_mod.f90:
+// 100-118 and 252-269, with the DG interpolation/projection matrices): the coarse face trace is
+// prolonged to the four sub-faces, the Riemann flux is evaluated on every sub-face node against the
+// fine quad's trace (plus, for MHD, each side's own non-conservative term), the fine quads take it as
+// is and the coarse face takes the projection of the four sub-face fluxes.
+void mortar_fluxes(const Ctx& c, const Mesh& M, const double* u, int nthreads) {
+    const Ops& op = c.op;
+    const int V = c.V;
+    const MhdPar P = c.mp();
+#pragma omp parallel for schedule(static) num_threads(nthreads)
+    for (int64_t m = 0; m < M.nm; ++m) {
+        const int32_t* t = M.mortar + 6 * m;
+        const int64_t qc = t[0];
+        const int fc = t[1], ff = fc ^ 1, d = fc >> 1;
+        const bool coarse_left = (fc & 1) != 0;
+        double uc[NF][VMAX], fsub[4][NF][VMAX];
+        for (int b = 0; b < NN; ++b)
+            for (int a = 0; a < NN; ++a)
+                for (int v = 0; v < V; ++v) uc[a + NN * b][v] = u[(v * M.E + qc) * NP + face_node(fc, a, b)];
+        for (int k = 0; k < 4; ++k) {
+            const int s = k & 1, tt = k >> 1;
+            const int64_t qf = t[2 + k];
+            double* mf = M.mflux + (size_t)(5 * m + 1 + k) * NF * VMAX;
+            for (int j = 0; j < NN; ++j)
+                for (int i = 0; i < NN; ++i) {
+                    double up[VMAX], uf[VMAX], F[VMAX], Gf[VMAX], Gc[VMAX];
+                    for (int v = 0; v < V; ++v) {
+                        double acc = 0.0;
+                        for (int bb = 0; bb < NN; ++bb) {
+                            double in = 0.0;
+                            for (int aa = 0; aa < NN; ++aa) in = in + op.pro[s][i * NN + aa] * uc[aa + NN * bb][v];
+                            acc = acc + op.pro[tt][j * NN + bb] * in;
+                        }
+                        up[v] = acc;
+                        uf[v] = u[(v * M.E + qf) * NP + face_node(ff, i, j)];
+                    }
+                    const double* uL = coarse_left ? up : uf;
+                    const double* uR = coarse_left ? uf : up;
+                    if (c.mhd()) {
+                        m_riemann(c.cfg.surface_flux, d, uL, uR, F, P);
+                        m_nc(d, uf, uL, uR, Gf, P);
+                        m_nc(d, up, uL, uR, Gc, P);
+                        for (int v = 0; v < V; ++v) {
+                            mf[(i + NN * j) * VMAX + v] = F[v] + Gf[v];
+                            fsub[k][i + NN * j][v] = F[v] + Gc[v];
+                        }
+                    } else {
+                        e_riemann(c.cfg.surface_flux, d, uL, uR, F, c.cfg.kappa);
+                        for (int v = 0; v < V; ++v) {
+                            mf[(i + NN * j) * VMAX + v] = F[v];
+                            fsub[k][i + NN * j][v] = F[v];
+                        }
+                    }
+                }
+        }
+        double* mc = M.mflux + (size_t)(5 * m) * NF * VMAX;
+        for (int b = 0; b < NN; ++b)
+            for (int a = 0; a < NN; ++a)
+                for (int v = 0; v < V; ++v) {
+                    double acc = 0.0;
+                    for (int tt = 0; tt < 2; ++tt)
+                        for (int s = 0; s < 2; ++s)
+                            for (int j = 0; j < NN; ++j) {
+                                double in = 0.0;
+                                for (int i = 0; i < NN; ++i)
+                                    in = in + op.prj[s][a * NN + i] * fsub[s + 2 * tt][i + NN * j][v];
+                                acc = acc + op.prj[tt][b * NN + j] * in;
+                            }
+                    mc[(a + NN * b) * VMAX + v] = acc;
+                }
+    }
+}
+
+Mesh make_mesh(int64_t E, const int32_t* nbr, const double* delta) {
+    Mesh M{E, nbr, delta};
+    M.nm = (int64_t)(g_mortar.size() / 6);
+    M.mortar = g_mortar.data();
+    return M;
+}
+
 void compute_alpha(const Ctx& c, const Mesh& M, const double* u, double* alpha, int nthreads) {
     if (c.cfg.indicator == NEMO_IND_NONE) {
         for (int64_t e = 0; e < M.E; ++e) alpha[e] = 0.0;
@@ -1249,6 +1367,19 @@ void or_operators(double* x, double* w, double* D, double* S, double* Vinv) {
 
 void or_lgl(int N, double* x, double* w) { lgl_nodes(N, x, w); }
 
+// mortar prolongation and projection matrices [2][NN][NN] each
+void or_mortar_operators(double* pro, double* prj) {
+    Ops op;
+    build_ops(op);
+    std::memcpy(pro, op.pro, sizeof op.pro);
+    std::memcpy(prj, op.prj, sizeof op.prj);
+}
+
+// mortar table [nm][6] of the mesh that the following calls use (nm = 0: conforming mesh)
+void or_set_mortars(int64_t nm, const int32_t* table) {
+    g_mortar.assign(table, table + 6 * nm);
+}
+
 void or_rk_coeffs(double* a, double* b, double* c) {
     for (int k = 0; k < 5; ++k) { a[k] = RK_A[k]; b[k] = RK_B[k]; c[k] = RK_C[k]; }
 }
@@ -1276,7 +1407,7 @@ void or_twopoint(int kind, int d, const double* u, const double* v, double* F, d
 void or_alpha(const nemo_cfg* cfg, int64_t E, const int32_t* nbr, const double* delta, const double* u,
               double* alpha, int nthreads) {
     Ctx c = make_ctx(cfg);
-    Mesh M{E, nbr, delta};
+    Mesh M = make_mesh(E, nbr, delta);
     compute_alpha(c, M, u, alpha, nthreads);
 }
 
@@ -1284,10 +1415,12 @@ void or_alpha(const nemo_cfg* cfg, int64_t E, const int32_t* nbr, const double* 
 void or_rhs(const nemo_cfg* cfg, int64_t E, const int32_t* nbr, const double* delta, const double* u,
             const double* alpha_in, double* rhs, int nthreads) {
     Ctx c = make_ctx(cfg);
-    Mesh M{E, nbr, delta};
-    std::vector<double> alpha(E);
+    Mesh M = make_mesh(E, nbr, delta);
+    std::vector<double> alpha(E), mflux((size_t)5 * M.nm * NF * VMAX);
+    M.mflux = mflux.data();
     if (alpha_in) std::memcpy(alpha.data(), alpha_in, sizeof(double) * E);
     else compute_alpha(c, M, u, alpha.data(), nthreads);
+    mortar_fluxes(c, M, u, nthreads);
 #pragma omp parallel for schedule(dynamic, 16) num_threads(nthreads)
     for (int64_t e = 0; e < E; ++e) {
         if (c.mhd()) mhd_element_rhs(c, M, u, e, alpha[e], rhs);
@@ -1344,10 +1477,12 @@ double or_timestep(const nemo_cfg* cfg, int64_t E, const double* delta, const do
 int64_t or_stage(const nemo_cfg* cfg, int64_t E, const int32_t* nbr, const double* delta, int stage, double dt,
                  double* u, double* reg, int nthreads) {
     Ctx c = make_ctx(cfg);
-    Mesh M{E, nbr, delta};
+    Mesh M = make_mesh(E, nbr, delta);
     const int V = c.V;
-    std::vector<double> rhs((size_t)V * E * NP), alpha(E);
+    std::vector<double> rhs((size_t)V * E * NP), alpha(E), mflux((size_t)5 * M.nm * NF * VMAX);
+    M.mflux = mflux.data();
     compute_alpha(c, M, u, alpha.data(), nthreads);
+    mortar_fluxes(c, M, u, nthreads);
 #pragma omp parallel for schedule(dynamic, 16) num_threads(nthreads)
     for (int64_t e = 0; e < E; ++e) {
         if (c.mhd()) mhd_element_rhs(c, M, u, e, alpha[e], rhs.data());

@@ -42,6 +42,8 @@ def lib():
         L.or_twopoint.argtypes = [ctypes.c_int, ctypes.c_int, _dp, _dp, _dp, ctypes.c_double]
         L.or_lgl.argtypes = [ctypes.c_int, _dp, _dp]
         L.or_operators.argtypes = [_dp] * 5
+        L.or_mortar_operators.argtypes = [_dp, _dp]
+        L.or_set_mortars.argtypes = [ctypes.c_int64, ctypes.c_void_p]
         L.or_rk_coeffs.argtypes = [_dp] * 3
         L.or_alpha.argtypes = [ctypes.c_void_p, ctypes.c_int64, _ip, _dp, _dp, _dp, ctypes.c_int]
         L.or_rhs.argtypes = [ctypes.c_void_p, ctypes.c_int64, _ip, _dp, _dp, ctypes.c_void_p, _dp,
@@ -97,6 +99,13 @@ def operators():
     D, S, Vi = np.zeros((n, n)), np.zeros((n, n)), np.zeros((n, n))
     lib().or_operators(_p(x), _p(w), _p(D), _p(S), _p(Vi))
     return x, w, D, S, Vi
+
+
+def mortar_operators():
+    """(prolongation [2,4,4], projection [2,4,4]) of the 2:1 mortar, lower/upper half."""
+    pro, prj = np.zeros((2, 4, 4)), np.zeros((2, 4, 4))
+    lib().or_mortar_operators(_p(pro), _p(prj))
+    return pro, prj
 
 
 def lgl(N):
@@ -198,17 +207,26 @@ def twopoint(kind, d, u, v, kappa=1.4):
 
 
 class Oracle:
-    """Oracle bound to one configuration and mesh (nbr = per-element face neighbours)."""
+    """Oracle bound to one configuration and mesh (nbr = per-element face neighbours with the mortar
+    encoding of Mesh.neighbors(); mortars = Mesh.mortars() for a 2:1 forest)."""
 
-    def __init__(self, cfg, nbr, delta, nthreads=None):
+    def __init__(self, cfg, nbr, delta, nthreads=None, mortars=None):
         self.cfg = cfg                       # a nemo_b200.abi.NemoCfg (ctypes struct)
         self.nbr = np.ascontiguousarray(nbr, dtype=np.int32)
         self.delta = _f64(delta)
         self.E = self.nbr.shape[0]
         self.V = int(cfg.n_vars)
         self.nthreads = nthreads or nthreads_default()
+        self.mortars = np.ascontiguousarray(np.zeros((0, 6)) if mortars is None else mortars, dtype=np.int32)
+        if (self.nbr <= -2).any() and len(self.mortars) == 0:
+            raise ValueError("mesh has mortar faces: pass mortars=mesh.mortars()")
+
+    @classmethod
+    def for_mesh(cls, cfg, mesh, nthreads=None):
+        return cls(cfg, mesh.neighbors(), mesh.delta, nthreads=nthreads, mortars=mesh.mortars())
 
     def _c(self):
+        lib().or_set_mortars(len(self.mortars), self.mortars.ctypes.data)
         return ctypes.byref(self.cfg)
 
     def alpha(self, u):

@@ -42,6 +42,12 @@ def test_operators_bit_identical_to_oracle(lib):
                                atol=1e-14)
 
 
+def test_mortar_operators_bit_identical_to_oracle(lib):
+    pro, prj = abi.mortar_operators()
+    opro, oprj = orc.mortar_operators()
+    assert np.array_equal(pro, opro) and np.array_equal(prj, oprj)
+
+
 def orc_leg(n, x):
     from numpy.polynomial import legendre
     c = np.zeros(n + 1)
