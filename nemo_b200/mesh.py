@@ -280,3 +280,27 @@ def kh_forest(nb=24, max_level=2, seed=7, band=(0.06, 0.05)):
         return dist < band[min(level, len(band) - 1)] + 0.5 * size[:, 1]
 
     return forest(nb, refine, max_level=max_level, lo=(-1.0,) * 3, hi=(1.0,) * 3)
+
+
+def concat(meshes):
+    """Independent meshes side by side in one element list (a batch): element ids of mesh i are
+    offset by the element count of the meshes before it.  Returns (mesh, group_of_element) with
+    group i = mesh i; each group keeps its own time step and simulation time on the device."""
+    off = np.cumsum([0] + [m.E for m in meshes])
+    quads = np.concatenate([np.where(m.side_quads >= 0, m.side_quads + off[i], -1) for i, m in enumerate(meshes)])
+    mesh = Mesh(np.concatenate([m.delta for m in meshes]), np.concatenate([m.center for m in meshes]), quads,
+                np.concatenate([m.side_faceid for m in meshes]), np.concatenate([m.side_nquads for m in meshes]),
+                np.concatenate([m.boundary for m in meshes]), level=np.concatenate([m.level for m in meshes]))
+    groups = np.concatenate([np.full(m.E, i, dtype=np.int32) for i, m in enumerate(meshes)])
+    return mesh, groups
+
+
+def batched_workload(nb=24, members=256, member_nx=8, seed=11):
+    """The batched uneven workload: the Kelvin-Helmholtz forest (group 0) and `members` independent
+    periodic member_nx^3 bricks (groups 1..members) in one element list.  Returns (mesh, groups,
+    forest, member_mesh, amplitudes) with the Gaussian-blob amplitudes drawn from U[0.1, 1]."""
+    f = kh_forest(nb=nb)
+    one = brick(member_nx)
+    mesh, groups = concat([f] + [one] * members)
+    amps = np.random.default_rng(seed).uniform(0.1, 1.0, size=members)
+    return mesh, groups, f, one, amps

@@ -109,3 +109,18 @@ def test_forest_convergence():
         errs.append(np.max(np.abs(uc[0] - exact)))
     order = np.log2(errs[0] / errs[1])
     assert order > 3.0, (errs, order)
+
+
+def test_concat_batch_neighbors():
+    f = band_forest(2, max_level=1)
+    b = mesh.brick(2)
+    m, g = mesh.concat([f, b, b])
+    assert m.E == f.E + 2 * b.E and list(np.bincount(g)) == [f.E, b.E, b.E]
+    nbr = m.neighbors()
+    nf = f.neighbors()
+    # the forest part keeps its neighbours and mortar rows; members point into their own block
+    assert np.array_equal(nbr[: f.E], nf)
+    assert np.array_equal(m.mortars(), f.mortars())
+    for i in range(2):
+        blk = nbr[f.E + i * b.E: f.E + (i + 1) * b.E]
+        assert blk.min() >= f.E + i * b.E and blk.max() < f.E + (i + 1) * b.E
