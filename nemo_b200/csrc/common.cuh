@@ -24,7 +24,8 @@ struct Control {
     double dt_factor;                         // 0.5^(D-1) * cfl / (2*N_NODES - 1)
     int32_t ngroups;
     int32_t done;                             // all groups reached t_end
-    int32_t error;                            // bit 0: bounded wait expired; bit 1: non-finite dt
+    int32_t error;                            // bit 0: bounded TMA wait expired; bit 1: non-finite dt;
+                                              // bit 2: bounded wait on a mortar flag expired
     int32_t pad;
     unsigned long long nbad;                  // elements whose positivity repair failed
     unsigned long long steps;
@@ -36,6 +37,10 @@ struct Control {
     unsigned long long vmax_bits;             // max |velocity component| (positive double bits, MHD)
     int32_t mhd;                              // 1: update glm_ch/glm_alpha from lmax/vmax each step
     int32_t pad2;
+    uint32_t epoch;                           // persistent stage launches: current launch number (>= 1)
+    uint32_t work;                            // persistent stage launches: next task (reset by the last CTA)
+    uint32_t exit_count;                      // persistent stage launches: CTAs finished
+    uint32_t pad3;
 };
 
 // Learned indicator: packed MLP weights (W1[32][12], b1[32], W2[32][32], b2[32], W3[32], b3)

@@ -35,6 +35,7 @@ struct StageArgs {
     float* feat_out;          // FP32 form, prepare launches: indicator features [E][12] or null
     double* alpha_modal_out;  // FP32 form, prepare launches: modal alpha [E] or null
     const double* mflux;      // [5 M][V][16] mortar face fluxes in the face's rotated frame (mortar.cu)
+    const uint32_t* mflag;    // [M] persistent launches: epoch at which a mortar's rows are complete
 };
 
 // 2:1 mortars (mortar.cu): per mortar, the coarse face flux (row 5m) and the four fine face fluxes
@@ -49,6 +50,8 @@ struct MortarArgs {
     int32_t mhd;
     int32_t surface_flux;
     int32_t skip_if_done;     // stage launches: nothing to do once the run reached t_end
+    uint32_t* mflag;          // [nm] or null: set to epoch (release) once a mortar's rows are written
+    uint32_t epoch;
 };
 cudaError_t setup_mortar(const OpConsts& ops);
 cudaError_t launch_mortar(const MortarArgs& a, cudaStream_t s);
@@ -63,6 +66,9 @@ int stage_smem_bytes64();
 // FP32-bulk Euler path (stage_fp32.cu)
 cudaError_t setup_stage_euler32(const OpConsts& ops);
 cudaError_t launch_stage_euler32(const StageArgs& a, bool blend, bool rhs_only, cudaStream_t s);
+// persistent FP32 stage with the mortar pairs as its first tasks (grid = CTAs, <= SMs x resident)
+cudaError_t launch_stage_euler32p(const StageArgs& a, const MortarArgs& ma, bool blend, int grid, cudaStream_t s);
+cudaError_t stage32p_max_ctas_per_sm(bool blend, int* n);
 int stage_smem_bytes32();
 
 // GLM-MHD stages (stage_mhd.cuh instantiated in stage_fp64.cu / stage_fp32.cu)

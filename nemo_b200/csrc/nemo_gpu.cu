@@ -190,6 +190,12 @@ struct Lib {
     int64_t nm = 0;               // 2:1 mortars
     int32_t* mortar = nullptr;    // [nm][6]
     double* mflux = nullptr;      // [5 nm][V][16]
+    uint32_t* mflag = nullptr;    // [nm] persistent FP32 stage: epoch of each mortar's rows
+
+    // stage schedule of the FP32 Euler form (nemo_gpu_autotune): 0 = one CTA per tile plus the
+    // mortar kernel, 1 = persistent CTAs (tune_ctas of them) taking mortar and tile tasks
+    int tune_mode = 0;
+    int tune_ctas = 0;
     double* cdel = nullptr;
     double* delta = nullptr;
     int32_t* group = nullptr;
@@ -246,8 +252,10 @@ void release_mesh() {
     free_dev(g.u[0]); free_dev(g.u[1]); free_dev(g.reg); free_dev(g.stagebuf);
     free_dev(g.alpha[0]); free_dev(g.alpha[1]); free_dev(g.alpha_used);
     free_dev(g.nbr); free_dev(g.cdel); free_dev(g.delta); free_dev(g.group);
-    free_dev(g.mortar); free_dev(g.mflux);
-    g.mortar = nullptr; g.mflux = nullptr; g.nm = 0;
+    free_dev(g.mortar); free_dev(g.mflux); free_dev(g.mflag);
+    g.mortar = nullptr; g.mflux = nullptr; g.mflag = nullptr; g.nm = 0;
+    g.tune_mode = 0;
+    g.tune_ctas = 0;
     free_dev(g.part);
     free_dev(g.feat_dev);
     g.feat_dev = nullptr;
@@ -288,12 +296,36 @@ StageArgs stage_args(int st, bool rhs_only) {
     a.feat_out = nullptr;
     a.alpha_modal_out = nullptr;
     a.mflux = g.mflux;
+    a.mflag = g.mflag;
     return a;
 }
 
 bool is_mhd() { return g.cfg.eqn == NEMO_EQN_MHD; }
 
+MortarArgs mortar_args(const StageArgs& a, bool rhs_only) {
+    MortarArgs m{};
+    m.E = a.E;
+    m.nm = g.nm;
+    m.u_in = a.u_in;
+    m.mortar = g.mortar;
+    m.mflux = g.mflux;
+    m.ctrl = g.ctrl;
+    m.mhd = is_mhd() ? 1 : 0;
+    m.surface_flux = g.cfg.surface_flux;
+    m.skip_if_done = rhs_only ? 0 : 1;
+    return m;
+}
+
+bool persistent_stage(const StageArgs& a, bool rhs_only) {
+    return g.tune_mode == 1 && !rhs_only && !a.prep_only && !is_mhd() && g.cfg.precision == NEMO_PREC_FP32;
+}
+
 cudaError_t launch_stage_any(const StageArgs& a, bool rhs_only, cudaStream_t s) {
+    if (persistent_stage(a, rhs_only)) {
+        MortarArgs m = mortar_args(a, rhs_only);
+        m.mflag = g.mflag;
+        return launch_stage_euler32p(a, m, blended(), g.tune_ctas, s);
+    }
     if (g.nm > 0 && !a.prep_only) {  // fluxes of the 2:1 faces of u_in first
         MortarArgs m{};
         m.E = a.E;
@@ -358,6 +390,7 @@ int check_ctrl_error() {
     CK(cudaStreamSynchronize(g.stream));
     if (err & 1) return fail(NEMO_ERR_CUDA, "a bounded device wait expired (TMA copy did not complete)");
     if (err & 2) return fail(NEMO_ERR_NONFINITE, "non-finite or negative time step");
+    if (err & 4) return fail(NEMO_ERR_CUDA, "a bounded wait on a mortar flag expired");
     return NEMO_OK;
 }
 
@@ -586,6 +619,8 @@ int nemo_gpu_set_mesh(int64_t nelems, const double* delta, const double* center,
         CK(cudaMemcpy(g.mortar, mort.data(), sizeof(int32_t) * 6 * nm, cudaMemcpyHostToDevice));
         CK(cudaMalloc(&g.mflux, sizeof(double) * 5 * nm * g.V * NF));
         CK(cudaMemset(g.mflux, 0, sizeof(double) * 5 * nm * g.V * NF));
+        CK(cudaMalloc(&g.mflag, sizeof(uint32_t) * nm));
+        CK(cudaMemset(g.mflag, 0, sizeof(uint32_t) * nm));
     }
     g.ngroups = 1;
     Control c{};
@@ -594,6 +629,7 @@ int nemo_gpu_set_mesh(int64_t nelems, const double* delta, const double* center,
     c.glm_ch = g.cfg.glm_ch;
     c.glm_alpha = g.cfg.glm_alpha;
     c.mhd = is_mhd() ? 1 : 0;
+    c.epoch = 1u;   // mortar flags start at 0: never equal to a launch's epoch before it sets them
     CK(cudaMemcpy(g.ctrl, &c, sizeof c, cudaMemcpyHostToDevice));
     g.has_mesh = true;
     return NEMO_OK;
@@ -761,7 +797,8 @@ int nemo_gpu_run(int64_t nsteps, double t_end, double* t_out, int64_t* steps_out
             g.n_total += 1;
         }
         for (auto& ev : evs) cudaEventDestroy(ev);
-        if (g.nm > 0) g.n_total += 5 * nsteps;  // mortar launches, timed inside their stage interval
+        const bool fused = g.tune_mode == 1 && !is_mhd() && g.cfg.precision == NEMO_PREC_FP32;
+        if (g.nm > 0 && !fused) g.n_total += 5 * nsteps;  // mortar launches, timed inside their stage interval
         issued = nsteps;
     } else {
         for (int s = 0; s < 2; ++s)
@@ -848,6 +885,140 @@ int nemo_gpu_status(double* t_out, int64_t* nbad_out) {
     CK(cudaStreamSynchronize(g.stream));
     if (t_out) *t_out = t;
     if (nbad_out) *nbad_out = (int64_t)nb;
+    return NEMO_OK;
+}
+
+int nemo_gpu_autotune(int32_t nsteps, int32_t* mode_out, int32_t* ctas_out, double* ms_out) {
+    int st = ensure_ready();
+    if (st) return st;
+    if (nsteps < 1 || nsteps > 1000) return fail(NEMO_ERR_ARG, "nsteps must be in [1, 1000]");
+    if (ms_out)
+        for (int i = 0; i < 4; ++i) ms_out[i] = -1.0;
+    const bool tunable = !is_mhd() && g.cfg.precision == NEMO_PREC_FP32;
+    if (!tunable) {  // the other forms have a single schedule
+        g.tune_mode = 0;
+        if (mode_out) *mode_out = 0;
+        if (ctas_out) *ctas_out = 0;
+        return NEMO_OK;
+    }
+    if ((st = prepare_if_needed())) return st;
+    int nsm = 0, dev = 0, occ = 0;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    CK(stage32p_max_ctas_per_sm(blended(), &occ));
+    if (occ < 1) return fail(NEMO_ERR_CUDA, "the persistent stage kernel does not fit on an SM");
+    // snapshot of everything a step changes: state, register, indicator, control block
+    const size_t bytes = sizeof(double) * (size_t)g.V * g.E * NP;
+    double* reg_snap = nullptr;
+    double* alpha_snap = nullptr;
+    CK(cudaMalloc(&reg_snap, bytes));
+    CK(cudaMalloc(&alpha_snap, sizeof(double) * g.E));
+    Control* csnap = new Control;   // the control block as found
+    Control* ctrial = new Control;  // the same without an end time: the trial steps always run
+    Control* cnow = new Control;
+    auto cleanup = [&]() {
+        cudaFree(reg_snap);
+        cudaFree(alpha_snap);
+        delete csnap;
+        delete ctrial;
+        delete cnow;
+    };
+    const int cur0 = g.cur;
+    const bool regv = g.reg_valid;
+    auto save_or_restore = [&](bool save, Control* src) -> cudaError_t {
+        cudaError_t e;
+        if (save) {
+            if ((e = cudaMemcpyAsync(g.stagebuf, g.u[cur0], bytes, cudaMemcpyDeviceToDevice, g.stream))) return e;
+            if ((e = cudaMemcpyAsync(reg_snap, g.reg, bytes, cudaMemcpyDeviceToDevice, g.stream))) return e;
+            if ((e = cudaMemcpyAsync(alpha_snap, g.alpha[cur0], sizeof(double) * g.E, cudaMemcpyDeviceToDevice, g.stream))) return e;
+            if ((e = cudaMemcpyAsync(csnap, g.ctrl, sizeof(Control), cudaMemcpyDeviceToHost, g.stream))) return e;
+            if ((e = cudaStreamSynchronize(g.stream))) return e;
+            *ctrial = *csnap;
+            ctrial->t_end = 0.0;
+            ctrial->done = 0;
+            return cudaSuccess;
+        }
+        // keep the epoch monotonic: mortar flags may carry the epochs of the trial launches
+        if ((e = cudaMemcpyAsync(cnow, g.ctrl, sizeof(Control), cudaMemcpyDeviceToHost, g.stream))) return e;
+        if ((e = cudaStreamSynchronize(g.stream))) return e;
+        src->epoch = cnow->epoch;
+        src->work = 0u;
+        src->exit_count = 0u;
+        if ((e = cudaMemcpyAsync(g.u[cur0], g.stagebuf, bytes, cudaMemcpyDeviceToDevice, g.stream))) return e;
+        if ((e = cudaMemcpyAsync(g.reg, reg_snap, bytes, cudaMemcpyDeviceToDevice, g.stream))) return e;
+        if ((e = cudaMemcpyAsync(g.alpha[cur0], alpha_snap, sizeof(double) * g.E, cudaMemcpyDeviceToDevice, g.stream))) return e;
+        if ((e = cudaMemcpyAsync(g.ctrl, src, sizeof(Control), cudaMemcpyHostToDevice, g.stream))) return e;
+        if ((e = cudaStreamSynchronize(g.stream))) return e;
+        g.cur = cur0;
+        g.reg_valid = regv;
+        return cudaSuccess;
+    };
+    cudaError_t e = save_or_restore(true, nullptr);
+    if (e == cudaSuccess) e = save_or_restore(false, ctrial);
+    double best = 1e300;
+    int best_mode = 0, best_ctas = 0;
+    const int ncand = 1 + std::min(occ, 3);
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (e == cudaSuccess) e = cudaEventCreate(&e0);
+    if (e == cudaSuccess) e = cudaEventCreate(&e1);
+    for (int c = 0; c < ncand && e == cudaSuccess; ++c) {
+        g.tune_mode = c == 0 ? 0 : 1;
+        g.tune_ctas = c == 0 ? 0 : nsm * c;
+        // one untimed step (first-launch costs), then nsteps timed steps, from the same state
+        for (int rep = 0; rep < 2 && e == cudaSuccess; ++rep) {
+            const int n = rep == 0 ? 1 : nsteps;
+            if ((e = cudaEventRecord(e0, g.stream))) break;
+            for (int i = 0; i < n && e == cudaSuccess; ++i) {
+                e = launch_ctrl_step(g.ctrl, g.stream);
+                for (int s2 = 0; s2 < 5 && e == cudaSuccess; ++s2) e = launch_stage(s2, g.stream);
+            }
+            if (e == cudaSuccess) e = cudaEventRecord(e1, g.stream);
+            if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+            if (e == cudaSuccess && rep == 1) {
+                float ms = 0.f;
+                e = cudaEventElapsedTime(&ms, e0, e1);
+                const double per = ms / nsteps;
+                if (ms_out) ms_out[c] = per;
+                if (per < best) {
+                    best = per;
+                    best_mode = g.tune_mode;
+                    best_ctas = g.tune_ctas;
+                }
+            }
+            if (e == cudaSuccess) e = save_or_restore(false, ctrial);
+        }
+    }
+    if (e == cudaSuccess) e = save_or_restore(false, csnap);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    cleanup();
+    if (e != cudaSuccess) {
+        g.tune_mode = 0;
+        return fail(NEMO_ERR_CUDA, "autotune: %s", cudaGetErrorString(e));
+    }
+    if ((st = check_ctrl_error())) return st;
+    g.tune_mode = best_mode;
+    g.tune_ctas = best_ctas;
+    release_graphs();   // rebuilt with the chosen schedule
+    if (mode_out) *mode_out = best_mode;
+    if (ctas_out) *ctas_out = best_ctas;
+    return NEMO_OK;
+}
+
+int nemo_gpu_set_schedule(int32_t mode, int32_t ctas) {
+    if (!g.inited) return fail(NEMO_ERR_STATE, "nemo_gpu_init has not been called");
+    if (mode != 0 && mode != 1) return fail(NEMO_ERR_ARG, "mode must be 0 (grid) or 1 (persistent)");
+    if (mode == 1) {
+        int nsm = 0, dev = 0, occ = 0;
+        CK(cudaGetDevice(&dev));
+        CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+        CK(stage32p_max_ctas_per_sm(blended(), &occ));
+        if (ctas < 1 || ctas > nsm * occ)
+            return fail(NEMO_ERR_ARG, "persistent CTAs must be in [1, %d] (SMs x resident CTAs)", nsm * occ);
+    }
+    g.tune_mode = mode;
+    g.tune_ctas = mode == 1 ? ctas : 0;
+    release_graphs();
     return NEMO_OK;
 }
 

@@ -13,6 +13,7 @@
 #include "common.cuh"
 #include "euler_fp64.cuh"
 #include "kernels.h"
+#include "mortar.cuh"
 #include "repair64.cuh"
 
 namespace nemo {
@@ -46,18 +47,13 @@ __device__ __forceinline__ bool mbar_wait32(uint64_t* bar, unsigned phase) {
 }
 
 // Stage the tile's state (and, from the second RK stage on, its register) into shared memory with
-// 1D bulk copies (V arrays of nel*64 doubles, contiguous per variable), completing on one mbarrier.
+// 1D bulk copies (V arrays of nel*64 doubles, contiguous per variable), completing on the CTA's
+// mbarrier (initialised once by mbar_init32; one phase per tile).
 __device__ __forceinline__ void tile_issue32(double* su, const double* __restrict__ u, double* sg,
                                              const double* __restrict__ reg, int64_t E, int64_t e0, int nel,
                                              uint64_t* bar) {
     if (threadIdx.x == 0) {
-        unsigned b = smem_u32(bar);
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(b) : "memory");
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
         unsigned b = smem_u32(bar);
         unsigned bytes = (unsigned)(nel * NP * 8);
         unsigned total = bytes * V * (reg ? 2u : 1u);
@@ -80,11 +76,11 @@ __device__ __forceinline__ void tile_issue32(double* su, const double* __restric
     }
 }
 
-__device__ __forceinline__ bool tile_wait32(uint64_t* bar, Control* ctrl) {
-    bool ok = mbar_wait32(bar, 0);
+__device__ __forceinline__ bool tile_wait32(uint64_t* bar, unsigned phase, Control* ctrl) {
+    bool ok = mbar_wait32(bar, phase);
     if (!ok) {
         atomicOr(&ctrl->error, 1);
-        mbar_wait32(bar, 0);  // second bounded wait for the copies still in flight
+        mbar_wait32(bar, phase);  // second bounded wait for the copies still in flight
     }
     return ok;
 }
@@ -429,30 +425,21 @@ __device__ __forceinline__ void epilogue32(const StageArgs& a, const double* su,
 
 }  // namespace
 
-// One CTA = EPC elements x 16 threads; thread (a,b) of an element owns the x-, y- and z-lines
-// through (a,b) and processes them one direction after the other, accumulating into one shared
-// rhs array (x, then y, then z).  A warp holds exactly two elements.
-template <bool BLEND, bool RHS_ONLY>
-__global__ void __launch_bounds__(NT, 3) k_stage_euler32(StageArgs a) {
-    extern __shared__ __align__(128) double smem[];
-    double* su = smem;                                          // [V][EPC][64] FP64 state
-    double* sg = su + V * EPC * NP;                             // [V][EPC][64] FP64 RK register
-    float* sq = reinterpret_cast<float*>(sg + V * EPC * NP);    // [NQ][EPC][64] FP32 node data
-    float* sR = sq + NQ * EPC * NP;                             // [V][EPC][64] FP32 rhs terms
-    __shared__ uint64_t bar;
-    __shared__ float s_alpha[EPC];
-    __shared__ int s_bad[EPC];
-    __shared__ __align__(16) float s_w[MLP_NW];   // learned indicator, transposed layout
+// Shared-memory carve-up of one CTA of the FP32 stage.
+struct Smem32 {
+    double* su;        // [V][EPC][64] FP64 state
+    double* sg;        // [V][EPC][64] FP64 RK register
+    float* sq;         // [NQ][EPC][64] FP32 node data
+    float* sR;         // [V][EPC][64] FP32 rhs terms
+    uint64_t* bar;     // TMA completion barrier (initialised once per CTA)
+    float* s_alpha;    // [EPC]
+    int* s_bad;        // [EPC]
+    const float* s_w;  // learned indicator, transposed layout
+};
 
-    const OpConsts& k = c_ops32;
-    Control* ctrl = a.ctrl;
-    if (!RHS_ONLY && ctrl->done) return;
-    const int tid = threadIdx.x;
-    const int64_t E = a.E;
-    const int64_t e0 = (int64_t)blockIdx.x * EPC;
-    const int nel = (int)min((int64_t)EPC, E - e0);
+__device__ __forceinline__ void load_mlp32(const StageArgs& a, float* s_w) {
     if (a.mlp32) {  // visible to the epilogue after the barriers of the stage
-        for (int i = tid; i < MLP_NW; i += NT) {
+        for (int i = threadIdx.x; i < MLP_NW; i += NT) {
             float v;
             if (i < 12 * 32) v = a.mlp32[(i % 32) * 12 + i / 32];                           // W1T[i/32][i%32]
             else if (i < 12 * 32 + 32) v = a.mlp32[i];                                        // b1
@@ -463,6 +450,60 @@ __global__ void __launch_bounds__(NT, 3) k_stage_euler32(StageArgs a) {
             s_w[i] = v;
         }
     }
+}
+
+__device__ __forceinline__ Smem32 smem32(double* smem, uint64_t* bar, float* s_alpha, int* s_bad, const float* s_w) {
+    Smem32 S;
+    S.su = smem;
+    S.sg = S.su + V * EPC * NP;
+    S.sq = reinterpret_cast<float*>(S.sg + V * EPC * NP);
+    S.sR = S.sq + NQ * EPC * NP;
+    S.bar = bar;
+    S.s_alpha = s_alpha;
+    S.s_bad = s_bad;
+    S.s_w = s_w;
+    return S;
+}
+
+// Acquire a mortar's flux rows: wait (bounded) until its flag carries this launch's epoch.
+__device__ __forceinline__ void mortar_acquire(const uint32_t* flag, uint32_t epoch, Control* ctrl) {
+    for (int it = 0; it < (1 << 20); ++it) {
+        uint32_t v;
+        asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(flag) : "memory");
+        if (v == epoch) return;
+        __nanosleep(64);
+    }
+    atomicOr(&ctrl->error, 4);
+}
+
+__device__ __forceinline__ void mbar_init32(uint64_t* bar) {
+    if (threadIdx.x == 0) {
+        unsigned b = smem_u32(bar);
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(b) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+}
+
+// One tile of EPC elements (tile index `tile`, TMA barrier parity `phase`): thread (a,b) of an
+// element owns the x-, y- and z-lines through (a,b) and processes them one direction after the
+// other, accumulating into one shared rhs array (x, then y, then z).  A warp holds two elements.
+template <bool BLEND, bool RHS_ONLY, bool PERSIST>
+__device__ __forceinline__ void tile32(const StageArgs& a, const Smem32& S, int64_t tile, unsigned phase,
+                                       uint32_t epoch) {
+    const OpConsts& k = c_ops32;
+    Control* ctrl = a.ctrl;
+    double* su = S.su;
+    double* sg = S.sg;
+    float* sq = S.sq;
+    float* sR = S.sR;
+    float* s_alpha = S.s_alpha;
+    int* s_bad = S.s_bad;
+    const float* s_w = S.s_w;
+    const int tid = threadIdx.x;
+    const int64_t E = a.E;
+    const int64_t e0 = tile * EPC;
+    const int nel = (int)min((int64_t)EPC, E - e0);
 
     if (tid < EPC) {
         s_bad[tid] = 0;
@@ -483,8 +524,9 @@ __global__ void __launch_bounds__(NT, 3) k_stage_euler32(StageArgs a) {
         s_alpha[tid] = al;
     }
     const bool load_reg = !RHS_ONLY && !a.prep_only && a.stage > 0;
-    tile_issue32(su, a.u_in, sg, load_reg ? a.reg : nullptr, E, e0, nel, &bar);
-    if (!tile_wait32(&bar, ctrl)) return;
+    tile_issue32(su, a.u_in, sg, load_reg ? a.reg : nullptr, E, e0, nel, S.bar);
+    __syncthreads();   // s_alpha / s_bad visible
+    if (!tile_wait32(S.bar, phase, ctrl)) return;
 
     const int el = tid >> 4, ab = tid & 15, la = ab & 3, lb = ab >> 2;
     const bool active = el < nel;
@@ -553,7 +595,8 @@ __global__ void __launch_bounds__(NT, 3) k_stage_euler32(StageArgs a) {
                 const P32 qo = prim(side ? NN - 1 : 0);
                 P32 qn = qo;
                 const int32_t ne = a.nbr[e * 6 + f];
-                if (ne <= -2) {  // 2:1 mortar face: flux row of the mortar kernel (FP64)
+                if (ne <= -2) {  // 2:1 mortar face: flux row of the mortar kernel / task (FP64)
+                    if (PERSIST) mortar_acquire(a.mflag + (-2 - ne) / 5, epoch, ctrl);
                     const double* mf = a.mflux + (int64_t)(-2 - ne) * V * NF + ab;
 #pragma unroll
                     for (int v = 0; v < V; ++v) Fs[side][v] = (float)mf[v * NF];
@@ -718,13 +761,78 @@ __global__ void __launch_bounds__(NT, 3) k_stage_euler32(StageArgs a) {
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncthreads();
     if (tid == 0) tile_store32(su, a.u_out, sg, a.reg, E, e0, nel);
-    if (st == 4 && blockIdx.x == 0 && tid == 0) {
+    if (st == 4 && tile == 0 && tid == 0) {
         for (int g = 0; g < ctrl->ngroups; ++g) ctrl->t[g] = ctrl->t[g] + ctrl->dt[g];
         ctrl->steps += 1;
     }
 
     epilogue32(a, su, sq, s_w, el, ab, la, lb, active, e, k);
     if (tid == 0) tile_store_wait32();
+}
+
+
+template <bool BLEND, bool RHS_ONLY>
+__global__ void __launch_bounds__(NT, 3) k_stage_euler32(StageArgs a) {
+    extern __shared__ __align__(128) double smem[];
+    __shared__ uint64_t bar;
+    __shared__ float s_alpha[EPC];
+    __shared__ int s_bad[EPC];
+    __shared__ __align__(16) float s_w[MLP_NW];   // learned indicator, transposed layout
+    if (!RHS_ONLY && !a.prep_only && a.ctrl->done) return;
+    load_mlp32(a, s_w);
+    const Smem32 S = smem32(smem, &bar, s_alpha, s_bad, s_w);
+    mbar_init32(&bar);
+    tile32<BLEND, RHS_ONLY, false>(a, S, (int64_t)blockIdx.x, 0u, 0u);
+}
+
+// Persistent form: gridDim.x CTAs (a multiple of the SM count) take tasks from a device counter --
+// first the pairs of 2:1 mortars (their flux rows, published with the launch's epoch), then the
+// element tiles in Morton order.  Tiles that meet a mortar face acquire its flag; every mortar task
+// was taken before any tile task, by a running CTA that waits on nothing, so the waits end.  The
+// last CTA to finish resets the counter and advances the epoch for the next launch.
+template <bool BLEND>
+__global__ void __launch_bounds__(NT, 3) k_stage_euler32p(StageArgs a, MortarArgs ma) {
+    extern __shared__ __align__(128) double smem[];
+    __shared__ uint64_t bar;
+    __shared__ float s_alpha[EPC];
+    __shared__ int s_bad[EPC];
+    __shared__ __align__(16) float s_w[MLP_NW];
+    __shared__ uint32_t s_task;
+    Control* ctrl = a.ctrl;
+    if (ctrl->done) return;
+    const uint32_t epoch = ctrl->epoch;
+    ma.epoch = epoch;
+    load_mlp32(a, s_w);
+    const Smem32 S = smem32(smem, &bar, s_alpha, s_bad, s_w);
+    mbar_init32(&bar);
+    const int64_t ntiles = (a.E + EPC - 1) / EPC;
+    const int64_t npairs = (ma.nm + mortar::MPB - 1) / mortar::MPB;
+    unsigned phase = 0;
+    for (;;) {
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // generic smem writes before TMA
+        __syncthreads();   // the previous task is finished with shared memory and s_task
+        if (threadIdx.x == 0) s_task = atomicAdd(&ctrl->work, 1u);
+        __syncthreads();
+        const int64_t task = s_task;
+        if (task < npairs) {
+            mortar::mortar_pair<false>(ma, task, smem, c_ops32);
+            continue;
+        }
+        const int64_t tile = task - npairs;
+        if (tile >= ntiles) break;
+        tile32<BLEND, false, true>(a, S, tile, phase, epoch);
+        phase ^= 1u;
+    }
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const unsigned n = atomicAdd(&ctrl->exit_count, 1u);
+        if (n == gridDim.x - 1) {
+            ctrl->work = 0u;
+            ctrl->exit_count = 0u;
+            ctrl->epoch = epoch + 1u;
+            __threadfence();
+        }
+    }
 }
 
 int stage_smem_bytes32() {
@@ -751,9 +859,24 @@ static cudaError_t set_attrs32(K kernel, int smem) {
     return cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
 }
 
+cudaError_t launch_stage_euler32p(const StageArgs& a, const MortarArgs& ma, bool blend, int grid, cudaStream_t s) {
+    const int smem = stage_smem_bytes32();
+    if (blend) k_stage_euler32p<true><<<grid, NT, smem, s>>>(a, ma);
+    else k_stage_euler32p<false><<<grid, NT, smem, s>>>(a, ma);
+    return cudaGetLastError();
+}
+
+cudaError_t stage32p_max_ctas_per_sm(bool blend, int* n) {
+    const int smem = stage_smem_bytes32();
+    if (blend) return cudaOccupancyMaxActiveBlocksPerMultiprocessor(n, k_stage_euler32p<true>, NT, smem);
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(n, k_stage_euler32p<false>, NT, smem);
+}
+
 cudaError_t setup_stage_euler32(const OpConsts& ops) {
     const int smem = stage_smem_bytes32();
     cudaError_t err;
+    if ((err = set_attrs32(k_stage_euler32p<true>, smem)) != cudaSuccess) return err;
+    if ((err = set_attrs32(k_stage_euler32p<false>, smem)) != cudaSuccess) return err;
     if ((err = set_attrs32(k_stage_euler32<true, true>, smem)) != cudaSuccess) return err;
     if ((err = set_attrs32(k_stage_euler32<false, true>, smem)) != cudaSuccess) return err;
     if ((err = set_attrs32(k_stage_euler32<true, false>, smem)) != cudaSuccess) return err;

@@ -110,6 +110,17 @@ class Solver:
         call("nemo_gpu_alpha", abi.ptr(a))
         return a
 
+    def autotune(self, nsteps=3):
+        """Pick the stage schedule by timing (FP32 Euler form); returns (mode, ctas, ms per step of
+        each candidate)."""
+        mode, ctas = ctypes.c_int32(), ctypes.c_int32()
+        ms = np.zeros(4)
+        call("nemo_gpu_autotune", int(nsteps), ctypes.byref(mode), ctypes.byref(ctas), abi.ptr(ms))
+        return mode.value, ctas.value, ms
+
+    def set_schedule(self, mode, ctas=0):
+        call("nemo_gpu_set_schedule", int(mode), int(ctas))
+
     def totals(self):
         out = np.zeros(10)
         call("nemo_gpu_totals", abi.ptr(out))
