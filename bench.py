@@ -31,6 +31,10 @@ WORKLOADS = {
                     desc="Sedov blast 32^3 elements N=3 (2.1M nodes), DG/FV blending, FP64"),
     "wave16": dict(nx=16, setup="wave", indicator=0, positivity=0,
                    desc="periodic density wave 16^3 elements N=3 (262k nodes), EC volume + HLLC, FP64"),
+    "batch": dict(nx=24, setup="batch", indicator=1, positivity=1, t_end=0.05,
+                  desc="batched uneven workload: Kelvin-Helmholtz forest on 24^3 base elements with 0-2 "
+                       "levels of refinement at the shear layers (2:1 mortars) + 256 independent 8^3 "
+                       "Gaussian-blob runs (amplitudes U[0.1,1]), N=3, one element list, per-run time steps"),
     "ot64": dict(nx=64, setup="orszag_tang", indicator=1, positivity=1, mhd=True, t_end=0.1,
                  desc="GLM-MHD Orszag-Tang 64^3 elements N=3 (16.8M nodes, 9 variables), gamma 5/3, "
                       "b0 = 1/sqrt(4 pi), HLLD surface + EC volume, DG/FV blending"),
@@ -51,8 +55,13 @@ def load_peaks():
 
 
 def make_state(wl):
+    """(mesh, state, groups or None)."""
     from nemo_b200 import mesh, setups
     w = WORKLOADS[wl]
+    if w["setup"] == "batch":
+        m, g, f, one, amps = mesh.batched_workload(nb=w["nx"])
+        u = np.concatenate([setups.kelvin_helmholtz(f)] + [setups.gaussian_blob(one, a) for a in amps], axis=1)
+        return m, np.ascontiguousarray(u), g
     if w["setup"] == "sedov":
         m = mesh.brick(w["nx"], lo=(-0.5,) * 3, hi=(0.5,) * 3)
         u = setups.sedov(m, sigma=0.05)
@@ -62,7 +71,7 @@ def make_state(wl):
     else:
         m = mesh.brick(w["nx"])
         u = setups.density_wave(m, seed=1234)
-    return m, u
+    return m, u, None
 
 
 def make_cfg(wl, precision=0, learned=False):
@@ -76,9 +85,9 @@ def make_cfg(wl, precision=0, learned=False):
     return abi.default_cfg(indicator=ind, positivity=w["positivity"], cfl=0.5, precision=precision)
 
 
-def make_solver(wl, m, precision, learned=False):
+def make_solver(wl, m, precision, learned=False, groups=None):
     from nemo_b200.solver import Solver
-    s = Solver(make_cfg(wl, precision, learned), m)
+    s = Solver(make_cfg(wl, precision, learned), m, groups)
     if learned and WORKLOADS[wl]["indicator"]:
         from nemo_b200 import learned as lm
         lm.install()
@@ -159,10 +168,10 @@ class ClockSampler:
 
 def cpu_baseline(wl, u, m, nthreads=None, sample_stages=5):
     """The oracle (C++ FP64 restatement, OpenMP) on the host cores, on a bounded sample of the same
-    workload: sample_stages RK stages of the full state."""
+    workload: sample_stages RK stages of the full state (one common time step for all elements)."""
     from oracle import oracle as orc
     c = make_cfg(wl)
-    o = orc.Oracle(c, m.neighbors(), m.delta, nthreads=nthreads)
+    o = orc.Oracle.for_mesh(c, m, nthreads=nthreads)
     uu, reg = u.copy(), np.zeros_like(u)
     dt, _ = o.timestep(uu)
     o.stage(uu, reg, 0, dt)  # untimed warm-up stage (page-in)
@@ -177,7 +186,7 @@ def cpu_baseline(wl, u, m, nthreads=None, sample_stages=5):
                       f"{o.nthreads} OpenMP threads, {el:.2f} s"}
 
 
-def accuracy_check(wl, m, u, abi, Solver, t_end=0.05):  # noqa: C901
+def accuracy_check(wl, m, u, abi, Solver, t_end=0.05, groups=None):  # noqa: C901
     """All forms to t_end.  The chosen form (FP32 bulk + learned indicator) against the FP64 form of
     the same method (learned indicator evaluated in FP64 from the same BF16 weights; that plain
     path reproduces the FP64 oracle bit for bit, see tests/test_gpu_learned.py), and both against
@@ -186,8 +195,10 @@ def accuracy_check(wl, m, u, abi, Solver, t_end=0.05):  # noqa: C901
     res = {}
     for key, prec, learned in (("fp64_modal", abi.PREC_FP64, False), ("fp64_learned", abi.PREC_FP64, True),
                                ("fp32_learned", abi.PREC_FP32, True)):
-        s = make_solver(wl, m, prec, learned)
+        s = make_solver(wl, m, prec, learned, groups)
         s.upload(u)
+        if prec == abi.PREC_FP32:
+            s.autotune(nsteps=2)
         t0 = time.perf_counter()
         t, n = s.run(t_end=t_end)
         el = time.perf_counter() - t0
@@ -232,9 +243,9 @@ def run_reference(args, rank, world):
         return
     from oracle import oracle as orc
     orc.build()
-    m, u = make_state(args.workload)
+    m, u, groups = make_state(args.workload)
     c = make_cfg(args.workload)
-    o = orc.Oracle(c, m.neighbors(), m.delta)
+    o = orc.Oracle.for_mesh(c, m)
     uu = u.copy()
     for _ in range(args.warmup):
         uu, _, _, _ = o.run(uu, nsteps=1)
@@ -290,13 +301,13 @@ def main():
     from nemo_b200.solver import Solver
     import ctypes
 
-    m, u = make_state(args.workload)
+    m, u, groups = make_state(args.workload)
     dof_per_step = m.E * 64 * 5
     V = nvars(args.workload)
     mhd = bool(WORKLOADS[args.workload].get("mhd"))
 
     # ---- the plain FP64 form (the comparison point of the metric)
-    s = Solver(make_cfg(args.workload, abi.PREC_FP64), m)
+    s = Solver(make_cfg(args.workload, abi.PREC_FP64), m, groups)
     s.upload(u)
     stream_ptr = ctypes.c_uint64()
     abi.call("nemo_gpu_stream", ctypes.byref(stream_ptr))
@@ -307,8 +318,9 @@ def main():
     s.finalize()
 
     # ---- the chosen form: FP32 bulk + learned indicator, FP64 state/register/update/repair/reductions
-    s = make_solver(args.workload, m, abi.PREC_FP32, learned=True)
+    s = make_solver(args.workload, m, abi.PREC_FP32, learned=True, groups=groups)
     s.upload(u)
+    tune_mode, tune_ctas, tune_ms = s.autotune(nsteps=3)   # restores the state it times
     abi.call("nemo_gpu_stream", ctypes.byref(stream_ptr))
     stream = torch.cuda.ExternalStream(stream_ptr.value)
     s.run(nsteps=args.warmup)
@@ -360,8 +372,9 @@ def main():
 
     s.finalize()
     accuracy = None
-    if not args.no_accuracy and WORKLOADS[args.workload]["setup"] in ("sedov", "orszag_tang"):
-        accuracy = accuracy_check(args.workload, m, u, abi, Solver, t_end=WORKLOADS[args.workload].get("t_end", 0.05))
+    if not args.no_accuracy and WORKLOADS[args.workload]["setup"] in ("sedov", "orszag_tang", "batch"):
+        accuracy = accuracy_check(args.workload, m, u, abi, Solver, t_end=WORKLOADS[args.workload].get("t_end", 0.05),
+                                  groups=groups)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -385,6 +398,11 @@ def main():
                        "stages_per_step": 5,
                        "form": "chosen: FP32 bulk + FP64 accumulation, learned indicator with modal fallback",
                        "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
+                       "schedule": {"chosen": "persistent" if tune_mode == 1 else "grid", "persistent_ctas": tune_ctas,
+                                    "autotune_ms_per_step": {"grid": tune_ms[0], "persistent_1_per_sm": tune_ms[1],
+                                                             "persistent_2_per_sm": tune_ms[2],
+                                                             "persistent_3_per_sm": tune_ms[3]}},
+                       "groups": int(groups.max()) + 1 if groups is not None else 1,
                        "l2": f"working set (u in/out + register, 3 x {u.nbytes / 1e6:.0f} MB) larger than L2"},
             "clocks": clk.summary(),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
