@@ -47,6 +47,10 @@ struct Control {
 // followed by the lower and upper bounds of the 12 normalised inputs.
 constexpr int MLP_NW = 32 * 12 + 32 + 32 * 32 + 32 + 32 + 1;
 constexpr int MLP_NPACK = MLP_NW + 24;
+// FP32 form: the same weights with W1 and W2 transposed ([12][32], [32][32]) followed by the input
+// bounds, padded to whole float4s, stored after the packed copy; a CTA copies them to shared memory
+// with float4 loads.
+constexpr int MLP_NT = (MLP_NPACK + 3) / 4 * 4;
 
 // Operator constants (filled once by nemo_gpu_init from the host-built matrices).
 struct OpConsts {

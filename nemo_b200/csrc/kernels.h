@@ -32,6 +32,7 @@ struct StageArgs {
     int32_t prep_only;        // only the epilogue on u_in (indicator and CFL bound of a state)
     const double* mlp64;      // learned indicator (FP64 values of the BF16 weights) or null
     const float* mlp32;       // same, FP32
+    const float* mlp32t;      // FP32, W1 and W2 transposed (MLP_NT floats, 16-byte aligned)
     float* feat_out;          // FP32 form, prepare launches: indicator features [E][12] or null
     double* alpha_modal_out;  // FP32 form, prepare launches: modal alpha [E] or null
     const double* mflux;      // [5 M][V][16] mortar face fluxes in the face's rotated frame (mortar.cu)

@@ -268,6 +268,9 @@ void release_mesh() {
 
 bool blended() { return g.cfg.indicator != NEMO_IND_NONE; }
 
+// float offset of the transposed weights in g.mlp32 (16-byte aligned)
+int mlp_t_offset() { return (MLP_NPACK + 3) / 4 * 4; }
+
 StageArgs stage_args(int st, bool rhs_only) {
     StageArgs a{};
     a.E = g.E;
@@ -293,6 +296,7 @@ StageArgs stage_args(int st, bool rhs_only) {
     const bool learned = g.cfg.indicator == NEMO_IND_LEARNED && g.mlp_ready;
     a.mlp64 = learned ? g.mlp64 : nullptr;
     a.mlp32 = learned ? g.mlp32 : nullptr;
+    a.mlp32t = learned ? g.mlp32 + mlp_t_offset() : nullptr;
     a.feat_out = nullptr;
     a.alpha_modal_out = nullptr;
     a.mflux = g.mflux;
@@ -525,7 +529,7 @@ int nemo_gpu_init(const nemo_cfg* cfg) {
     CK(cudaMalloc(&g.ctrl, sizeof(Control)));
     CK(cudaMemset(g.ctrl, 0, sizeof(Control)));
     CK(cudaMalloc(&g.tot, 16 * sizeof(double)));
-    CK(cudaMalloc(&g.mlp32, sizeof(float) * MLP_NPACK));
+    CK(cudaMalloc(&g.mlp32, sizeof(float) * (MLP_NPACK + 8 + MLP_NT)));
     CK(cudaMalloc(&g.mlp64, sizeof(double) * MLP_NPACK));
     g.mlp_ready = false;
     g.inited = true;
@@ -1064,7 +1068,21 @@ int nemo_gpu_set_mlp(const float* weights, int32_t nweights, const float* lo, co
         w64[MLP_NW + i] = (double)lo[i];
         w64[MLP_NW + 12 + i] = (double)hi[i];
     }
+    // transposed copy for the FP32 stage: W1T[i][j] = W1[j][i], W2T[i][j] = W2[j][i]
+    std::vector<float> wt(MLP_NT, 0.0f);
+    for (int i = 0; i < MLP_NW; ++i) {
+        float v;
+        if (i < 12 * 32) v = w32[(i % 32) * 12 + i / 32];
+        else if (i < 12 * 32 + 32) v = w32[i];
+        else if (i < 12 * 32 + 32 + 32 * 32) {
+            const int r = i - (12 * 32 + 32);
+            v = w32[12 * 32 + 32 + (r % 32) * 32 + r / 32];
+        } else v = w32[i];
+        wt[i] = v;
+    }
+    for (int i = MLP_NW; i < MLP_NPACK; ++i) wt[i] = w32[i];   // input bounds
     CK(cudaMemcpy(g.mlp32, w32.data(), sizeof(float) * MLP_NPACK, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(g.mlp32 + mlp_t_offset(), wt.data(), sizeof(float) * MLP_NT, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(g.mlp64, w64.data(), sizeof(double) * MLP_NPACK, cudaMemcpyHostToDevice));
     g.mlp_ready = true;
     release_graphs();

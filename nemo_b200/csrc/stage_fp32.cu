@@ -220,12 +220,33 @@ __device__ __forceinline__ float hmin16(float v) {
     return v;
 }
 
+// Transposed all-reduce over the 16 lanes of an element: lane l returns the sum over the 16 lanes
+// of v[l] (15 shuffles for 16 sums instead of 64).
+__device__ __forceinline__ float tsum16(float (&v)[16], int l) {
+#pragma unroll
+    for (int o = 8; o > 0; o >>= 1) {
+        const bool up = (l & o) != 0;
+#pragma unroll
+        for (int i = 0; i < o; ++i) {
+            const float send = up ? v[i] : v[i + o];
+            const float keep = up ? v[i + o] : v[i];
+            v[i] = keep + __shfl_xor_sync(0xffffffffu, send, o);
+        }
+    }
+    return v[0];
+}
+
 __device__ __forceinline__ void epilogue32(const StageArgs& a, const double* su, float* scratch, const float* sw,
                                            int el, int ab, int la, int lb, bool active, int64_t e,
                                            const OpConsts& k) {
     Control* ctrl = a.ctrl;
     const bool need_lam = a.epi_dt != 0;
     if (!a.alpha_out && !need_lam) return;
+    __shared__ int s_fb[EPC];
+    __shared__ float s_jd[EPC];
+    __shared__ double s_dt[EPC], s_lm[EPC];
+    __shared__ int s_gr[EPC];
+    if (threadIdx.x < EPC) s_fb[threadIdx.x] = 0;
     float qr[NN], qp[NN];
     float lx = 0.f, ly = 0.f, lz = 0.f;
 #pragma unroll
@@ -339,10 +360,9 @@ __device__ __forceinline__ void epilogue32(const StageArgs& a, const double* su,
             if (active && ab == 0 && a.alpha_modal_out) a.alpha_modal_out[e] = (double)am;
         }
         if (learned) {
-            const float* W = a.mlp32;
-            const float* lo = W + MLP_NW;
-            const float* hi = lo + 12;
-            // positivity-risk check and the 12 features
+            // positivity-risk check and the 12 features: one transposed reduction over the 16 lanes
+            // leaves lane i with the element total of quantity i (0..11 the order energies, 12/13
+            // the rho and p energies, 14/15 the sums of rho and p), then each lane forms its feature
             float rs = 0.f, ps = 0.f, rmn = 3.4e38f, pmn = 3.4e38f;
 #pragma unroll
             for (int i = 0; i < NN; ++i) {
@@ -351,22 +371,31 @@ __device__ __forceinline__ void epilogue32(const StageArgs& a, const double* su,
                 rmn = fminf(rmn, qr[i]);
                 pmn = fminf(pmn, qp[i]);
             }
-            rs = hsum16(rs);
-            ps = hsum16(ps);
+            float red[16];
+#pragma unroll
+            for (int i = 0; i < 6; ++i) {
+                red[i] = Eo[0][i];
+                red[6 + i] = Eo[1][i];
+            }
+            red[12] = tot[1];
+            red[13] = tot[2];
+            red[14] = rs;
+            red[15] = ps;
+            const float mine = tsum16(red, ab);
+            const float tq = __shfl_sync(0xffffffffu, mine, 12 + (ab >= 6 ? 1 : 0), 16);
+            rs = __shfl_sync(0xffffffffu, mine, 14, 16);
+            ps = __shfl_sync(0xffffffffu, mine, 15, 16);
             rmn = hmin16(rmn);
             pmn = hmin16(pmn);
-            bool fb = rmn < 0.1f * (rs / 64.0f) || pmn < 0.1f * (ps / 64.0f);
+            const float lo = sw[MLP_NW + (ab < 12 ? ab : 0)], hi = sw[MLP_NW + 12 + (ab < 12 ? ab : 0)];
+            const float xm = __logf(mine / tq + 1e-12f) * 0.1f + 1.0f;
+            const bool out_of_bounds = ab < 12 && (xm < lo || xm > hi);
+            // the vote runs in every lane of the warp (the two elements of a warp may differ in fb)
+            const unsigned oob = __ballot_sync(0xffffffffu, out_of_bounds) & (0xffffu << (threadIdx.x & 16));
+            const bool fb = rmn < 0.1f * (rs / 64.0f) || pmn < 0.1f * (ps / 64.0f) || oob != 0u;
             float x[12];
 #pragma unroll
-            for (int w = 0; w < 2; ++w) {
-                const float tw = hsum16(tot[1 + w]);
-#pragma unroll
-                for (int i = 0; i < 6; ++i) {
-                    const float f = __logf(hsum16(Eo[w][i]) / tw + 1e-12f);
-                    x[6 * w + i] = f * 0.1f + 1.0f;
-                    fb = fb || x[6 * w + i] < lo[6 * w + i] || x[6 * w + i] > hi[6 * w + i];
-                }
-            }
+            for (int i = 0; i < 12; ++i) x[i] = __shfl_sync(0xffffffffu, xm, i, 16);
             // sw: W1 transposed [12][32], b1[32], W2 transposed [32][32], b2[32], W3[32], b3
             const float* W1T = sw;
             const float* b1 = W1T + 12 * 32;
@@ -398,13 +427,10 @@ __device__ __forceinline__ void epilogue32(const StageArgs& a, const double* su,
             if (al < (float)k.alpha_min) al = 0.0f;
             if (fb) {
                 alpha = am;
-                if (active && ab == 0) atomicAdd(&ctrl->fallback, 1ull);
+                if (active && ab == 0) s_fb[el] = 1;
             } else {
                 alpha = al;
-                if (active && ab == 0) {
-                    atomicAdd(&ctrl->judge_sum, (double)fabsf(al - am));
-                    atomicAdd(&ctrl->judge_n, 1ull);
-                }
+                if (active && ab == 0) s_jd[el] = fabsf(al - am);
             }
         }
         if (active && ab == 0) a.alpha_out[e] = (double)alpha;
@@ -416,9 +442,49 @@ __device__ __forceinline__ void epilogue32(const StageArgs& a, const double* su,
         if (active && ab == 0) {
             const double dte = fmin(fmin(a.delta[e * 3 + 0] / (double)lx, a.delta[e * 3 + 1] / (double)ly),
                                     a.delta[e * 3 + 2] / (double)lz);
-            const int g = a.group ? a.group[e] : 0;
-            atomicMin(&ctrl->dtmin_bits[g], (unsigned long long)__double_as_longlong(dte));
-            atomicMax(&ctrl->lmax_bits[g], (unsigned long long)__double_as_longlong((double)fmaxf(fmaxf(lx, ly), lz)));
+            s_dt[el] = dte;
+            s_lm[el] = (double)fmaxf(fmaxf(lx, ly), lz);
+            s_gr[el] = a.group ? a.group[e] : 0;
+        }
+    }
+    // one set of atomics per CTA instead of per element: the counters and minima are single
+    // addresses that every element of the launch would otherwise hit
+    if (!a.alpha_out && !need_lam) return;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const int nel = (int)min((int64_t)EPC, a.E - (e - el));
+        if (a.alpha_out && a.mlp32) {
+            unsigned long long nfb = 0, nj = 0;
+            double js = 0.0;
+            for (int i = 0; i < nel; ++i) {
+                if (s_fb[i]) nfb += 1;
+                else {
+                    js += (double)s_jd[i];
+                    nj += 1;
+                }
+            }
+            if (nfb) atomicAdd(&ctrl->fallback, nfb);
+            if (nj) {
+                atomicAdd(&ctrl->judge_sum, js);
+                atomicAdd(&ctrl->judge_n, nj);
+            }
+        }
+        if (need_lam) {
+            int g = s_gr[0];
+            double dmin = s_dt[0], lmx = s_lm[0];
+            for (int i = 1; i <= nel; ++i) {
+                if (i == nel || s_gr[i] != g) {
+                    atomicMin(&ctrl->dtmin_bits[g], (unsigned long long)__double_as_longlong(dmin));
+                    atomicMax(&ctrl->lmax_bits[g], (unsigned long long)__double_as_longlong(lmx));
+                    if (i == nel) break;
+                    g = s_gr[i];
+                    dmin = s_dt[i];
+                    lmx = s_lm[i];
+                } else {
+                    dmin = fmin(dmin, s_dt[i]);
+                    lmx = fmax(lmx, s_lm[i]);
+                }
+            }
         }
     }
 }
@@ -438,17 +504,10 @@ struct Smem32 {
 };
 
 __device__ __forceinline__ void load_mlp32(const StageArgs& a, float* s_w) {
-    if (a.mlp32) {  // visible to the epilogue after the barriers of the stage
-        for (int i = threadIdx.x; i < MLP_NW; i += NT) {
-            float v;
-            if (i < 12 * 32) v = a.mlp32[(i % 32) * 12 + i / 32];                           // W1T[i/32][i%32]
-            else if (i < 12 * 32 + 32) v = a.mlp32[i];                                        // b1
-            else if (i < 12 * 32 + 32 + 32 * 32) {
-                const int r = i - (12 * 32 + 32);
-                v = a.mlp32[12 * 32 + 32 + (r % 32) * 32 + r / 32];                           // W2T[r/32][r%32]
-            } else v = a.mlp32[i];                                                            // b2, W3, b3
-            s_w[i] = v;
-        }
+    if (a.mlp32t) {  // visible to the epilogue after the barriers of the stage
+        const float4* src = reinterpret_cast<const float4*>(a.mlp32t);
+        float4* dst = reinterpret_cast<float4*>(s_w);
+        for (int i = threadIdx.x; i < MLP_NT / 4; i += NT) dst[i] = __ldg(src + i);
     }
 }
 
@@ -777,7 +836,7 @@ __global__ void __launch_bounds__(NT, 3) k_stage_euler32(StageArgs a) {
     __shared__ uint64_t bar;
     __shared__ float s_alpha[EPC];
     __shared__ int s_bad[EPC];
-    __shared__ __align__(16) float s_w[MLP_NW];   // learned indicator, transposed layout
+    __shared__ __align__(16) float s_w[MLP_NT];   // learned indicator, transposed layout
     if (!RHS_ONLY && !a.prep_only && a.ctrl->done) return;
     load_mlp32(a, s_w);
     const Smem32 S = smem32(smem, &bar, s_alpha, s_bad, s_w);
@@ -796,7 +855,7 @@ __global__ void __launch_bounds__(NT, 3) k_stage_euler32p(StageArgs a, MortarArg
     __shared__ uint64_t bar;
     __shared__ float s_alpha[EPC];
     __shared__ int s_bad[EPC];
-    __shared__ __align__(16) float s_w[MLP_NW];
+    __shared__ __align__(16) float s_w[MLP_NT];
     __shared__ uint32_t s_task;
     Control* ctrl = a.ctrl;
     if (ctrl->done) return;
