@@ -77,6 +77,86 @@ __device__ __noinline__ bool repair_elem(double* su, int el, const OpConsts& k) 
 }
 
 
+// The same repair done by the element's 16 threads together (a half-warp that calls it as a whole):
+// no per-thread tile arrays, so it inlines without a call frame.  Level 1 squeezes the 8 octants
+// (lanes 0..7, one octant each); level 2 squeezes the 8 nodes of each octant (lanes 0..7 and 8..15
+// take one octant each, four rounds).  Each lane sums its tile in the serial routine's node order,
+// the means run over the tiles in tile order, and all lanes of a block take the same squeeze steps.
+template <int EPC>
+__device__ __forceinline__ bool repair_elem16(double* su, int el, int lane, const OpConsts& k) {
+    constexpr int V = 5;
+    auto at = [&](int v, int p) -> double& { return su[(v * EPC + el) * NP + p]; };
+    const unsigned half = threadIdx.x & 16;
+#pragma unroll 1
+    for (int level = 1; level <= 2; ++level) {
+        const int rounds = level == 1 ? 1 : 4;
+#pragma unroll 1
+        for (int rd = 0; rd < rounds; ++rd) {
+            const int grp = lane >> 3, t = lane & 7;
+            const bool use = level == 2 || grp == 0;
+            const unsigned gm = 0xffu << (half + 8 * grp);   // the 8 lanes of this block
+            const int ii = t & 1, jj = (t >> 1) & 1, kk = t >> 2;
+            // block origin (level 2: octant (q, pp, r) = blk bits) and the tile's node range
+            const int blk = level == 1 ? 0 : 2 * rd + grp;
+            const int q = blk & 1, pp = (blk >> 1) & 1, r = blk >> 2;
+            const int nn = level == 1 ? 2 : 1;
+            const int i0 = level == 1 ? 2 * ii : 2 * q + ii;
+            const int j0 = level == 1 ? 2 * jj : 2 * pp + jj;
+            const int k0 = level == 1 ? 2 * kk : 2 * r + kk;
+            const double ws = level == 1 ? 0.125 : 1.0;
+            double tile[V];
+#pragma unroll
+            for (int v = 0; v < V; ++v) {
+                double acc = 0.0;
+                if (use)
+                    for (int kx = k0; kx < k0 + nn; ++kx)
+                        for (int jx = j0; jx < j0 + nn; ++jx)
+                            for (int ix = i0; ix < i0 + nn; ++ix) acc = acc + ws * at(v, nidx(ix, jx, kx));
+                tile[v] = acc;
+            }
+            if (!use) continue;
+            const bool bad = !isvalid64(tile, k);
+            if (__ballot_sync(gm, bad) == 0u) continue;   // the block's tiles are admissible
+            double mean[V], hile[V];
+#pragma unroll
+            for (int v = 0; v < V; ++v) {
+                double sum = 0.0;
+#pragma unroll
+                for (int tt = 0; tt < 8; ++tt) sum = sum + __shfl_sync(gm, tile[v], (int)(half + 8 * grp) + tt);
+                mean[v] = 0.125 * sum;
+                hile[v] = tile[v] - mean[v];
+            }
+            double squeeze = 1.0;
+#pragma unroll 1
+            while (squeeze > 0.0) {
+                squeeze = fmax(0.0, squeeze - k.repair_decr);
+                double tv[V];
+#pragma unroll
+                for (int v = 0; v < V; ++v) tv[v] = mean[v] + squeeze * hile[v];
+                if (__ballot_sync(gm, !isvalid64(tv, k)) == 0u) break;
+            }
+            for (int kx = k0; kx < k0 + nn; ++kx)
+                for (int jx = j0; jx < j0 + nn; ++jx)
+                    for (int ix = i0; ix < i0 + nn; ++ix) {
+                        const int p = nidx(ix, jx, kx);
+#pragma unroll
+                        for (int v = 0; v < V; ++v) at(v, p) = mean[v] + squeeze * (at(v, p) - mean[v]);
+                    }
+        }
+        __syncwarp(0xffffu << half);
+    }
+    bool ok = true;
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+        const int p = lane + 16 * m;
+        double qv[V];
+#pragma unroll
+        for (int v = 0; v < V; ++v) qv[v] = at(v, p);
+        ok = ok && isvalid64(qv, k);
+    }
+    return __ballot_sync(0xffffu << half, !ok) == 0u;
+}
+
 // The same repair for the 9 GLM-MHD variables (MHD pressure in the admissibility check).
 template <int EPC>
 __device__ __noinline__ bool repair_elem_mhd(double* su, int el, const OpConsts& k) {

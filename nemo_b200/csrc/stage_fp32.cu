@@ -813,8 +813,9 @@ __device__ __forceinline__ void tile32(const StageArgs& a, const Smem32& S, int6
     }
     if (RHS_ONLY) return;
     __syncthreads();
-    if (a.positivity && active && ab == 0 && s_bad[el]) {
-        if (!repair_elem<EPC>(su, el, k)) atomicAdd(&ctrl->nbad, 1ull);
+    if (a.positivity && active && s_bad[el]) {   // the element's 16 threads together
+        const bool repaired = repair_elem16<EPC>(su, el, ab, k);
+        if (!repaired && ab == 0) atomicAdd(&ctrl->nbad, 1ull);
     }
     // make the generic-proxy writes of su/sg visible to the bulk copies, then store the tile
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");

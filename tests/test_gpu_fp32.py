@@ -87,3 +87,37 @@ def test_fp32_sedov32_to_t_end_within_1e6_l1():
     assert b64 == 0 and b32 == 0
     err = rel_l1(u32[0], u64[0])
     assert err < 1e-6, err
+
+
+def test_fp32_repair_path():
+    """A stage that leaves inadmissible nodes: the FP32 form's cooperative repair (16 threads per
+    element) restores admissibility like the oracle's serial repair, and reports the elements it
+    cannot repair."""
+    kappa = 1.4
+    m = mesh.brick(4)
+    x = m.node_coords(setups.LGL4)[0]
+    one = np.ones_like(x)
+    u = np.ascontiguousarray(setups.prim2cons(one, np.where(x < 0.5, -3.0, 3.0), 0 * one, 0 * one, 0.05 * one, kappa))
+    c = abi.default_cfg(precision=abi.PREC_FP32, positivity=1)
+    s = Solver(c, m)
+    o = orc.Oracle(abi.default_cfg(positivity=1), m.neighbors(), m.delta)
+    s.upload(u)
+    dt, _ = o.timestep(u)
+    uc, reg = u.copy(), np.zeros_like(u)
+    # without the repair the stage would leave negative pressures
+    bare = u.copy()
+    orc.Oracle(abi.default_cfg(positivity=0), m.neighbors(), m.delta).stage(bare, np.zeros_like(u), 0, 32 * dt)
+    p_bare = 0.4 * (bare[4] - 0.5 * (bare[1] ** 2 + bare[2] ** 2 + bare[3] ** 2) / bare[0])
+    assert (p_bare <= 0).any()
+    assert o.stage(uc, reg, 0, 32 * dt) == 0
+    assert s.stage(1, 32 * dt) == 0
+    got = s.download()
+    p = 0.4 * (got[4] - 0.5 * (got[1] ** 2 + got[2] ** 2 + got[3] ** 2) / got[0])
+    assert (got[0] > 0).all() and (p > 0).all()
+    assert rel_l1(got, uc) < 1e-3
+    s.upload(u)
+    uc, reg = u.copy(), np.zeros_like(u)
+    nb_c = o.stage(uc, reg, 0, 64 * dt)
+    with pytest.raises(abi.NemoError) as ei:
+        s.stage(1, 64 * dt)
+    assert ei.value.code == 4 and nb_c > 0 and s.status()[1] > 0
