@@ -125,6 +125,19 @@ int nemo_gpu_set_mesh(int64_t nelems, const double* delta, const double* center,
    Each group gets its own time step and simulation time.  Default: one group. */
 int nemo_gpu_set_groups(int32_t ngroups, const int32_t* group_of_elem);
 
+/* Element partition across processes (the reference partitions quads over MPI ranks with p4est and
+   exchanges the partition-boundary payloads, source/mesh/p4est/mesh_utils_mod.f90:623-675, 1014-).
+   Elements [0, n_owned) of this process's mesh are advanced; [n_owned, nelems) are ghost copies of
+   other processes' elements that only serve as face neighbours (and mortar partners).  The caller
+   refreshes the ghosts before every stage: nemo_gpu_pack_elements gathers the listed elements of the
+   current state into buf_dev ([n][n_vars*64 + 1] doubles: the element's state, then its raw blending
+   coefficient), nemo_gpu_unpack_elements scatters such a buffer into the listed (ghost) elements.
+   idx_dev and buf_dev are device pointers; both calls return after the copy has completed.  The
+   time step of a partitioned run is the minimum over processes of nemo_gpu_calc_timestep. */
+int nemo_gpu_set_owned(int64_t n_owned);
+int nemo_gpu_pack_elements(const int32_t* idx_dev, int64_t n, double* buf_dev);
+int nemo_gpu_unpack_elements(const int32_t* idx_dev, int64_t n, const double* buf_dev);
+
 /* Copy the conserved state host->device.  host points at the first element's state(1,1,1,1);
    consecutive elements are elem_stride_bytes apart (sizeof(quad_t) when the state sits in the
    reference's quad_t array, n^3*V*8 for a packed [E][V][n^3] array).  Resets the RK register. */

@@ -27,7 +27,8 @@ EXPORTS = [
     "nemo_gpu_last_error", "nemo_gpu_set_timing", "nemo_gpu_kernel_timing", "nemo_gpu_stream",
     "nemo_gpu_totals_noalloc", "nemo_gpu_set_mlp", "nemo_gpu_features", "nemo_gpu_indicator_stats",
     "nemo_gpu_mlp_train", "nemo_gpu_mlp_grad", "nemo_gpu_mlp_forward", "nemo_gpu_mortar_operators",
-    "nemo_gpu_autotune", "nemo_gpu_set_schedule",
+    "nemo_gpu_autotune", "nemo_gpu_set_schedule", "nemo_gpu_set_owned", "nemo_gpu_pack_elements",
+    "nemo_gpu_unpack_elements",
 ]
 
 
@@ -96,6 +97,9 @@ def load(path=LIB_PATH):
         "nemo_gpu_mortar_operators": [i32, vp, vp],
         "nemo_gpu_autotune": [i32, ctypes.POINTER(i32), ctypes.POINTER(i32), vp],
         "nemo_gpu_set_schedule": [i32, i32],
+        "nemo_gpu_set_owned": [i64],
+        "nemo_gpu_pack_elements": [vp, i64, vp],
+        "nemo_gpu_unpack_elements": [vp, i64, vp],
     }
     for name, args in sig.items():
         f = getattr(L, name)

@@ -79,7 +79,43 @@ __global__ void k_soa_to_aos(const double* __restrict__ soa, double* __restrict_
     aos[i] = soa[(v * E + e) * NP + n];
 }
 
+// element exchange buffers: per listed element its V x 64 state values and its raw indicator
+__global__ void k_pack(const double* __restrict__ u, const double* __restrict__ alpha, const int32_t* __restrict__ idx,
+                       int64_t n, int64_t E, int nv, double* __restrict__ buf) {
+    const int64_t row = (int64_t)nv * NP + 1;
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n * row) return;
+    const int64_t m = i / row, r = i % row;
+    const int64_t e = idx[m];
+    buf[i] = r < (int64_t)nv * NP ? u[((r / NP) * E + e) * NP + r % NP] : (alpha ? alpha[e] : 0.0);
+}
+
+__global__ void k_unpack(double* __restrict__ u, double* __restrict__ alpha, const int32_t* __restrict__ idx,
+                         int64_t n, int64_t E, int nv, const double* __restrict__ buf) {
+    const int64_t row = (int64_t)nv * NP + 1;
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n * row) return;
+    const int64_t m = i / row, r = i % row;
+    const int64_t e = idx[m];
+    if (r < (int64_t)nv * NP) u[((r / NP) * E + e) * NP + r % NP] = buf[i];
+    else if (alpha) alpha[e] = buf[i];
+}
+
 }  // namespace
+
+cudaError_t launch_pack(const double* u, const double* alpha, const int32_t* idx, int64_t n, int64_t E, int nv,
+                        double* buf, cudaStream_t s) {
+    const int64_t total = n * ((int64_t)nv * NP + 1);
+    if (total > 0) k_pack<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(u, alpha, idx, n, E, nv, buf);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_unpack(double* u, double* alpha, const int32_t* idx, int64_t n, int64_t E, int nv,
+                          const double* buf, cudaStream_t s) {
+    const int64_t total = n * ((int64_t)nv * NP + 1);
+    if (total > 0) k_unpack<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(u, alpha, idx, n, E, nv, buf);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_ctrl_reset(Control* c, cudaStream_t s) {
     k_ctrl_reset<<<MAX_GROUPS / 256, 256, 0, s>>>(c);

@@ -10,7 +10,8 @@
 namespace nemo {
 
 struct StageArgs {
-    int64_t E;
+    int64_t E;                // element stride of the SoA arrays
+    int64_t E_own;            // elements processed: [0, E_own); [E_own, E) are ghost copies (neighbour data)
     const double* u_in;       // [V][E][64]
     double* u_out;            // [V][E][64]
     double* reg;              // [V][E][64] LSRK register (FP64)
@@ -60,8 +61,9 @@ cudaError_t launch_mortar(const MortarArgs& a, cudaStream_t s);
 // plain FP64 Euler path (stage_fp64.cu)
 cudaError_t setup_stage_euler64(const OpConsts& ops);
 cudaError_t launch_stage_euler64(const StageArgs& a, bool blend, bool ind, bool rhs_only, cudaStream_t s);
-cudaError_t launch_totals64(const double* u, const double* delta, int64_t E, int nv, double* part, double* out,
-                            cudaStream_t s);
+// conserved totals of the first n elements of an SoA state with element stride E
+cudaError_t launch_totals64(const double* u, const double* delta, int64_t E, int64_t n, int nv, double* part,
+                            double* out, cudaStream_t s);
 int stage_smem_bytes64();
 
 // FP32-bulk Euler path (stage_fp32.cu)
@@ -85,6 +87,11 @@ cudaError_t mlp_adam_launch(float* W, const float* grad, float* m, float* v, int
 cudaError_t mlp_forward_launch(const float* feat, int64_t n, const float* W, float amax, float* out, cudaStream_t s);
 
 // control kernels (control.cu)
+// element exchange (partitioned runs): buf[m] = (state of element idx[m], V x 64, then its raw alpha)
+cudaError_t launch_pack(const double* u, const double* alpha, const int32_t* idx, int64_t n, int64_t E, int nv,
+                        double* buf, cudaStream_t s);
+cudaError_t launch_unpack(double* u, double* alpha, const int32_t* idx, int64_t n, int64_t E, int nv,
+                          const double* buf, cudaStream_t s);
 cudaError_t launch_ctrl_reset(Control* c, cudaStream_t s);
 cudaError_t launch_ctrl_set_dt(Control* c, double dt, cudaStream_t s);
 cudaError_t launch_ctrl_step(Control* c, cudaStream_t s);

@@ -177,6 +177,7 @@ struct Lib {
     char err[512] = "";
 
     int64_t E = 0;
+    int64_t E_own = 0;            // elements advanced by this process; [E_own, E) are ghost copies
     int V = 5;
     bool has_mesh = false, has_state = false;
     int ngroups = 1;
@@ -274,6 +275,7 @@ int mlp_t_offset() { return (MLP_NPACK + 3) / 4 * 4; }
 StageArgs stage_args(int st, bool rhs_only) {
     StageArgs a{};
     a.E = g.E;
+    a.E_own = g.E_own;
     a.u_in = g.u[g.cur];
     a.u_out = g.u[g.cur ^ 1];
     a.reg = g.reg;
@@ -599,6 +601,7 @@ int nemo_gpu_set_mesh(int64_t nelems, const double* delta, const double* center,
     }
     release_mesh();
     g.E = E;
+    g.E_own = E;
     const size_t bytes = sizeof(double) * (size_t)g.V * E * NP;
     CK(cudaMalloc(&g.u[0], bytes));
     CK(cudaMalloc(&g.u[1], bytes));
@@ -636,6 +639,35 @@ int nemo_gpu_set_mesh(int64_t nelems, const double* delta, const double* center,
     c.epoch = 1u;   // mortar flags start at 0: never equal to a launch's epoch before it sets them
     CK(cudaMemcpy(g.ctrl, &c, sizeof c, cudaMemcpyHostToDevice));
     g.has_mesh = true;
+    return NEMO_OK;
+}
+
+int nemo_gpu_set_owned(int64_t n_owned) {
+    if (!g.has_mesh) return fail(NEMO_ERR_STATE, "set the mesh first");
+    if (n_owned < 1 || n_owned > g.E) return fail(NEMO_ERR_ARG, "n_owned must be in [1, %lld]", (long long)g.E);
+    g.E_own = n_owned;
+    release_graphs();
+    g.prepared = false;
+    return NEMO_OK;
+}
+
+int nemo_gpu_pack_elements(const int32_t* idx_dev, int64_t n, double* buf_dev) {
+    int st = ensure_ready();
+    if (st) return st;
+    if (n < 0 || (n > 0 && (!idx_dev || !buf_dev))) return fail(NEMO_ERR_ARG, "bad pack arguments");
+    if ((st = prepare_if_needed())) return st;
+    CK(launch_pack(g.u[g.cur], blended() ? g.alpha[g.cur] : nullptr, idx_dev, n, g.E, g.V, buf_dev, g.stream));
+    CK(cudaStreamSynchronize(g.stream));
+    return NEMO_OK;
+}
+
+int nemo_gpu_unpack_elements(const int32_t* idx_dev, int64_t n, const double* buf_dev) {
+    int st = ensure_ready();
+    if (st) return st;
+    if (n < 0 || (n > 0 && (!idx_dev || !buf_dev))) return fail(NEMO_ERR_ARG, "bad unpack arguments");
+    if ((st = prepare_if_needed())) return st;
+    CK(launch_unpack(g.u[g.cur], blended() ? g.alpha[g.cur] : nullptr, idx_dev, n, g.E, g.V, buf_dev, g.stream));
+    CK(cudaStreamSynchronize(g.stream));
     return NEMO_OK;
 }
 
@@ -871,7 +903,7 @@ int nemo_gpu_totals(double* out) {
     int st = ensure_ready();
     if (st) return st;
     if (!out) return fail(NEMO_ERR_ARG, "out is NULL");
-    CK(launch_totals64(g.u[g.cur], g.delta, g.E, g.V, g.part, g.tot, g.stream));
+    CK(launch_totals64(g.u[g.cur], g.delta, g.E, g.E_own, g.V, g.part, g.tot, g.stream));
     double tmp[16] = {0};
     CK(cudaMemcpyAsync(tmp, g.tot, sizeof(double) * g.V, cudaMemcpyDeviceToHost, g.stream));
     CK(cudaStreamSynchronize(g.stream));

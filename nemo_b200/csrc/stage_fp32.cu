@@ -452,7 +452,7 @@ __device__ __forceinline__ void epilogue32(const StageArgs& a, const double* su,
     if (!a.alpha_out && !need_lam) return;
     __syncthreads();
     if (threadIdx.x == 0) {
-        const int nel = (int)min((int64_t)EPC, a.E - (e - el));
+        const int nel = (int)min((int64_t)EPC, a.E_own - (e - el));
         if (a.alpha_out && a.mlp32) {
             unsigned long long nfb = 0, nj = 0;
             double js = 0.0;
@@ -562,7 +562,7 @@ __device__ __forceinline__ void tile32(const StageArgs& a, const Smem32& S, int6
     const int tid = threadIdx.x;
     const int64_t E = a.E;
     const int64_t e0 = tile * EPC;
-    const int nel = (int)min((int64_t)EPC, E - e0);
+    const int nel = (int)min((int64_t)EPC, a.E_own - e0);
 
     if (tid < EPC) {
         s_bad[tid] = 0;
@@ -865,7 +865,7 @@ __global__ void __launch_bounds__(NT, 3) k_stage_euler32p(StageArgs a, MortarArg
     load_mlp32(a, s_w);
     const Smem32 S = smem32(smem, &bar, s_alpha, s_bad, s_w);
     mbar_init32(&bar);
-    const int64_t ntiles = (a.E + EPC - 1) / EPC;
+    const int64_t ntiles = (a.E_own + EPC - 1) / EPC;
     const int64_t npairs = (ma.nm + mortar::MPB - 1) / mortar::MPB;
     unsigned phase = 0;
     for (;;) {
@@ -900,7 +900,7 @@ int stage_smem_bytes32() {
 }
 
 cudaError_t launch_stage_euler32(const StageArgs& a, bool blend, bool rhs_only, cudaStream_t s) {
-    const int grid = (int)((a.E + EPC - 1) / EPC);
+    const int grid = (int)((a.E_own + EPC - 1) / EPC);
     const int smem = stage_smem_bytes32();
     if (rhs_only) {
         if (blend) k_stage_euler32<true, true><<<grid, NT, smem, s>>>(a);
@@ -964,7 +964,7 @@ cudaError_t setup_stage_mhd32() {
 }
 
 cudaError_t launch_stage_mhd32(const StageArgs& a, bool blend, bool rhs_only, cudaStream_t s) {
-    const int grid = (int)((a.E + mhd::EPC - 1) / mhd::EPC);
+    const int grid = (int)((a.E_own + mhd::EPC - 1) / mhd::EPC);
     const int smem = stage_smem_bytes_mhd32();
     if (rhs_only) {
         if (blend) k_stage_mhd<float, true, true><<<grid, mhd::NT, smem, s>>>(a);

@@ -295,7 +295,7 @@ __global__ void __launch_bounds__(NT, 1) k_stage_euler64(StageArgs a) {
     const int tid = threadIdx.x;
     const int64_t E = a.E;
     const int64_t e0 = (int64_t)blockIdx.x * EPC;
-    const int nel = (int)min((int64_t)EPC, E - e0);
+    const int nel = (int)min((int64_t)EPC, a.E_own - e0);
 
     if (tid < EPC) {
         s_bad[tid] = 0;
@@ -556,11 +556,11 @@ __global__ void __launch_bounds__(NT, 1) k_stage_euler64(StageArgs a) {
 
 // Conserved totals: per-element weighted sums in the oracle's order, then a serial sum per
 // variable (deterministic, bit-reproducible).
-__global__ void k_totals_elem64(const double* __restrict__ u, const double* __restrict__ delta, int64_t E, int nv,
-                                double* __restrict__ part) {
+__global__ void k_totals_elem64(const double* __restrict__ u, const double* __restrict__ delta, int64_t E,
+                                int64_t n, int nv, double* __restrict__ part) {
     const OpConsts& k = c_ops64;
     const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= E) return;
+    if (e >= n) return;
     const double vol = delta[e * 3 + 0] * delta[e * 3 + 1] * delta[e * 3 + 2];
     for (int v = 0; v < nv; ++v) {
         double s = 0.0;
@@ -568,7 +568,7 @@ __global__ void k_totals_elem64(const double* __restrict__ u, const double* __re
         for (int kk = 0; kk < NN; ++kk)
             for (int j = 0; j < NN; ++j)
                 for (int i = 0; i < NN; ++i) s = s + k.wt[i] * k.wt[j] * k.wt[kk] * ue[nidx(i, j, kk)];
-        part[(int64_t)v * E + e] = vol * s;
+        part[(int64_t)v * n + e] = vol * s;
     }
 }
 
@@ -586,7 +586,7 @@ __global__ void k_totals_sum64(const double* __restrict__ part, int64_t E, int n
 int stage_smem_bytes64() { return (V * EPC * NP + 6 * EPC * NP + 2 * V * EPC * NP) * (int)sizeof(double); }
 
 cudaError_t launch_stage_euler64(const StageArgs& a, bool blend, bool ind, bool rhs_only, cudaStream_t s) {
-    const int grid = (int)((a.E + EPC - 1) / EPC);
+    const int grid = (int)((a.E_own + EPC - 1) / EPC);
     const int smem = stage_smem_bytes64();
     (void)ind;
     if (rhs_only) {
@@ -613,10 +613,10 @@ cudaError_t setup_stage_euler64(const OpConsts& ops) {
     return cudaMemcpyToSymbol(c_ops64, &ops, sizeof(OpConsts));
 }
 
-cudaError_t launch_totals64(const double* u, const double* delta, int64_t E, int nv, double* part, double* out,
-                            cudaStream_t s) {
-    k_totals_elem64<<<(unsigned)((E + 127) / 128), 128, 0, s>>>(u, delta, E, nv, part);
-    k_totals_sum64<<<1, 32, 0, s>>>(part, E, nv, out);
+cudaError_t launch_totals64(const double* u, const double* delta, int64_t E, int64_t n, int nv, double* part,
+                            double* out, cudaStream_t s) {
+    k_totals_elem64<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(u, delta, E, n, nv, part);
+    k_totals_sum64<<<1, 32, 0, s>>>(part, n, nv, out);
     return cudaGetLastError();
 }
 
@@ -640,7 +640,7 @@ cudaError_t setup_stage_mhd64() {
 }
 
 cudaError_t launch_stage_mhd64(const StageArgs& a, bool blend, bool rhs_only, cudaStream_t s) {
-    const int grid = (int)((a.E + mhd::EPC - 1) / mhd::EPC);
+    const int grid = (int)((a.E_own + mhd::EPC - 1) / mhd::EPC);
     const int smem = stage_smem_bytes_mhd64();
     if (rhs_only) {
         if (blend) k_stage_mhd<double, true, true><<<grid, mhd::NT, smem, s>>>(a);

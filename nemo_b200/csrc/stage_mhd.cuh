@@ -327,7 +327,7 @@ __global__ void __launch_bounds__(mhd::NT, 1) k_stage_mhd(StageArgs a) {
     const int tid = threadIdx.x;
     const int64_t E = a.E;
     const int64_t e0 = (int64_t)blockIdx.x * MEPC;
-    const int nel = (int)min((int64_t)MEPC, E - e0);
+    const int nel = (int)min((int64_t)MEPC, a.E_own - e0);
     const R kap = (R)k.kappa, mu0 = (R)k.mu0;
     const R ch = (R)ctrl->glm_ch;
 

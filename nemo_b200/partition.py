@@ -1,0 +1,193 @@
+"""Element partition of a mesh over processes, with ghost copies of the face neighbours.
+
+The reference partitions its quads over MPI ranks along the p4est space-filling curve and exchanges
+the payloads of the partition-boundary quads every stage (source/mesh/p4est/mesh_utils_mod.f90:
+623-675 for the exchange, :1014- for the partition); the time step is an MPI_Allreduce minimum
+(source/kernel/mcfv/3d/kernel_timestep_mod.f90:48-52).  Here rank r takes a contiguous range of the
+element list (Morton order, so the ranges are compact), and its local mesh is those elements followed
+by ghost copies of every element that shares a side with one of them (conforming neighbours and the
+other quads of a 2:1 mortar).  Before every RK stage each rank sends the current state and raw
+blending coefficient of the owned elements that other ranks hold as ghosts; the ghosts' remaining
+faces become boundary sides (they are never advanced, only read).  Each element's update only reads
+its own state and its neighbours' traces, so every owned element evolves exactly as in the unsplit
+run.
+
+One exchange per stage, point to point (torch.distributed isend/irecv: NCCL with device buffers on
+GPUs, gloo with host buffers on CPUs), and one minimum reduction of the time step per step.
+"""
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from .mesh import Mesh
+
+
+@dataclass
+class Part:
+    """One rank's share: local mesh (owned elements first), global id of each local element, and
+    the exchange plan (local element indices, matched in order between sender and receiver)."""
+    rank: int
+    mesh: Mesh
+    n_owned: int
+    glob: np.ndarray                                  # [E_local] global element ids
+    send: dict = field(default_factory=dict)          # peer -> local owned indices to send
+    recv: dict = field(default_factory=dict)          # peer -> local ghost indices to fill
+
+
+def owner_ranges(E, nranks):
+    """Contiguous, balanced element ranges [lo_r, hi_r) along the element order."""
+    b = [(E * r) // nranks for r in range(nranks + 1)]
+    return [(b[r], b[r + 1]) for r in range(nranks)]
+
+
+def partition(mesh, nranks):
+    """Split mesh over nranks ranks; returns [Part] (one per rank)."""
+    E = mesh.E
+    ranges = owner_ranges(E, nranks)
+    owner = np.empty(E, dtype=np.int64)
+    for r, (lo, hi) in enumerate(ranges):
+        owner[lo:hi] = r
+    # quads of every side (1, 2 or 5 of them)
+    side_elems = []
+    for s in range(mesh.S):
+        q = []
+        for h in range(2):
+            n = int(mesh.side_nquads[s, h])
+            q.extend(int(x) for x in mesh.side_quads[s, h, :n])
+        side_elems.append(q)
+    parts = []
+    for r, (lo, hi) in enumerate(ranges):
+        sides = [s for s in range(mesh.S) if any(lo <= e < hi for e in side_elems[s])]
+        need = sorted({e for s in sides for e in side_elems[s] if not lo <= e < hi},
+                      key=lambda e: (owner[e], e))
+        glob = np.concatenate([np.arange(lo, hi), np.asarray(need, dtype=np.int64)])
+        loc = {int(g): i for i, g in enumerate(glob)}
+        Q, F, NQ, B = [], [], [], []
+        covered = set()
+        for s in sides:
+            q = np.full((2, 4), -1, dtype=np.int32)
+            for h in range(2):
+                n = int(mesh.side_nquads[s, h])
+                for k in range(n):
+                    gq = int(mesh.side_quads[s, h, k])
+                    q[h, k] = loc[gq]
+                    covered.add((loc[gq], int(mesh.side_faceid[s, h])))
+            Q.append(q)
+            F.append(mesh.side_faceid[s])
+            NQ.append(mesh.side_nquads[s])
+            B.append(mesh.boundary[s])
+        # faces of ghosts that no included side covers: boundary sides (mirrored state, never used)
+        for i in range(hi - lo, len(glob)):
+            for f in range(6):
+                if (i, f) not in covered:
+                    q = np.full((2, 4), -1, dtype=np.int32)
+                    q[0, 0] = i
+                    Q.append(q)
+                    F.append(np.array([f, f ^ 1], dtype=np.int8))
+                    NQ.append(np.array([1, 0], dtype=np.int8))
+                    B.append(1 + f)
+        gl = glob
+        local = Mesh(mesh.delta[gl], mesh.center[gl], np.stack(Q), np.stack(F), np.stack(NQ),
+                     np.asarray(B, dtype=np.int32), level=mesh.level[gl])
+        parts.append(Part(rank=r, mesh=local, n_owned=hi - lo, glob=glob))
+    # exchange plan: rank r receives its ghosts owned by p; p sends them in the same (global) order
+    for r, pr in enumerate(parts):
+        ghosts = pr.glob[pr.n_owned:]
+        for p in range(nranks):
+            sel = np.nonzero(owner[ghosts] == p)[0]
+            if len(sel) == 0:
+                continue
+            pr.recv[p] = (pr.n_owned + sel).astype(np.int32)
+            lo_p = ranges[p][0]
+            parts[p].send[r] = (ghosts[sel] - lo_p).astype(np.int32)
+    return parts
+
+
+def exchange(part, dist, get_rows, set_rows, make_buffer):
+    """One ghost refresh: get_rows(idx) -> buffer of those local elements, set_rows(idx, buffer);
+    make_buffer(n) -> an empty receive buffer for n elements.  Sends and receives are posted
+    together (batch_isend_irecv) so no ordering between peers is needed."""
+    ops, incoming = [], []
+    for peer, idx in sorted(part.send.items()):
+        ops.append(dist.P2POp(dist.isend, get_rows(idx), peer))
+    for peer, idx in sorted(part.recv.items()):
+        buf = make_buffer(len(idx))
+        incoming.append((idx, buf))
+        ops.append(dist.P2POp(dist.irecv, buf, peer))
+    if ops:
+        for req in dist.batch_isend_irecv(ops):
+            req.wait()
+    for idx, buf in incoming:
+        set_rows(idx, buf)
+
+
+class PartitionedRun:
+    """Advance one rank's share on its GPU: ghosts refreshed before every stage through the library's
+    pack/unpack entry points, Δt = all-reduce minimum of the ranks' CFL bounds.  Euler only (the GLM
+    cleaning speed of MHD would need its own all-reduce of λmax and vmax)."""
+
+    def __init__(self, cfg, part, dist, host_buffers=None):
+        import torch
+        from . import abi
+        from .solver import Solver
+        if cfg.eqn != abi.EQN_EULER:
+            raise ValueError("partitioned runs support the Euler equations only")
+        if cfg.n_vars != 5:
+            raise ValueError("n_vars must be 5")
+        self.torch, self.abi, self.dist, self.part = torch, abi, dist, part
+        self.cfg = cfg
+        self.s = Solver(cfg, part.mesh)
+        abi.call("nemo_gpu_set_owned", int(part.n_owned))
+        self.row = cfg.n_vars * 64 + 1
+        # gloo moves host tensors, NCCL device tensors
+        self.host = (dist.get_backend() != "nccl") if host_buffers is None else host_buffers
+        dev = torch.device("cuda", torch.cuda.current_device())
+        self.idx_dev = {}
+        for d in (part.send, part.recv):
+            for peer, idx in d.items():
+                self.idx_dev[id(idx)] = torch.as_tensor(idx, dtype=torch.int32, device=dev)
+        self.dev = dev
+
+    def _get(self, idx):
+        t = self.torch
+        i = self.idx_dev[id(idx)]
+        buf = t.empty((len(idx), self.row), dtype=t.float64, device=self.dev)
+        self.abi.call("nemo_gpu_pack_elements", self.abi.ctypes.c_void_p(i.data_ptr()), len(idx),
+                      self.abi.ctypes.c_void_p(buf.data_ptr()))
+        return buf.cpu() if self.host else buf
+
+    def _set(self, idx, buf):
+        i = self.idx_dev[id(idx)]
+        b = buf.to(self.dev) if self.host else buf
+        b = b.contiguous()
+        self.abi.call("nemo_gpu_unpack_elements", self.abi.ctypes.c_void_p(i.data_ptr()), len(idx),
+                      self.abi.ctypes.c_void_p(b.data_ptr()))
+
+    def _buf(self, n):
+        t = self.torch
+        return t.empty((n, self.row), dtype=t.float64, device="cpu" if self.host else self.dev)
+
+    def upload(self, u_local):
+        self.s.upload(u_local)
+
+    def exchange(self):
+        exchange(self.part, self.dist, self._get, self._set, self._buf)
+
+    def step(self):
+        t = self.torch
+        self.exchange()   # ghosts' raw blending coefficients for the CFL-independent first stage
+        dt_loc, _ = self.s.calc_timestep(self.cfg.cfl)
+        dt = t.tensor([dt_loc], dtype=t.float64, device="cpu" if self.host else self.dev)
+        self.dist.all_reduce(dt, op=self.dist.ReduceOp.MIN)
+        dt = float(dt.item())
+        for st in range(1, 6):
+            if st > 1:
+                self.exchange()
+            self.s.stage(st, dt)
+        return dt
+
+    def run(self, nsteps):
+        return [self.step() for _ in range(nsteps)]
+
+    def download_owned(self):
+        return self.s.download()[:, : self.part.n_owned]
