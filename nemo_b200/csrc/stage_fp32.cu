@@ -47,32 +47,35 @@ __device__ __forceinline__ bool mbar_wait32(uint64_t* bar, unsigned phase) {
 }
 
 // Stage the tile's state (and, from the second RK stage on, its register) into shared memory with
-// 1D bulk copies (V arrays of nel*64 doubles, contiguous per variable), completing on the CTA's
-// mbarrier (initialised once by mbar_init32; one phase per tile).
+// 1D bulk copies (V arrays of nel*64 doubles, contiguous per variable).  The state completes on
+// bar[0] and the register on bar[1], so the flux phase starts as soon as the state has arrived and
+// the register keeps streaming in until the update needs it.  Both barriers are initialised once
+// per CTA (mbar_init32); each tile is one phase.
 __device__ __forceinline__ void tile_issue32(double* su, const double* __restrict__ u, double* sg,
                                              const double* __restrict__ reg, int64_t E, int64_t e0, int nel,
                                              uint64_t* bar) {
     if (threadIdx.x == 0) {
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        unsigned b = smem_u32(bar);
-        unsigned bytes = (unsigned)(nel * NP * 8);
-        unsigned total = bytes * V * (reg ? 2u : 1u);
-        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(b), "r"(total) : "memory");
+        const unsigned bytes = (unsigned)(nel * NP * 8);
+        const unsigned b0 = smem_u32(bar), b1 = smem_u32(bar + 1);
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(b0), "r"(bytes * V) : "memory");
         for (int v = 0; v < V; ++v) {
             asm volatile(
                 "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
                     smem_u32(su + v * EPC * NP)),
-                "l"(u + ((int64_t)v * E + e0) * NP), "r"(bytes), "r"(b)
+                "l"(u + ((int64_t)v * E + e0) * NP), "r"(bytes), "r"(b0)
                 : "memory");
         }
-        if (reg)
+        if (reg) {
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(b1), "r"(bytes * V) : "memory");
             for (int v = 0; v < V; ++v) {
                 asm volatile(
                     "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
                         smem_u32(sg + v * EPC * NP)),
-                    "l"(reg + ((int64_t)v * E + e0) * NP), "r"(bytes), "r"(b)
+                    "l"(reg + ((int64_t)v * E + e0) * NP), "r"(bytes), "r"(b1)
                     : "memory");
             }
+        }
     }
 }
 
@@ -497,7 +500,7 @@ struct Smem32 {
     double* sg;        // [V][EPC][64] FP64 RK register
     float* sq;         // [NQ][EPC][64] FP32 node data
     float* sR;         // [V][EPC][64] FP32 rhs terms
-    uint64_t* bar;     // TMA completion barrier (initialised once per CTA)
+    uint64_t* bar;     // TMA completion barriers [2]: state, register (initialised once per CTA)
     float* s_alpha;    // [EPC]
     int* s_bad;        // [EPC]
     const float* s_w;  // learned indicator, transposed layout
@@ -535,10 +538,10 @@ __device__ __forceinline__ void mortar_acquire(const uint32_t* flag, uint32_t ep
     atomicOr(&ctrl->error, 4);
 }
 
-__device__ __forceinline__ void mbar_init32(uint64_t* bar) {
+__device__ __forceinline__ void mbar_init32(uint64_t* bar) {   // bar[0]: state, bar[1]: register
     if (threadIdx.x == 0) {
-        unsigned b = smem_u32(bar);
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(b) : "memory");
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)) : "memory");
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar + 1)) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
@@ -777,7 +780,8 @@ __device__ __forceinline__ void tile32(const StageArgs& a, const Smem32& S, int6
         __syncthreads();
     }
 
-    // ---- FP64 register/state update of the thread's x-line nodes
+    // ---- FP64 register/state update of the thread's x-line nodes (the register has arrived)
+    if (load_reg && !tile_wait32(S.bar + 1, phase, ctrl)) return;
     const int st = a.stage;
     const double A = rk_a(st);
     const double cdt = a.group ? (active ? rk_c(st) * ctrl->dt[a.group[e]] : 0.0) : rk_c(st) * ctrl->dt[0];
@@ -834,14 +838,14 @@ __device__ __forceinline__ void tile32(const StageArgs& a, const Smem32& S, int6
 template <bool BLEND, bool RHS_ONLY>
 __global__ void __launch_bounds__(NT, 3) k_stage_euler32(StageArgs a) {
     extern __shared__ __align__(128) double smem[];
-    __shared__ uint64_t bar;
+    __shared__ uint64_t bar[2];
     __shared__ float s_alpha[EPC];
     __shared__ int s_bad[EPC];
     __shared__ __align__(16) float s_w[MLP_NT];   // learned indicator, transposed layout
     if (!RHS_ONLY && !a.prep_only && a.ctrl->done) return;
     load_mlp32(a, s_w);
-    const Smem32 S = smem32(smem, &bar, s_alpha, s_bad, s_w);
-    mbar_init32(&bar);
+    const Smem32 S = smem32(smem, bar, s_alpha, s_bad, s_w);
+    mbar_init32(bar);
     tile32<BLEND, RHS_ONLY, false>(a, S, (int64_t)blockIdx.x, 0u, 0u);
 }
 
@@ -853,7 +857,7 @@ __global__ void __launch_bounds__(NT, 3) k_stage_euler32(StageArgs a) {
 template <bool BLEND>
 __global__ void __launch_bounds__(NT, 3) k_stage_euler32p(StageArgs a, MortarArgs ma) {
     extern __shared__ __align__(128) double smem[];
-    __shared__ uint64_t bar;
+    __shared__ uint64_t bar[2];
     __shared__ float s_alpha[EPC];
     __shared__ int s_bad[EPC];
     __shared__ __align__(16) float s_w[MLP_NT];
@@ -863,8 +867,8 @@ __global__ void __launch_bounds__(NT, 3) k_stage_euler32p(StageArgs a, MortarArg
     const uint32_t epoch = ctrl->epoch;
     ma.epoch = epoch;
     load_mlp32(a, s_w);
-    const Smem32 S = smem32(smem, &bar, s_alpha, s_bad, s_w);
-    mbar_init32(&bar);
+    const Smem32 S = smem32(smem, bar, s_alpha, s_bad, s_w);
+    mbar_init32(bar);
     const int64_t ntiles = (a.E_own + EPC - 1) / EPC;
     const int64_t npairs = (ma.nm + mortar::MPB - 1) / mortar::MPB;
     unsigned phase = 0;
