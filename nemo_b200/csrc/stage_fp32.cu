@@ -108,6 +108,20 @@ __device__ __forceinline__ void tile_store_wait32() {
     asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
 }
 
+// 1/x in FP64 from the FP32 reciprocal by two Newton steps (relative error ~1e-16 for the positive,
+// normal densities it is used on; the FP32 form needs no correctly rounded division here).
+__device__ __forceinline__ double rcp64(double x) {
+    double y = (double)__frcp_rn((float)x);
+    y = y * fma(-x, y, 2.0);
+    return y * fma(-x, y, 2.0);
+}
+
+// Admissibility screen without a division: rho > 0 and rho E > |m|^2 / 2 (same sign as the
+// pressure for rho > 0), with a small relative margin so borderline nodes go to the exact check.
+__device__ __forceinline__ bool admissible_screen(const double* q) {
+    return q[0] > 0.0 && q[0] * q[4] > 0.5 * (q[1] * q[1] + q[2] * q[2] + q[3] * q[3]) * (1.0 + 1e-12);
+}
+
 // Per-node FP32 primitives in the frame of direction d.
 struct P32 {
     float rho, vn, vt1, vt2, p, E;
@@ -264,7 +278,7 @@ __device__ __forceinline__ void epilogue32(const StageArgs& a, const double* su,
             const double r = su[(0 * EPC + el) * NP + n];
             const double mx = su[(1 * EPC + el) * NP + n], my = su[(2 * EPC + el) * NP + n];
             const double mz = su[(3 * EPC + el) * NP + n], en = su[(4 * EPC + el) * NP + n];
-            const double ir = 1.0 / r;
+            const double ir = rcp64(r);
             const double prd = k.km1 * (en - 0.5 * ir * (mx * mx + my * my + mz * mz));
             qr[i] = (float)r;
             qp[i] = (float)prd;
@@ -587,6 +601,23 @@ __device__ __forceinline__ void tile32(const StageArgs& a, const Smem32& S, int6
     }
     const bool load_reg = !RHS_ONLY && !a.prep_only && a.stage > 0;
     tile_issue32(su, a.u_in, sg, load_reg ? a.reg : nullptr, E, e0, nel, S.bar);
+    if (!a.prep_only) {
+        // pull the neighbour traces that lie outside the tile into L1 while the tile streams in
+        const int pel = tid >> 4, pab = tid & 15;
+        if (pel < nel) {
+            const int64_t pe = e0 + pel;
+#pragma unroll
+            for (int f = 0; f < 6; ++f) {
+                const int32_t ne = a.nbr[pe * 6 + f];
+                if (ne >= 0 && (ne < e0 || ne >= e0 + nel)) {
+                    const int nn = line_node(f >> 1, pab & 3, pab >> 2, (f & 1) ? 0 : NN - 1);
+#pragma unroll
+                    for (int v = 0; v < V; ++v)
+                        asm volatile("prefetch.global.L1 [%0];" ::"l"(a.u_in + ((int64_t)v * E + ne) * NP + nn));
+                }
+            }
+        }
+    }
     __syncthreads();   // s_alpha / s_bad visible
     if (!tile_wait32(S.bar, phase, ctrl)) return;
 
@@ -608,15 +639,16 @@ __device__ __forceinline__ void tile32(const StageArgs& a, const Smem32& S, int6
             const double r = su[(0 * EPC + el) * NP + n];
             const double mx = su[(1 * EPC + el) * NP + n], my = su[(2 * EPC + el) * NP + n];
             const double mz = su[(3 * EPC + el) * NP + n], en = su[(4 * EPC + el) * NP + n];
-            const double ir = 1.0 / r;
+            const double ir = rcp64(r);
             const double vx = mx * ir, vy = my * ir, vz = mz * ir;
             const double pr = k.km1 * (en - 0.5 * (mx * vx + my * vy + mz * vz));
-            SQ(0, el, n) = (float)r;
+            const float rf = (float)r, pf = (float)pr;
+            SQ(0, el, n) = rf;
             SQ(1, el, n) = (float)vx;
             SQ(2, el, n) = (float)vy;
             SQ(3, el, n) = (float)vz;
-            SQ(4, el, n) = (float)pr;
-            SQ(5, el, n) = (float)(0.5 * r / pr);
+            SQ(4, el, n) = pf;
+            SQ(5, el, n) = 0.5f * rf / pf;
         }
     }
     __syncthreads();
@@ -810,7 +842,7 @@ __device__ __forceinline__ void tile32(const StageArgs& a, const Smem32& S, int6
                 double q[V];
 #pragma unroll
                 for (int v = 0; v < V; ++v) q[v] = su[(v * EPC + el) * NP + n];
-                ok = ok && isvalid64(q, k);
+                ok = ok && admissible_screen(q);   // flagged elements get the exact check in the repair
             }
             if (!ok) s_bad[el] = 1;
         }
