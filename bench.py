@@ -401,7 +401,8 @@ def main():
                        "schedule": {"chosen": "persistent" if tune_mode == 1 else "grid", "persistent_ctas": tune_ctas,
                                     "autotune_ms_per_step": {"grid": tune_ms[0], "persistent_1_per_sm": tune_ms[1],
                                                              "persistent_2_per_sm": tune_ms[2],
-                                                             "persistent_3_per_sm": tune_ms[3]}},
+                                                             "persistent_3_per_sm": tune_ms[3],
+                                                             "persistent_4_per_sm": tune_ms[4]}},
                        "groups": int(groups.max()) + 1 if groups is not None else 1,
                        "l2": f"working set (u in/out + register, 3 x {u.nbytes / 1e6:.0f} MB) larger than L2"},
             "clocks": clk.summary(),

@@ -229,11 +229,11 @@ int nemo_gpu_last_error(char* buf, int32_t len);
 
 /* Stage schedule autotuner (no reference counterpart: the reference has one CPU loop).  For the
    FP32 Euler form it times nsteps full steps of each candidate from the current state -- one CTA per
-   tile of 8 elements plus the mortar kernel, and the persistent kernel with 1, 2 or 3 CTAs per SM
-   taking the mortar pairs and then the tiles from a device queue -- restores the state, the
-   register, the indicator and the control block after each, and keeps the fastest.  mode_out
-   (0 grid, 1 persistent), ctas_out (persistent grid size) and ms_out[4] (ms per step of each
-   candidate, -1 if not run) may be NULL.  Other forms have one schedule (mode 0). */
+   tile of 8 elements plus the mortar kernel, and the persistent kernel with 1 to 4 CTAs per SM
+   (as many as fit) taking the mortar pairs and then the tiles from a device queue -- restores the
+   state, the register, the indicator and the control block after each, and keeps the fastest.
+   mode_out (0 grid, 1 persistent), ctas_out (persistent grid size) and ms_out[5] (ms per step of
+   each candidate, -1 if not run) may be NULL.  Other forms have one schedule (mode 0). */
 int nemo_gpu_autotune(int32_t nsteps, int32_t* mode_out, int32_t* ctas_out, double* ms_out);
 
 /* Set the FP32 Euler stage schedule directly (mode 0 grid, 1 persistent with ctas CTAs). */

@@ -929,7 +929,7 @@ int nemo_gpu_autotune(int32_t nsteps, int32_t* mode_out, int32_t* ctas_out, doub
     if (st) return st;
     if (nsteps < 1 || nsteps > 1000) return fail(NEMO_ERR_ARG, "nsteps must be in [1, 1000]");
     if (ms_out)
-        for (int i = 0; i < 4; ++i) ms_out[i] = -1.0;
+        for (int i = 0; i < 5; ++i) ms_out[i] = -1.0;
     const bool tunable = !is_mhd() && g.cfg.precision == NEMO_PREC_FP32;
     if (!tunable) {  // the other forms have a single schedule
         g.tune_mode = 0;
@@ -993,7 +993,7 @@ int nemo_gpu_autotune(int32_t nsteps, int32_t* mode_out, int32_t* ctas_out, doub
     if (e == cudaSuccess) e = save_or_restore(false, ctrial);
     double best = 1e300;
     int best_mode = 0, best_ctas = 0;
-    const int ncand = 1 + std::min(occ, 3);
+    const int ncand = 1 + std::min(occ, 4);
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     if (e == cudaSuccess) e = cudaEventCreate(&e0);
     if (e == cudaSuccess) e = cudaEventCreate(&e1);

@@ -46,18 +46,17 @@ __device__ __forceinline__ bool mbar_wait32(uint64_t* bar, unsigned phase) {
     return false;
 }
 
-// Stage the tile's state (and, from the second RK stage on, its register) into shared memory with
-// 1D bulk copies (V arrays of nel*64 doubles, contiguous per variable).  The state completes on
-// bar[0] and the register on bar[1], so the flux phase starts as soon as the state has arrived and
-// the register keeps streaming in until the update needs it.  Both barriers are initialised once
-// per CTA (mbar_init32); each tile is one phase.
-__device__ __forceinline__ void tile_issue32(double* su, const double* __restrict__ u, double* sg,
+// Stage the tile's state into shared memory with 1D bulk copies (V arrays of nel*64 doubles,
+// contiguous per variable), completing on the CTA's mbarrier (initialised once by mbar_init32; one
+// phase per tile).  The RK register does not pass through shared memory: the update reads and
+// writes it straight from global memory with coalesced accesses, after an L2 prefetch issued here.
+__device__ __forceinline__ void tile_issue32(double* su, const double* __restrict__ u,
                                              const double* __restrict__ reg, int64_t E, int64_t e0, int nel,
                                              uint64_t* bar) {
     if (threadIdx.x == 0) {
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         const unsigned bytes = (unsigned)(nel * NP * 8);
-        const unsigned b0 = smem_u32(bar), b1 = smem_u32(bar + 1);
+        const unsigned b0 = smem_u32(bar);
         asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(b0), "r"(bytes * V) : "memory");
         for (int v = 0; v < V; ++v) {
             asm volatile(
@@ -66,16 +65,11 @@ __device__ __forceinline__ void tile_issue32(double* su, const double* __restric
                 "l"(u + ((int64_t)v * E + e0) * NP), "r"(bytes), "r"(b0)
                 : "memory");
         }
-        if (reg) {
-            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(b1), "r"(bytes * V) : "memory");
-            for (int v = 0; v < V; ++v) {
-                asm volatile(
-                    "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                        smem_u32(sg + v * EPC * NP)),
-                    "l"(reg + ((int64_t)v * E + e0) * NP), "r"(bytes), "r"(b1)
-                    : "memory");
-            }
-        }
+        if (reg)
+            for (int v = 0; v < V; ++v)
+                asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(reg + ((int64_t)v * E + e0) * NP),
+                             "r"(bytes)
+                             : "memory");
     }
 }
 
@@ -88,19 +82,15 @@ __device__ __forceinline__ bool tile_wait32(uint64_t* bar, unsigned phase, Contr
     return ok;
 }
 
-// Write the tile's new state and register back with 1D bulk copies from shared memory.  The
-// calling thread waits until the copies have read shared memory before the CTA may exit.
-__device__ __forceinline__ void tile_store32(const double* su, double* __restrict__ u_out, const double* sg,
-                                             double* __restrict__ reg, int64_t E, int64_t e0, int nel) {
+// Write the tile's new state back with 1D bulk copies from shared memory.  The calling thread waits
+// until the copies have read shared memory before the CTA may reuse or leave it.
+__device__ __forceinline__ void tile_store32(const double* su, double* __restrict__ u_out, int64_t E, int64_t e0,
+                                             int nel) {
     const unsigned bytes = (unsigned)(nel * NP * 8);
-    for (int v = 0; v < V; ++v) {
+    for (int v = 0; v < V; ++v)
         asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(u_out + ((int64_t)v * E + e0) * NP),
                      "r"(smem_u32(su + v * EPC * NP)), "r"(bytes)
                      : "memory");
-        asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(reg + ((int64_t)v * E + e0) * NP),
-                     "r"(smem_u32(sg + v * EPC * NP)), "r"(bytes)
-                     : "memory");
-    }
     asm volatile("cp.async.bulk.commit_group;" ::: "memory");
 }
 
@@ -511,10 +501,9 @@ __device__ __forceinline__ void epilogue32(const StageArgs& a, const double* su,
 // Shared-memory carve-up of one CTA of the FP32 stage.
 struct Smem32 {
     double* su;        // [V][EPC][64] FP64 state
-    double* sg;        // [V][EPC][64] FP64 RK register
     float* sq;         // [NQ][EPC][64] FP32 node data
     float* sR;         // [V][EPC][64] FP32 rhs terms
-    uint64_t* bar;     // TMA completion barriers [2]: state, register (initialised once per CTA)
+    uint64_t* bar;     // TMA completion barrier of the state (initialised once per CTA)
     float* s_alpha;    // [EPC]
     int* s_bad;        // [EPC]
     const float* s_w;  // learned indicator, transposed layout
@@ -531,8 +520,7 @@ __device__ __forceinline__ void load_mlp32(const StageArgs& a, float* s_w) {
 __device__ __forceinline__ Smem32 smem32(double* smem, uint64_t* bar, float* s_alpha, int* s_bad, const float* s_w) {
     Smem32 S;
     S.su = smem;
-    S.sg = S.su + V * EPC * NP;
-    S.sq = reinterpret_cast<float*>(S.sg + V * EPC * NP);
+    S.sq = reinterpret_cast<float*>(S.su + V * EPC * NP);
     S.sR = S.sq + NQ * EPC * NP;
     S.bar = bar;
     S.s_alpha = s_alpha;
@@ -552,10 +540,9 @@ __device__ __forceinline__ void mortar_acquire(const uint32_t* flag, uint32_t ep
     atomicOr(&ctrl->error, 4);
 }
 
-__device__ __forceinline__ void mbar_init32(uint64_t* bar) {   // bar[0]: state, bar[1]: register
+__device__ __forceinline__ void mbar_init32(uint64_t* bar) {
     if (threadIdx.x == 0) {
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)) : "memory");
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar + 1)) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
@@ -570,7 +557,6 @@ __device__ __forceinline__ void tile32(const StageArgs& a, const Smem32& S, int6
     const OpConsts& k = c_ops32;
     Control* ctrl = a.ctrl;
     double* su = S.su;
-    double* sg = S.sg;
     float* sq = S.sq;
     float* sR = S.sR;
     float* s_alpha = S.s_alpha;
@@ -600,7 +586,7 @@ __device__ __forceinline__ void tile32(const StageArgs& a, const Smem32& S, int6
         s_alpha[tid] = al;
     }
     const bool load_reg = !RHS_ONLY && !a.prep_only && a.stage > 0;
-    tile_issue32(su, a.u_in, sg, load_reg ? a.reg : nullptr, E, e0, nel, S.bar);
+    tile_issue32(su, a.u_in, load_reg ? a.reg : nullptr, E, e0, nel, S.bar);
     if (!a.prep_only) {
         // pull the neighbour traces that lie outside the tile into L1 while the tile streams in
         const int pel = tid >> 4, pab = tid & 15;
@@ -812,40 +798,34 @@ __device__ __forceinline__ void tile32(const StageArgs& a, const Smem32& S, int6
         __syncthreads();
     }
 
-    // ---- FP64 register/state update of the thread's x-line nodes (the register has arrived)
-    if (load_reg && !tile_wait32(S.bar + 1, phase, ctrl)) return;
+    // ---- FP64 register/state update: thread ab of an element takes nodes ab + 16 q, so the register
+    // moves between global memory and registers in coalesced 128-byte rows
     const int st = a.stage;
     const double A = rk_a(st);
     const double cdt = a.group ? (active ? rk_c(st) * ctrl->dt[a.group[e]] : 0.0) : rk_c(st) * ctrl->dt[0];
     if (active) {
         bool ok = true;
 #pragma unroll
-        for (int v = 0; v < V; ++v)
+        for (int q = 0; q < 4; ++q) {
+            const int n = ab + 16 * q;
+            double qv[V];
 #pragma unroll
-            for (int i = 0; i < NN; ++i) {
-                const int n = nidx(i, la, lb);
+            for (int v = 0; v < V; ++v) {
                 const int s = (v * EPC + el) * NP + n;
                 const double rhs = -(double)sR[s];
                 const int64_t g = ((int64_t)v * E + e) * NP + n;
                 if (RHS_ONLY) {
                     a.rhs_out[g] = rhs;
                 } else {
-                    const double r2 = st == 0 ? rhs : A * sg[s] + rhs;
-                    sg[s] = r2;
+                    const double r2 = st == 0 ? rhs : A * a.reg[g] + rhs;
+                    a.reg[g] = r2;
                     su[s] = su[s] + cdt * r2;
                 }
+                qv[v] = su[s];
             }
-        if (!RHS_ONLY && a.positivity) {
-#pragma unroll
-            for (int i = 0; i < NN; ++i) {
-                const int n = nidx(i, la, lb);
-                double q[V];
-#pragma unroll
-                for (int v = 0; v < V; ++v) q[v] = su[(v * EPC + el) * NP + n];
-                ok = ok && admissible_screen(q);   // flagged elements get the exact check in the repair
-            }
-            if (!ok) s_bad[el] = 1;
+            if (!RHS_ONLY && a.positivity) ok = ok && admissible_screen(qv);   // exact check in the repair
         }
+        if (!ok) s_bad[el] = 1;
     }
     if (RHS_ONLY) return;
     __syncthreads();
@@ -853,10 +833,10 @@ __device__ __forceinline__ void tile32(const StageArgs& a, const Smem32& S, int6
         const bool repaired = repair_elem16<EPC>(su, el, ab, k);
         if (!repaired && ab == 0) atomicAdd(&ctrl->nbad, 1ull);
     }
-    // make the generic-proxy writes of su/sg visible to the bulk copies, then store the tile
+    // make the generic-proxy writes of su visible to the bulk copies, then store the tile
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncthreads();
-    if (tid == 0) tile_store32(su, a.u_out, sg, a.reg, E, e0, nel);
+    if (tid == 0) tile_store32(su, a.u_out, E, e0, nel);
     if (st == 4 && tile == 0 && tid == 0) {
         for (int g = 0; g < ctrl->ngroups; ++g) ctrl->t[g] = ctrl->t[g] + ctrl->dt[g];
         ctrl->steps += 1;
@@ -868,9 +848,9 @@ __device__ __forceinline__ void tile32(const StageArgs& a, const Smem32& S, int6
 
 
 template <bool BLEND, bool RHS_ONLY>
-__global__ void __launch_bounds__(NT, 3) k_stage_euler32(StageArgs a) {
+__global__ void __launch_bounds__(NT, 4) k_stage_euler32(StageArgs a) {
     extern __shared__ __align__(128) double smem[];
-    __shared__ uint64_t bar[2];
+    __shared__ uint64_t bar[1];
     __shared__ float s_alpha[EPC];
     __shared__ int s_bad[EPC];
     __shared__ __align__(16) float s_w[MLP_NT];   // learned indicator, transposed layout
@@ -887,9 +867,9 @@ __global__ void __launch_bounds__(NT, 3) k_stage_euler32(StageArgs a) {
 // was taken before any tile task, by a running CTA that waits on nothing, so the waits end.  The
 // last CTA to finish resets the counter and advances the epoch for the next launch.
 template <bool BLEND>
-__global__ void __launch_bounds__(NT, 3) k_stage_euler32p(StageArgs a, MortarArgs ma) {
+__global__ void __launch_bounds__(NT, 4) k_stage_euler32p(StageArgs a, MortarArgs ma) {
     extern __shared__ __align__(128) double smem[];
-    __shared__ uint64_t bar[2];
+    __shared__ uint64_t bar[1];
     __shared__ float s_alpha[EPC];
     __shared__ int s_bad[EPC];
     __shared__ __align__(16) float s_w[MLP_NT];
@@ -932,7 +912,7 @@ __global__ void __launch_bounds__(NT, 3) k_stage_euler32p(StageArgs a, MortarArg
 }
 
 int stage_smem_bytes32() {
-    return 2 * V * EPC * NP * (int)sizeof(double) + (NQ + V) * EPC * NP * (int)sizeof(float);
+    return V * EPC * NP * (int)sizeof(double) + (NQ + V) * EPC * NP * (int)sizeof(float);
 }
 
 cudaError_t launch_stage_euler32(const StageArgs& a, bool blend, bool rhs_only, cudaStream_t s) {

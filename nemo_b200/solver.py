@@ -114,7 +114,7 @@ class Solver:
         """Pick the stage schedule by timing (FP32 Euler form); returns (mode, ctas, ms per step of
         each candidate)."""
         mode, ctas = ctypes.c_int32(), ctypes.c_int32()
-        ms = np.zeros(4)
+        ms = np.zeros(5)
         call("nemo_gpu_autotune", int(nsteps), ctypes.byref(mode), ctypes.byref(ctas), abi.ptr(ms))
         return mode.value, ctas.value, ms
 
