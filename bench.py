@@ -278,6 +278,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
     ap.add_argument("--no-accuracy", action="store_true", help="skip the run to t_end that checks the L1 error")
+    ap.add_argument("--schedule", default="auto", choices=["auto", "grid", "persistent"],
+                    help="FP32 stage schedule: autotuned (default) or fixed (profiling runs)")
     args = ap.parse_args()
     assert args.warmup >= 3 or args.impl == "reference" or os.environ.get("NEMO_BENCH_ALLOW_SHORT")
 
@@ -320,7 +322,13 @@ def main():
     # ---- the chosen form: FP32 bulk + learned indicator, FP64 state/register/update/repair/reductions
     s = make_solver(args.workload, m, abi.PREC_FP32, learned=True, groups=groups)
     s.upload(u)
-    tune_mode, tune_ctas, tune_ms = s.autotune(nsteps=3)   # restores the state it times
+    if args.schedule == "auto":
+        tune_mode, tune_ctas, tune_ms = s.autotune(nsteps=3)   # restores the state it times
+    else:
+        import torch as _t
+        nsm = _t.cuda.get_device_properties(local).multi_processor_count
+        tune_mode, tune_ctas, tune_ms = (0, 0, [-1.0] * 5) if args.schedule == "grid" else (1, 4 * nsm, [-1.0] * 5)
+        s.set_schedule(tune_mode, tune_ctas)
     abi.call("nemo_gpu_stream", ctypes.byref(stream_ptr))
     stream = torch.cuda.ExternalStream(stream_ptr.value)
     s.run(nsteps=args.warmup)
