@@ -307,7 +307,7 @@ __device__ __forceinline__ void epilogue32(const StageArgs& a, const double* su,
                 }
             }
         }
-        __syncthreads();
+        __syncwarp();   // the element's 16 threads share one warp
         if (active) {
             for (int w = 0; w < nq; ++w) {
 #pragma unroll
@@ -319,7 +319,7 @@ __device__ __forceinline__ void epilogue32(const StageArgs& a, const double* su,
                 }
             }
         }
-        __syncthreads();
+        __syncwarp();   // the element's 16 threads share one warp
         if (active) {
             for (int w = 0; w < nq; ++w) {
 #pragma unroll
@@ -795,7 +795,7 @@ __device__ __forceinline__ void tile32(const StageArgs& a, const Smem32& S, int6
                     R = (d == 0 ? 0.0f : R) + cd * t[i][v];
                 }
         }
-        __syncthreads();
+        __syncwarp();   // the element's 16 threads share one warp
     }
 
     // ---- FP64 register/state update: thread ab of an element takes nodes ab + 16 q, so the register
@@ -828,7 +828,7 @@ __device__ __forceinline__ void tile32(const StageArgs& a, const Smem32& S, int6
         if (!ok) s_bad[el] = 1;
     }
     if (RHS_ONLY) return;
-    __syncthreads();
+    __syncwarp();   // the element's 16 threads share one warp
     if (a.positivity && active && s_bad[el]) {   // the element's 16 threads together
         const bool repaired = repair_elem16<EPC>(su, el, ab, k);
         if (!repaired && ab == 0) atomicAdd(&ctrl->nbad, 1ull);
