@@ -77,14 +77,14 @@ __device__ __noinline__ bool repair_elem(double* su, int el, const OpConsts& k) 
 }
 
 
-// The same repair done by the element's 16 threads together (a half-warp that calls it as a whole):
+// The same repair done by the element's 16 threads together (a half-warp that calls it as a whole),
+// for V variables and an admissibility test valid(q):
 // no per-thread tile arrays, so it inlines without a call frame.  Level 1 squeezes the 8 octants
 // (lanes 0..7, one octant each); level 2 squeezes the 8 nodes of each octant (lanes 0..7 and 8..15
 // take one octant each, four rounds).  Each lane sums its tile in the serial routine's node order,
 // the means run over the tiles in tile order, and all lanes of a block take the same squeeze steps.
-template <int EPC>
-__device__ __forceinline__ bool repair_elem16(double* su, int el, int lane, const OpConsts& k) {
-    constexpr int V = 5;
+template <int EPC, int V, typename Valid>
+__device__ __forceinline__ bool repair_coop16(double* su, int el, int lane, double decr, Valid valid) {
     auto at = [&](int v, int p) -> double& { return su[(v * EPC + el) * NP + p]; };
     const unsigned half = threadIdx.x & 16;
 #pragma unroll 1
@@ -115,7 +115,7 @@ __device__ __forceinline__ bool repair_elem16(double* su, int el, int lane, cons
                 tile[v] = acc;
             }
             if (!use) continue;
-            const bool bad = !isvalid64(tile, k);
+            const bool bad = !valid(tile);
             if (__ballot_sync(gm, bad) == 0u) continue;   // the block's tiles are admissible
             double mean[V], hile[V];
 #pragma unroll
@@ -129,11 +129,11 @@ __device__ __forceinline__ bool repair_elem16(double* su, int el, int lane, cons
             double squeeze = 1.0;
 #pragma unroll 1
             while (squeeze > 0.0) {
-                squeeze = fmax(0.0, squeeze - k.repair_decr);
+                squeeze = fmax(0.0, squeeze - decr);
                 double tv[V];
 #pragma unroll
                 for (int v = 0; v < V; ++v) tv[v] = mean[v] + squeeze * hile[v];
-                if (__ballot_sync(gm, !isvalid64(tv, k)) == 0u) break;
+                if (__ballot_sync(gm, !valid(tv)) == 0u) break;
             }
             for (int kx = k0; kx < k0 + nn; ++kx)
                 for (int jx = j0; jx < j0 + nn; ++jx)
@@ -152,9 +152,20 @@ __device__ __forceinline__ bool repair_elem16(double* su, int el, int lane, cons
         double qv[V];
 #pragma unroll
         for (int v = 0; v < V; ++v) qv[v] = at(v, p);
-        ok = ok && isvalid64(qv, k);
+        ok = ok && valid(qv);
     }
     return __ballot_sync(0xffffu << half, !ok) == 0u;
+}
+
+template <int EPC>
+__device__ __forceinline__ bool repair_elem16(double* su, int el, int lane, const OpConsts& k) {
+    return repair_coop16<EPC, 5>(su, el, lane, k.repair_decr, [&](const double* q) { return isvalid64(q, k); });
+}
+
+template <int EPC>
+__device__ __forceinline__ bool repair_elem16_mhd(double* su, int el, int lane, const OpConsts& k) {
+    return repair_coop16<EPC, 9>(su, el, lane, k.repair_decr,
+                                 [&](const double* q) { return m_isvalid<double>(q, k.kappa, k.mu0); });
 }
 
 // The same repair for the 9 GLM-MHD variables (MHD pressure in the admissibility check).

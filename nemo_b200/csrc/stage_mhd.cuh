@@ -507,8 +507,13 @@ __global__ void __launch_bounds__(mhd::NT, 1) k_stage_mhd(StageArgs a) {
     }
     if (RHS_ONLY) return;
     __syncthreads();
-    if (a.positivity && active && ab == 0 && s_bad[el]) {
-        if (!repair_elem_mhd<mhd::EPC>(su, el, k)) atomicAdd(&ctrl->nbad, 1ull);
+    if (a.positivity && active && s_bad[el]) {
+        if constexpr (sizeof(R) == 4) {   // FP32 form: the element's 16 threads (a half-warp) together
+            const bool repaired = repair_elem16_mhd<mhd::EPC>(su, el, ab, k);
+            if (!repaired && ab == 0) atomicAdd(&ctrl->nbad, 1ull);
+        } else if (ab == 0) {             // plain form: one thread (register budget of the FP64 kernel)
+            if (!repair_elem_mhd<mhd::EPC>(su, el, k)) atomicAdd(&ctrl->nbad, 1ull);
+        }
     }
     __syncthreads();
     if (active) {
