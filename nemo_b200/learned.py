@@ -141,6 +141,13 @@ def load(path=WEIGHTS):
             np.array(d["hi"], dtype=np.float32), d.get("meta", {}))
 
 
+def bf16_round(w):
+    """The FP64 values of the BF16-rounded weights (nearest, ties to even) that nemo_gpu_set_mlp keeps."""
+    b = np.asarray(w, dtype=np.float32).view(np.uint32).astype(np.uint64)
+    b = (b + 0x7FFF + ((b >> 16) & 1)) & 0xFFFF0000
+    return b.astype(np.uint32).view(np.float32).astype(np.float64)
+
+
 def install(path=WEIGHTS):
     """Load the trained network into the library (after nemo_gpu_init)."""
     w, lo, hi, _ = load(path)
