@@ -102,6 +102,17 @@ __device__ __forceinline__ int unrot(int d, int c) {
     return 5 + (d + c - 5) % 3;
 }
 
+__device__ __forceinline__ float hsum16m(float v) {
+#pragma unroll
+    for (int o = 8; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+__device__ __forceinline__ float hmin16m(float v) {
+#pragma unroll
+    for (int o = 8; o > 0; o >>= 1) v = fminf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
 __device__ __forceinline__ double silu_m(double x) { return x / (1.0 + pexp64(-x)); }
 __device__ __forceinline__ float silu_m(float x) { return x / (1.0f + __expf(-x)); }
 __device__ __forceinline__ double expneg(double x) { return pexp64(x); }
@@ -165,64 +176,147 @@ __device__ void epilogue_mhd(const StageArgs& a, const double* su, R* scr, unsig
             __syncthreads();
         }
         R* feat = q;
-        if (tid < nel) {
-            const R* m = scr + 3 * EPC * NP + tid * NP;
-            R total = R(0.0), clip1 = R(0.0), clip2 = R(0.0);
-            for (int cc = 0; cc < NN; ++cc)
-                for (int bj = 0; bj < NN; ++bj)
-                    for (int ai = 0; ai < NN; ++ai) {
-                        const R mv = m[nidx(ai, bj, cc)];
-                        const R e2 = mv * mv;
-                        total = total + e2;
-                        if (ai < NN - 1 && bj < NN - 1 && cc < NN - 1) clip1 = clip1 + e2;
-                        if (ai < NN - 2 && bj < NN - 2 && cc < NN - 2) clip2 = clip2 + e2;
-                    }
-            const R e1 = (total - clip1) / total;
-            const R e2 = (clip1 - clip2) / clip1;
-            const R energy = fmax(e1, e2);
-            R al = R(1.0) / (R(1.0) + expneg((R)k.ind_k * (energy - (R)k.ind_T)));
-            if (al < (R)k.alpha_min) al = R(0.0);
-            else if (al > (R)k.one_m_alpha_min) al = R(1.0);
-            s_am[tid] = fmin((R)k.alpha_max, al);
-            int fb = 0;
-            if (learned) {
-                R rs = R(0.0), ps = R(0.0), rmin = R(1e30), pmin = R(1e30);
-                for (int n = 0; n < NP; ++n) {
-                    R uu[V];
+        if constexpr (sizeof(R) == 4) {
+            // FP32 form: the element's 16 threads share the sums (modes / nodes lane + 16 q)
+            const int pel = tid >> 4, lane = tid & 15;
+            const bool act = pel < nel;
+            float total = 0.f, clip1 = 0.f, clip2 = 0.f;
+            if (act) {
+                const float* m = scr + 3 * EPC * NP + pel * NP;
 #pragma unroll
-                    for (int v = 0; v < V; ++v) uu[v] = (R)su[(v * EPC + tid) * NP + n];
-                    const R pr = m_pressure(uu, kap, mu0);
-                    rs = rs + uu[0];
-                    ps = ps + pr;
-                    rmin = fmin(rmin, uu[0]);
-                    pmin = fmin(pmin, pr);
-                }
-                if (rmin < R(0.1) * (rs / R(64.0)) || pmin < R(0.1) * (ps / R(64.0))) fb = 1;
-                for (int w = 0; w < 2; ++w) {
-                    const R* mw = scr + (4 + w) * EPC * NP + tid * NP;
-                    R tot = R(0.0), Eo[6] = {R(0), R(0), R(0), R(0), R(0), R(0)};
-                    for (int cc = 0; cc < NN; ++cc)
-                        for (int bj = 0; bj < NN; ++bj)
-                            for (int ai = 0; ai < NN; ++ai) {
-                                const R mv = mw[nidx(ai, bj, cc)];
-                                const R ee = mv * mv;
-                                tot = tot + ee;
-                                const int ord[3] = {ai, bj, cc};
-#pragma unroll
-                                for (int d = 0; d < 3; ++d) {
-                                    if (ord[d] == NN - 1) Eo[2 * d] = Eo[2 * d] + ee;
-                                    if (ord[d] == NN - 2) Eo[2 * d + 1] = Eo[2 * d + 1] + ee;
-                                }
-                            }
-                    for (int i = 0; i < 6; ++i) {
-                        const R f = mlog(Eo[i] / tot + R(1e-12));
-                        feat[tid * 12 + 6 * w + i] = f;
-                        const R x = f / R(10.0) + R(1.0);
-                        if (x < W[MLP_NW + 6 * w + i] || x > W[MLP_NW + 12 + 6 * w + i]) fb = 1;
-                    }
+                for (int qq = 0; qq < 4; ++qq) {
+                    const int n = lane + 16 * qq, ai = n & 3, bj = (n >> 2) & 3, cc = n >> 4;
+                    const float e2 = m[n] * m[n];
+                    total += e2;
+                    if (ai < NN - 1 && bj < NN - 1 && cc < NN - 1) clip1 += e2;
+                    if (ai < NN - 2 && bj < NN - 2 && cc < NN - 2) clip2 += e2;
                 }
             }
-            s_fb[tid] = fb;
+            total = hsum16m(total);
+            clip1 = hsum16m(clip1);
+            clip2 = hsum16m(clip2);
+            const float energy = fmaxf((total - clip1) / total, (clip1 - clip2) / clip1);
+            float al = 1.0f / (1.0f + __expf((float)k.ind_k * (energy - (float)k.ind_T)));
+            if (al < (float)k.alpha_min) al = 0.0f;
+            else if (al > (float)k.one_m_alpha_min) al = 1.0f;
+            if (act && lane == 0) s_am[pel] = fminf((float)k.alpha_max, al);
+            bool fb = false;
+            if (learned) {
+                float rs = 0.f, ps = 0.f, rmin = 3.4e38f, pmin = 3.4e38f;
+                if (act) {
+#pragma unroll
+                    for (int qq = 0; qq < 4; ++qq) {
+                        const int n = lane + 16 * qq;
+                        float uu[V];
+#pragma unroll
+                        for (int v = 0; v < V; ++v) uu[v] = (float)su[(v * EPC + pel) * NP + n];
+                        const float pr = m_pressure(uu, kap, mu0);
+                        rs += uu[0];
+                        ps += pr;
+                        rmin = fminf(rmin, uu[0]);
+                        pmin = fminf(pmin, pr);
+                    }
+                }
+                rs = hsum16m(rs);
+                ps = hsum16m(ps);
+                rmin = hmin16m(rmin);
+                pmin = hmin16m(pmin);
+                fb = rmin < 0.1f * (rs / 64.0f) || pmin < 0.1f * (ps / 64.0f);
+                float xmine = 0.f;
+#pragma unroll
+                for (int w = 0; w < 2; ++w) {
+                    float tot = 0.f, Eo[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+                    if (act) {
+                        const float* mw = scr + (4 + w) * EPC * NP + pel * NP;
+#pragma unroll
+                        for (int qq = 0; qq < 4; ++qq) {
+                            const int n = lane + 16 * qq;
+                            const int ord[3] = {n & 3, (n >> 2) & 3, n >> 4};
+                            const float ee = mw[n] * mw[n];
+                            tot += ee;
+#pragma unroll
+                            for (int d = 0; d < 3; ++d) {
+                                if (ord[d] == NN - 1) Eo[2 * d] += ee;
+                                if (ord[d] == NN - 2) Eo[2 * d + 1] += ee;
+                            }
+                        }
+                    }
+                    tot = hsum16m(tot);
+#pragma unroll
+                    for (int i = 0; i < 6; ++i) {
+                        const float Ei = hsum16m(Eo[i]);
+                        if (lane == 6 * w + i) xmine = __logf(Ei / tot + 1e-12f);
+                    }
+                }
+                const bool mine_out = lane < 12 && act &&
+                                      (xmine / 10.0f + 1.0f < W[MLP_NW + (lane < 12 ? lane : 0)] ||
+                                       xmine / 10.0f + 1.0f > W[MLP_NW + 12 + (lane < 12 ? lane : 0)]);
+                if (act && lane < 12) feat[pel * 12 + lane] = xmine;
+                // the vote runs in every lane of the warp
+                const unsigned oob = __ballot_sync(0xffffffffu, mine_out) & (0xffffu << (threadIdx.x & 16));
+                fb = fb || oob != 0u;
+            }
+            if (act && lane == 0) s_fb[pel] = fb ? 1 : 0;
+        } else {
+            if (tid < nel) {
+                const R* m = scr + 3 * EPC * NP + tid * NP;
+                R total = R(0.0), clip1 = R(0.0), clip2 = R(0.0);
+                for (int cc = 0; cc < NN; ++cc)
+                    for (int bj = 0; bj < NN; ++bj)
+                        for (int ai = 0; ai < NN; ++ai) {
+                            const R mv = m[nidx(ai, bj, cc)];
+                            const R e2 = mv * mv;
+                            total = total + e2;
+                            if (ai < NN - 1 && bj < NN - 1 && cc < NN - 1) clip1 = clip1 + e2;
+                            if (ai < NN - 2 && bj < NN - 2 && cc < NN - 2) clip2 = clip2 + e2;
+                        }
+                const R e1 = (total - clip1) / total;
+                const R e2 = (clip1 - clip2) / clip1;
+                const R energy = fmax(e1, e2);
+                R al = R(1.0) / (R(1.0) + expneg((R)k.ind_k * (energy - (R)k.ind_T)));
+                if (al < (R)k.alpha_min) al = R(0.0);
+                else if (al > (R)k.one_m_alpha_min) al = R(1.0);
+                s_am[tid] = fmin((R)k.alpha_max, al);
+                int fb = 0;
+                if (learned) {
+                    R rs = R(0.0), ps = R(0.0), rmin = R(1e30), pmin = R(1e30);
+                    for (int n = 0; n < NP; ++n) {
+                        R uu[V];
+    #pragma unroll
+                        for (int v = 0; v < V; ++v) uu[v] = (R)su[(v * EPC + tid) * NP + n];
+                        const R pr = m_pressure(uu, kap, mu0);
+                        rs = rs + uu[0];
+                        ps = ps + pr;
+                        rmin = fmin(rmin, uu[0]);
+                        pmin = fmin(pmin, pr);
+                    }
+                    if (rmin < R(0.1) * (rs / R(64.0)) || pmin < R(0.1) * (ps / R(64.0))) fb = 1;
+                    for (int w = 0; w < 2; ++w) {
+                        const R* mw = scr + (4 + w) * EPC * NP + tid * NP;
+                        R tot = R(0.0), Eo[6] = {R(0), R(0), R(0), R(0), R(0), R(0)};
+                        for (int cc = 0; cc < NN; ++cc)
+                            for (int bj = 0; bj < NN; ++bj)
+                                for (int ai = 0; ai < NN; ++ai) {
+                                    const R mv = mw[nidx(ai, bj, cc)];
+                                    const R ee = mv * mv;
+                                    tot = tot + ee;
+                                    const int ord[3] = {ai, bj, cc};
+    #pragma unroll
+                                    for (int d = 0; d < 3; ++d) {
+                                        if (ord[d] == NN - 1) Eo[2 * d] = Eo[2 * d] + ee;
+                                        if (ord[d] == NN - 2) Eo[2 * d + 1] = Eo[2 * d + 1] + ee;
+                                    }
+                                }
+                        for (int i = 0; i < 6; ++i) {
+                            const R f = mlog(Eo[i] / tot + R(1e-12));
+                            feat[tid * 12 + 6 * w + i] = f;
+                            const R x = f / R(10.0) + R(1.0);
+                            if (x < W[MLP_NW + 6 * w + i] || x > W[MLP_NW + 12 + 6 * w + i]) fb = 1;
+                        }
+                    }
+                }
+                s_fb[tid] = fb;
+            }
         }
         __syncthreads();
         if (learned) {
@@ -306,8 +400,10 @@ __device__ void epilogue_mhd(const StageArgs& a, const double* su, R* scr, unsig
 
 }  // namespace mhd
 
+// FP32 form: 4 CTAs per SM (128 registers; the spills cost less than the lost occupancy would);
+// plain FP64: 1 CTA per SM with the full register file.
 template <typename R, bool BLEND, bool RHS_ONLY>
-__global__ void __launch_bounds__(mhd::NT, 1) k_stage_mhd(StageArgs a) {
+__global__ void __launch_bounds__(mhd::NT, sizeof(R) == 4 ? 4 : 1) k_stage_mhd(StageArgs a) {
     constexpr int MEPC = mhd::EPC, MV = mhd::V;
     using mhd::load_rot;
     using mhd::load_rot_global;

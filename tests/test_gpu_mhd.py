@@ -94,3 +94,24 @@ def test_hlld_requires_unit_mu0():
     m = mesh.brick(2)
     with pytest.raises(abi.NemoError, match="mu0"):
         Solver(mcfg(surface_flux=abi.SURFFLUX_HLLD, mu0=2.0), m)
+
+
+def test_mhd_fp32_learned_indicator_close_to_fp64():
+    """FP32 form with the learned indicator (parallel 16-lane feature sums) against the plain FP64
+    form with the same BF16 network, which equals the oracle bit for bit."""
+    from nemo_b200 import learned
+    m = mesh.brick(8)
+    u = setups.orszag_tang(m)
+    out = {}
+    for prec in (abi.PREC_FP64, abi.PREC_FP32):
+        s = Solver(mcfg(precision=prec, indicator=abi.IND_LEARNED, positivity=1, surface_flux=abi.SURFFLUX_HLLD), m)
+        learned.install()
+        s.upload(u)
+        out[prec] = (s.alpha(), None)
+        s.run(nsteps=5)
+        out[prec] = (out[prec][0], s.download())
+        s.finalize()
+    a64, u64 = out[abi.PREC_FP64]
+    a32, u32 = out[abi.PREC_FP32]
+    assert np.max(np.abs(a32 - a64)) < 1e-3
+    assert np.sum(np.abs(u32[0] - u64[0])) / np.sum(np.abs(u64[0])) < 1e-6
