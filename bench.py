@@ -126,17 +126,18 @@ class ClockSampler:
     def __init__(self, index):
         self.index = index
         self.proc = None
-        self.out = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+        import tempfile
+        fd, self.out = tempfile.mkstemp(prefix="nemo_clocks_", suffix=".csv")
+        os.close(fd)
 
     def __enter__(self):
         q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
         try:
-            os.makedirs(os.path.dirname(self.out), exist_ok=True)
             self.f = open(self.out, "w")
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}", "--format=csv",
-                                          "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+                                          "-lms", "50"], stdout=self.f, stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
         return self
@@ -157,6 +158,10 @@ class ClockSampler:
                 parts = [p.strip() for p in line.split(",")]
                 if len(parts) >= 9:
                     rows.append(parts)
+        try:
+            os.remove(self.out)
+        except OSError:
+            pass
         if not rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
         sm = [float(r[1].split()[0]) for r in rows]
