@@ -536,8 +536,13 @@ __global__ void __launch_bounds__(NT, 1) k_stage_euler64(StageArgs a) {
     }
     if (RHS_ONLY) return;
     __syncthreads();
-    if (a.positivity && tid < nel && s_bad[tid]) {
-        if (!repair_elem<EPC>(su, tid, k)) atomicAdd(&ctrl->nbad, 1ull);
+    {   // element w is repaired by lanes 0..15 of warp w together (same arithmetic and order as the
+        // serial dgfv_repair_3d, no call frame in this kernel)
+        const int w = tid >> 5, lane = tid & 31;
+        if (a.positivity && w < nel && lane < 16 && s_bad[w]) {
+            const bool repaired = repair_elem16<EPC>(su, w, lane, k);
+            if (!repaired && lane == 0) atomicAdd(&ctrl->nbad, 1ull);
+        }
     }
     __syncthreads();
     // ---- store the new state
