@@ -29,6 +29,8 @@ WORKLOADS = {
     # name: (elements per direction, setup, indicator)
     "sedov32": dict(nx=32, setup="sedov", indicator=1, positivity=1,
                     desc="Sedov blast 32^3 elements N=3 (2.1M nodes), DG/FV blending, FP64"),
+    "sedov64": dict(nx=64, setup="sedov", indicator=1, positivity=1,
+                    desc="Sedov blast 64^3 elements N=3 (16.8M nodes), learned indicator vs the modal one, FP64"),
     "wave16": dict(nx=16, setup="wave", indicator=0, positivity=0,
                    desc="periodic density wave 16^3 elements N=3 (262k nodes), EC volume + HLLC, FP64"),
     "batch": dict(nx=24, setup="batch", indicator=1, positivity=1, t_end=0.05,
