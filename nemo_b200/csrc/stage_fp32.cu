@@ -8,7 +8,8 @@
 //   FP32: all two-point fluxes, Riemann fluxes, FV subcells, the lift and the indicator.
 // The logarithmic mean switches on the relative difference (Ismail-Roe form: f = (a-b)/(a+b),
 // 4-term series for f^2 < 1e-2, else (a-b)/log(a/b)), because the reference's absolute switch
-// |a-b| < 1e-4 is meaningless in FP32 for beta = rho/(2p) ~ 5e4.  The HBM traffic is that of the
+// |a-b| < 1e-4 is meaningless in FP32 for beta = rho/(2p) ~ 5e4; the Chandrashekar pair is written
+// in terms of g = atanh(f)/f, which leaves it three divisions.  The HBM traffic is that of the
 // plain path (FP64 u in/out, FP64 register in/out); the arithmetic per node pair is a third.
 #include "common.cuh"
 #include "euler_fp64.cuh"
@@ -197,16 +198,16 @@ __device__ __forceinline__ void riemann32(int kind, const P32& L, const P32& R, 
     else hllc32(L, R, F, k);
 }
 
-// Logarithmic mean with a relative switch (Ismail-Roe): (a-b)/log(a/b) = (a+b)/2 / g(f^2),
-// g(u) = atanh(sqrt u)/sqrt u = 1 + u/3 + u^2/5 + u^3/7 + ... for f = (a-b)/(a+b).
-__device__ __forceinline__ float lnmean32(float a, float b) {
-    const float s = a + b;
-    const float f = (a - b) / s;
+// g(a, b) = atanh(f)/f for f = (a-b)/(a+b) (rs = 1/(a+b)), so that the logarithmic mean
+// (a-b)/log(a/b) is (a+b)/(2g) and its inverse 2g/(a+b): the series 1 + u/3 + u^2/5 + u^3/7
+// (u = f^2) below u = 1e-2 (Ismail-Roe), else log(a/b)/(2f).  Written this way the Chandrashekar
+// pair needs three divisions instead of seven.
+__device__ __forceinline__ float lngain32(float a, float b, float rs) {
+    const float f = (a - b) * rs;
     const float u = f * f;
-    if (u < 1e-2f) return 0.5f * s / (1.0f + u * (1.0f / 3.0f + u * (0.2f + u * (1.0f / 7.0f))));
-    return (a - b) / __logf(a / b);
+    if (u < 1e-2f) return 1.0f + u * (1.0f / 3.0f + u * (0.2f + u * (1.0f / 7.0f)));
+    return 0.5f * __logf(a / b) / f;
 }
-
 
 // Epilogue on a state held in smem (FP64): the blending coefficient for the next stage (modal
 // indicator, or the learned indicator with the modal one as fallback and judge) and, if requested,
@@ -731,14 +732,20 @@ __device__ __forceinline__ void tile32(const StageArgs& a, const Smem32& S, int6
 #pragma unroll
                         for (int v = 0; v < V; ++v) F[v] = 0.5f * (fa[v] + fb[v]);
                     } else {
-                        const float dens = lnmean32(rho[i], rho[m]);
+                        // logarithmic means as (a+b)/(2g): dens = {rho}_ln, p^ = {rho}/(2{beta}),
+                        // p^/dens = g_rho/(beta_i+beta_m), 1/{beta}_ln = 2 g_beta/(beta_i+beta_m)
+                        const float srho = rho[i] + rho[m];
+                        const float rsb = 1.0f / (bt[i] + bt[m]);
+                        const float gr = lngain32(rho[i], rho[m], 1.0f / srho);
+                        const float gb = lngain32(bt[i], bt[m], rsb);
+                        const float dens = 0.5f * srho / gr;
                         const float velx = 0.5f * (vn[i] + vn[m]), vely = 0.5f * (w1[i] + w1[m]);
                         const float velz = 0.5f * (w2[i] + w2[m]);
-                        const float pres = 0.5f * (rho[i] + rho[m]) / (bt[i] + bt[m]);
+                        const float pres = 0.5f * srho * rsb;
                         const float vsq = (vn[i] * vn[i] + w1[i] * w1[i] + w2[i] * w2[i]) +
                                           (vn[m] * vn[m] + w1[m] * w1[m] + w2[m] * w2[m]);
-                        const float enth = c_enth / lnmean32(bt[i], bt[m]) + pres / dens + velx * velx + vely * vely +
-                                           velz * velz - 0.25f * vsq;
+                        const float enth = (2.0f * c_enth * gb + gr) * rsb + velx * velx + vely * vely + velz * velz -
+                                           0.25f * vsq;
                         F[0] = dens * velx;
                         F[1] = F[0] * velx + pres;
                         F[2] = F[0] * vely;
