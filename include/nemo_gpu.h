@@ -49,6 +49,9 @@ enum nemo_surfflux   { NEMO_SURFFLUX_HLLC = 0, NEMO_SURFFLUX_RUSANOV = 1, NEMO_S
 enum nemo_precision  { NEMO_PREC_FP64 = 0, NEMO_PREC_FP32 = 1 };
 /* DG/FV blending coefficient alpha: none, modal-energy indicator, learned MLP (modal fallback) */
 enum nemo_indicator  { NEMO_IND_NONE = 0, NEMO_IND_MODAL = 1, NEMO_IND_LEARNED = 2 };
+/* source terms applied after every stage (hook_post_rk_timestep): barotropic cooling resets the
+   energy to the barotropic equation of state, source/physics/cooling/barotropic_cooling_mod.f90:39-53 */
+enum nemo_source     { NEMO_SOURCE_NONE = 0, NEMO_SOURCE_BAROTROPIC_COOLING = 1 };
 
 enum nemo_face { NEMO_NOR = 0, NEMO_SOU = 1, NEMO_WES = 2, NEMO_EAS = 3, NEMO_FRO = 4, NEMO_BAC = 5 };
 
@@ -73,6 +76,8 @@ typedef struct nemo_cfg {
     int32_t positivity;       /* 1: element-tile squeeze repair after every stage
                                  (source/kernel/mcfv/3d/kernel_validate_mod.f90:159-272) */
     int32_t non_conservative; /* MHD: add the Powell/GLM non-conservative term */
+    int32_t source;           /* enum nemo_source (Euler only) */
+    int32_t pad_;
     double  kappa;            /* ratio of specific heats (setup_config_mod kappa) */
     double  mu0;              /* magnetic permeability (MHD) */
     double  cfl;              /* CFL number used by nemo_gpu_calc_timestep / run */
@@ -81,7 +86,10 @@ typedef struct nemo_cfg {
     double  repair_decr;      /* squeeze decrement of the repair (0.01, kernel_config_mod.f90:5) */
     double  glm_ch;           /* GLM cleaning speed (MHD); updated by calc_timestep */
     double  glm_alpha;        /* GLM damping (MHD); updated by calc_timestep */
-    double  reserved[4];
+    double  dens_critical;    /* barotropic cooling: rho <= dens_critical is isothermal */
+    double  k_isothermal;     /* barotropic cooling: p = k_isothermal rho below dens_critical */
+    double  k_adiabatic;      /* barotropic cooling: p = k_adiabatic rho^kappa above it */
+    double  reserved;
 } nemo_cfg;
 
 /* Fill *cfg with the defaults of the Euler DGSEM path (N=3, Chandrashekar, HLLC, FP64). */

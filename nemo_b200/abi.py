@@ -15,6 +15,7 @@ VOLFLUX_CHANDRASHEKAR, VOLFLUX_CENTRAL, VOLFLUX_EC_MHD = 0, 1, 2
 SURFFLUX_HLLC, SURFFLUX_RUSANOV, SURFFLUX_HLLD = 0, 1, 2
 PREC_FP64, PREC_FP32 = 0, 1
 IND_NONE, IND_MODAL, IND_LEARNED = 0, 1, 2
+SOURCE_NONE, SOURCE_BAROTROPIC_COOLING = 0, 1
 
 STATUS = {0: "OK", 1: "ERR_ARG", 2: "ERR_STATE", 3: "ERR_CUDA", 4: "ERR_REPAIR", 5: "ERR_NONFINITE"}
 
@@ -43,10 +44,11 @@ class NemoCfg(ctypes.Structure):
         ("n_nodes", ctypes.c_int32), ("n_vars", ctypes.c_int32), ("eqn", ctypes.c_int32),
         ("volume_flux", ctypes.c_int32), ("surface_flux", ctypes.c_int32), ("precision", ctypes.c_int32),
         ("indicator", ctypes.c_int32), ("alpha_smoothing", ctypes.c_int32), ("positivity", ctypes.c_int32),
-        ("non_conservative", ctypes.c_int32),
+        ("non_conservative", ctypes.c_int32), ("source", ctypes.c_int32), ("pad_", ctypes.c_int32),
         ("kappa", ctypes.c_double), ("mu0", ctypes.c_double), ("cfl", ctypes.c_double),
         ("alpha_max", ctypes.c_double), ("alpha_min", ctypes.c_double), ("repair_decr", ctypes.c_double),
-        ("glm_ch", ctypes.c_double), ("glm_alpha", ctypes.c_double), ("reserved", ctypes.c_double * 4),
+        ("glm_ch", ctypes.c_double), ("glm_alpha", ctypes.c_double), ("dens_critical", ctypes.c_double),
+        ("k_isothermal", ctypes.c_double), ("k_adiabatic", ctypes.c_double), ("reserved", ctypes.c_double),
     ]
 
 

@@ -65,6 +65,10 @@ struct OpConsts {
     double alpha_min, alpha_max, one_m_alpha_min;
     double repair_decr;
     double mu0;
+    int cool;              // barotropic cooling after every stage
+    double cool_rho;       // dens_critical
+    double cool_ci;        // k_isothermal / (kappa - 1)
+    double cool_ca;        // k_adiabatic / (kappa - 1)
     double pro[2][NN * NN];  // 2:1 mortar prolongation to the lower/upper half, [s][fine i][coarse j]
     double prj[2][NN * NN];  // 2:1 mortar projection from the lower/upper half, [s][coarse a][fine i]
 };

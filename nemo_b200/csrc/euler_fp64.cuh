@@ -148,4 +148,13 @@ __device__ __forceinline__ bool isvalid64(const double* u, const OpConsts& k) {
     return (u[0] > 0.0) && (pressure64(u, k) > 0.0);
 }
 
+// Barotropic cooling after a stage (hook_post_rk_timestep_200,
+// source/physics/cooling/barotropic_cooling_mod.f90:39-53): the energy of the barotropic equation of
+// state, isothermal at or below dens_critical, adiabatic above (rho^kappa = exp(kappa log rho)).
+__device__ __forceinline__ double cooled_energy64(const double* q, const OpConsts& k) {
+    const double kin = 0.5 / q[0] * (q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
+    if (q[0] <= k.cool_rho) return kin + k.cool_ci * q[0];
+    return kin + k.cool_ca * pexp64(k.kappa * plog64(q[0]));
+}
+
 }  // namespace nemo

@@ -496,6 +496,13 @@ int nemo_gpu_init(const nemo_cfg* cfg) {
     if (cfg->indicator != NEMO_IND_NONE && cfg->indicator != NEMO_IND_MODAL && cfg->indicator != NEMO_IND_LEARNED)
         return fail(NEMO_ERR_ARG, "unsupported indicator %d", cfg->indicator);
     if (!(cfg->kappa > 1.0)) return fail(NEMO_ERR_ARG, "kappa must be > 1");
+    if (cfg->source != NEMO_SOURCE_NONE && cfg->source != NEMO_SOURCE_BAROTROPIC_COOLING)
+        return fail(NEMO_ERR_ARG, "unknown source term %d", cfg->source);
+    if (cfg->source == NEMO_SOURCE_BAROTROPIC_COOLING) {
+        if (cfg->eqn != NEMO_EQN_EULER) return fail(NEMO_ERR_ARG, "barotropic cooling is an Euler source term");
+        if (!(cfg->dens_critical > 0.0) || !(cfg->k_isothermal > 0.0) || !(cfg->k_adiabatic > 0.0))
+            return fail(NEMO_ERR_ARG, "barotropic cooling needs dens_critical, k_isothermal, k_adiabatic > 0");
+    }
     int ndev = 0;
     CK(cudaGetDeviceCount(&ndev));
     if (ndev < 1) return fail(NEMO_ERR_CUDA, "no CUDA device");
@@ -520,6 +527,10 @@ int nemo_gpu_init(const nemo_cfg* cfg) {
     o.one_m_alpha_min = 1.0 - cfg->alpha_min;
     o.repair_decr = cfg->repair_decr;
     o.mu0 = cfg->mu0;
+    o.cool = cfg->source == NEMO_SOURCE_BAROTROPIC_COOLING ? 1 : 0;
+    o.cool_rho = cfg->dens_critical;
+    o.cool_ci = cfg->k_isothermal / (cfg->kappa - 1.0);
+    o.cool_ca = cfg->k_adiabatic / (cfg->kappa - 1.0);
     std::memcpy(o.pro, g.hops.pro, sizeof o.pro);
     std::memcpy(o.prj, g.hops.prj, sizeof o.prj);
     CK(cudaStreamCreateWithFlags(&g.stream, cudaStreamNonBlocking));

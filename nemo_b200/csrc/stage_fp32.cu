@@ -840,6 +840,19 @@ __device__ __forceinline__ void tile32(const StageArgs& a, const Smem32& S, int6
         const bool repaired = repair_elem16<EPC>(su, el, ab, k);
         if (!repaired && ab == 0) atomicAdd(&ctrl->nbad, 1ull);
     }
+    if (k.cool) {   // source term after the stage, on the element's own nodes (after its repair)
+        __syncwarp();
+        if (active) {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int n = ab + 16 * q;
+                double qv[V];
+#pragma unroll
+                for (int v = 0; v < V; ++v) qv[v] = su[(v * EPC + el) * NP + n];
+                su[(4 * EPC + el) * NP + n] = cooled_energy64(qv, k);
+            }
+        }
+    }
     // make the generic-proxy writes of su visible to the bulk copies, then store the tile
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncthreads();

@@ -545,9 +545,15 @@ __global__ void __launch_bounds__(NT, 1) k_stage_euler64(StageArgs a) {
         }
     }
     __syncthreads();
-    // ---- store the new state
+    // ---- source term after the stage, then store the new state
     for (int p = tid; p < nel * NP; p += NT) {
         const int pel = p / NP, n = p % NP;
+        if (k.cool) {
+            double q[V];
+#pragma unroll
+            for (int v = 0; v < V; ++v) q[v] = su[(v * EPC + pel) * NP + n];
+            su[(4 * EPC + pel) * NP + n] = cooled_energy64(q, k);
+        }
 #pragma unroll
         for (int v = 0; v < V; ++v) a.u_out[((int64_t)v * E + e0 + pel) * NP + n] = su[(v * EPC + pel) * NP + n];
     }

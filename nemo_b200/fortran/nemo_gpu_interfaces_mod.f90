@@ -17,13 +17,14 @@ integer(c_int), parameter :: NEMO_VOLFLUX_CHANDRASHEKAR = 0, NEMO_VOLFLUX_CENTRA
 integer(c_int), parameter :: NEMO_SURFFLUX_HLLC = 0, NEMO_SURFFLUX_RUSANOV = 1
 integer(c_int), parameter :: NEMO_PREC_FP64 = 0, NEMO_PREC_FP32 = 1
 integer(c_int), parameter :: NEMO_IND_NONE = 0, NEMO_IND_MODAL = 1, NEMO_IND_LEARNED = 2
+integer(c_int), parameter :: NEMO_SOURCE_NONE = 0, NEMO_SOURCE_BAROTROPIC_COOLING = 1
 
 !! mirrors struct nemo_cfg (include/nemo_gpu.h)
 type, bind(c) :: nemo_cfg_t
     integer(c_int)  :: n_nodes, n_vars, eqn, volume_flux, surface_flux, precision, indicator
-    integer(c_int)  :: alpha_smoothing, positivity, non_conservative
+    integer(c_int)  :: alpha_smoothing, positivity, non_conservative, source, pad_
     real(c_double)  :: kappa, mu0, cfl, alpha_max, alpha_min, repair_decr, glm_ch, glm_alpha
-    real(c_double)  :: reserved(4)
+    real(c_double)  :: dens_critical, k_isothermal, k_adiabatic, reserved
 end type
 
 interface

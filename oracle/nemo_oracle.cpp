@@ -1312,6 +1312,15 @@ void mortar_fluxes(const Ctx& c, const Mesh& M, const double* u, int nthreads) {
     }
 }
 
+// hook_post_rk_timestep_200 of source/physics/cooling/barotropic_cooling_mod.f90:39-53: the energy is
+// reset to the barotropic equation of state, isothermal at or below dens_critical, adiabatic above;
+// rho^kappa = exp(kappa log rho) with the IEEE-only exp and log of this file.
+void barotropic_cooling(const nemo_cfg* cfg, double* q) {
+    const double kin = 0.5 / q[0] * (q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
+    if (q[0] <= cfg->dens_critical) q[4] = kin + (cfg->k_isothermal / (cfg->kappa - 1.0)) * q[0];
+    else q[4] = kin + (cfg->k_adiabatic / (cfg->kappa - 1.0)) * own_exp(cfg->kappa * own_log(q[0]));
+}
+
 Mesh make_mesh(int64_t E, const int32_t* nbr, const double* delta) {
     Mesh M{E, nbr, delta};
     M.nm = (int64_t)(g_mortar.size() / 6);
@@ -1501,6 +1510,8 @@ int64_t or_stage(const nemo_cfg* cfg, int64_t E, const int32_t* nbr, const doubl
                 st[p][v] = u[g] + Cdt * r;
             }
         if (cfg->positivity && !repair_element(c, st)) nbad += 1;
+        if (cfg->source == NEMO_SOURCE_BAROTROPIC_COOLING)
+            for (int p = 0; p < NP; ++p) barotropic_cooling(cfg, st[p]);
         for (int v = 0; v < V; ++v)
             for (int p = 0; p < NP; ++p) u[((size_t)v * E + e) * NP + p] = st[p][v];
     }
