@@ -143,6 +143,29 @@ int nemo_gpu_set_groups(int32_t ngroups, const int32_t* group_of_elem);
    idx_dev and buf_dev are device pointers; both calls return after the copy has completed.  The
    time step of a partitioned run is the minimum over processes of nemo_gpu_calc_timestep. */
 int nemo_gpu_set_owned(int64_t n_owned);
+
+/* AMR adapt between steps (mesh_adapt, source/mesh/p4est/mesh_utils_mod.f90:879-1010, called by a
+   setup's hook_pre_timestep_300; payload transfer of kernel_amr_refine / kernel_amr_coarsen,
+   source/kernel/dgsem/weakform/2d/kernel_amr_mod.f90:12-73, in 3D as in the replace callbacks of
+   source/setups/euler/3d/sedov/setup_amr_mod.f90:67-125).  The host rebuilds the forest; the new mesh
+   comes in set_mesh form, plus remap[nelems][4] int32 rows (kind, src, depth, offsets): kind 0 copies
+   old element src; kind 1 interpolates the polynomial of old element src, an ancestor depth levels up
+   (1..7), at the nodes of the new element, which sits at offsets ox | oy << 8 | oz << 16 inside it;
+   kind 2 takes the sum of the DG projections of the 8 old children src .. src + 7 (child
+   c = sx + 2 sy + 4 sz).  A transferred element that is not admissible falls back to the mean: all
+   elements refined from that ancestor take its mean, a coarsened element the mean of its children
+   (the reference steps down through lower orders, :82-95 and :114-124).  The state is remapped on the
+   device, the mesh replaced, the simulation time kept; groups and ghost elements are not supported.
+   Rows are checked before anything on the device changes (NEMO_ERR_ARG). */
+int nemo_gpu_adapt(int64_t nelems, const double* delta, const double* center, int64_t nsides,
+                   const int32_t* side_quads, const int8_t* side_faceid, const int8_t* side_nquads,
+                   const int32_t* boundary, const int32_t* remap);
+/* Adapt flags of the current state, computed on the device (the density probes of the Sedov setup,
+   setup_amr_probe_refine / setup_amr_probe_coarsen, source/setups/euler/3d/sedov/setup_amr_mod.f90:
+   23-65): flags[e] = +1 if some node's density exceeds refine_threshold, else -1 if no node's density
+   exceeds coarsen_threshold, else 0.  flags is a host array of nelems int32; a family of 8 leaves
+   coarsens when all of its members hold -1.  Only the flags cross to the host. */
+int nemo_gpu_amr_flags(double refine_threshold, double coarsen_threshold, int32_t* flags);
 int nemo_gpu_pack_elements(const int32_t* idx_dev, int64_t n, double* buf_dev);
 int nemo_gpu_unpack_elements(const int32_t* idx_dev, int64_t n, const double* buf_dev);
 

@@ -29,7 +29,7 @@ EXPORTS = [
     "nemo_gpu_totals_noalloc", "nemo_gpu_set_mlp", "nemo_gpu_features", "nemo_gpu_indicator_stats",
     "nemo_gpu_mlp_train", "nemo_gpu_mlp_grad", "nemo_gpu_mlp_forward", "nemo_gpu_mortar_operators",
     "nemo_gpu_autotune", "nemo_gpu_set_schedule", "nemo_gpu_set_owned", "nemo_gpu_pack_elements",
-    "nemo_gpu_unpack_elements",
+    "nemo_gpu_unpack_elements", "nemo_gpu_adapt", "nemo_gpu_amr_flags",
 ]
 
 
@@ -102,6 +102,8 @@ def load(path=LIB_PATH):
         "nemo_gpu_set_owned": [i64],
         "nemo_gpu_pack_elements": [vp, i64, vp],
         "nemo_gpu_unpack_elements": [vp, i64, vp],
+        "nemo_gpu_adapt": [i64, vp, vp, i64, vp, vp, vp, vp, vp],
+        "nemo_gpu_amr_flags": [dbl, dbl, vp],
     }
     for name, args in sig.items():
         f = getattr(L, name)

@@ -69,6 +69,8 @@ struct OpConsts {
     double cool_rho;       // dens_critical
     double cool_ci;        // k_isothermal / (kappa - 1)
     double cool_ca;        // k_adiabatic / (kappa - 1)
+    double x[NN];            // Gauss-Lobatto nodes on [-1,1] (adapt: interpolation to descendants)
+    double w[NN];            // their weights (adapt: element means)
     double pro[2][NN * NN];  // 2:1 mortar prolongation to the lower/upper half, [s][fine i][coarse j]
     double prj[2][NN * NN];  // 2:1 mortar projection from the lower/upper half, [s][coarse a][fine i]
 };

@@ -56,6 +56,12 @@ struct MortarArgs {
     uint32_t epoch;
 };
 cudaError_t setup_mortar(const OpConsts& ops);
+// adapt: new SoA state [V][En][64] from the old one [V][Eo][64] by remap rows (kind, src, depth,
+// offsets) -- copy, interpolation from an ancestor, projection of 8 children
+cudaError_t launch_remap(const double* uo, int64_t Eo, double* un, int64_t En, const int32_t* remap, int nv,
+                         int32_t* bad, cudaStream_t s);
+cudaError_t launch_amr_flags(const double* u, int64_t E, double refine_thr, double coarsen_thr, int32_t* flags,
+                             cudaStream_t s);
 cudaError_t launch_mortar(const MortarArgs& a, cudaStream_t s);
 
 // plain FP64 Euler path (stage_fp64.cu)

@@ -2,7 +2,9 @@
 // node): coarse trace staged in shared memory and prolonged (tensor product of the 1D interpolation
 // matrices), Riemann flux against the fine quad's trace in the face's rotated frame (plus, for MHD,
 // each side's non-conservative term), the fine rows written directly and the coarse row projected
-// (1D projection matrices), sums in the oracle's order (oracle mortar_fluxes).  Used by the mortar
+// (1D projection matrices), sums in the oracle's order (oracle mortar_fluxes).  A prolonged sub-face
+// trace with an inadmissible node (a strong shock on the coarse side) is replaced by the coarse face's
+// mean, which is admissible; the reference interpolates without this guard.  Used by the mortar
 // kernel (mortar.cu) and by the persistent FP32 stage kernel, which runs the mortar pairs as its
 // first tasks and publishes each mortar with a release flag (epoch) that its element tiles acquire.
 // Reference: the mortar part of kernel_fill_faceflux, source/kernel/mcfv/3d/kernel_flux_mod.f90:
@@ -19,6 +21,16 @@ namespace mortar {
 
 constexpr int MPB = 2;          // mortars per 128-thread task
 constexpr int SCRATCH_DOUBLES = MPB * 9 * NF + MPB * 4 * 9 * NF;
+
+// LGL-weighted mean of a coarse face trace held as [V][NF] (out of line: taken only on a shock)
+static __device__ __noinline__ void face_mean(const double* uc, int V, double* out, const OpConsts& k) {
+    for (int v = 0; v < V; ++v) {
+        double acc = 0.0;
+        for (int bb = 0; bb < NN; ++bb)
+            for (int aa = 0; aa < NN; ++aa) acc = acc + (k.wt[aa] * k.wt[bb]) * uc[v * NF + aa + NN * bb];
+        out[v] = acc;
+    }
+}
 
 template <bool MHD>
 __device__ __forceinline__ void mortar_pair(const MortarArgs& a, int64_t pair, double* scratch, const OpConsts& k) {
@@ -56,8 +68,16 @@ __device__ __forceinline__ void mortar_pair(const MortarArgs& a, int64_t pair, d
                 acc = acc + k.pro[tt][j * NN + bb] * in;
             }
             up[v] = acc;
-            uf[v] = a.u_in[((int64_t)v * E + qf) * NP + nf];
         }
+        // a sub-face (16 lanes of this warp; act is warp-uniform) whose prolonged trace has an
+        // inadmissible node takes the coarse face's mean instead, as the oracle does
+        bool okn;
+        if constexpr (MHD) okn = m_isvalid<double>(up, k.kappa, k.mu0);
+        else okn = isvalid64(up, k);
+        const unsigned badl = __ballot_sync(0xffffffffu, !okn);
+        if (badl & (0xffffu << (16 * (kq & 1)))) face_mean(&s_uc[ml][0][0], V, up, k);
+#pragma unroll
+        for (int v = 0; v < V; ++v) uf[v] = a.u_in[((int64_t)v * E + qf) * NP + nf];
         // rotate into the face frame: component c of momentum (and field) -> original (d + c) % 3
         double rp[V], rf[V];
         rp[0] = up[0];

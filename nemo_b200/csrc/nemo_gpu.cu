@@ -531,6 +531,8 @@ int nemo_gpu_init(const nemo_cfg* cfg) {
     o.cool_rho = cfg->dens_critical;
     o.cool_ci = cfg->k_isothermal / (cfg->kappa - 1.0);
     o.cool_ca = cfg->k_adiabatic / (cfg->kappa - 1.0);
+    std::memcpy(o.x, g.hops.x, sizeof o.x);
+    std::memcpy(o.w, g.hops.w, sizeof o.w);
     std::memcpy(o.pro, g.hops.pro, sizeof o.pro);
     std::memcpy(o.prj, g.hops.prj, sizeof o.prj);
     CK(cudaStreamCreateWithFlags(&g.stream, cudaStreamNonBlocking));
@@ -650,6 +652,79 @@ int nemo_gpu_set_mesh(int64_t nelems, const double* delta, const double* center,
     c.epoch = 1u;   // mortar flags start at 0: never equal to a launch's epoch before it sets them
     CK(cudaMemcpy(g.ctrl, &c, sizeof c, cudaMemcpyHostToDevice));
     g.has_mesh = true;
+    return NEMO_OK;
+}
+
+int nemo_gpu_adapt(int64_t nelems, const double* delta, const double* center, int64_t nsides,
+                   const int32_t* side_quads, const int8_t* side_faceid, const int8_t* side_nquads,
+                   const int32_t* boundary, const int32_t* remap) {
+    int st = ensure_ready();
+    if (st) return st;
+    if (nelems <= 0 || !remap) return fail(NEMO_ERR_ARG, "adapt needs nelems > 0 and a remap table");
+    if (g.ngroups > 1 || g.E_own != g.E)
+        return fail(NEMO_ERR_STATE, "adapt supports one run on one process (no groups, no ghost elements)");
+    const int64_t Eo = g.E;
+    for (int64_t e = 0; e < nelems; ++e) {
+        const int32_t* r = remap + 4 * e;
+        const int kind = r[0];
+        const int64_t src = r[1];
+        bool ok = kind >= 0 && kind <= 2 && src >= 0;
+        if (kind == 0) ok = ok && src < Eo;
+        if (kind == 1) {
+            const int d = r[2], o = r[3];
+            ok = ok && src < Eo && d >= 1 && d <= 7 && (o & 0xff) < (1 << d) && ((o >> 8) & 0xff) < (1 << d) &&
+                 ((o >> 16) & 0xff) < (1 << d) && (o >> 24) == 0;
+        }
+        if (kind == 2) ok = ok && src + 8 <= Eo;
+        if (!ok) return fail(NEMO_ERR_ARG, "remap row %lld is invalid", (long long)e);
+    }
+    // the new state from the old one, before the mesh (and its buffers) is replaced
+    const size_t bytes = sizeof(double) * (size_t)g.V * nelems * NP;
+    double* tmp = nullptr;
+    int32_t* rm = nullptr;
+    CK(cudaMalloc(&tmp, bytes));
+    // remap rows, then one flag per old element and per new element for the admissibility fallback
+    cudaError_t e1 = cudaMalloc(&rm, sizeof(int32_t) * (4 * nelems + Eo + nelems));
+    if (e1 == cudaSuccess) e1 = cudaMemcpy(rm, remap, sizeof(int32_t) * 4 * nelems, cudaMemcpyHostToDevice);
+    if (e1 == cudaSuccess) e1 = launch_remap(g.u[g.cur], Eo, tmp, nelems, rm, g.V, rm + 4 * nelems, g.stream);
+    if (e1 == cudaSuccess) e1 = cudaStreamSynchronize(g.stream);
+    double t0 = 0.0;
+    unsigned long long steps = 0;
+    if (e1 == cudaSuccess) e1 = cudaMemcpy(&t0, &g.ctrl->t[0], sizeof t0, cudaMemcpyDeviceToHost);
+    if (e1 == cudaSuccess) e1 = cudaMemcpy(&steps, &g.ctrl->steps, sizeof steps, cudaMemcpyDeviceToHost);
+    cudaFree(rm);
+    if (e1 != cudaSuccess) {
+        cudaFree(tmp);
+        return fail(NEMO_ERR_CUDA, "adapt: %s", cudaGetErrorString(e1));
+    }
+    st = nemo_gpu_set_mesh(nelems, delta, center, nsides, side_quads, side_faceid, side_nquads, boundary);
+    if (st) {
+        cudaFree(tmp);
+        return st;
+    }
+    e1 = cudaMemcpy(g.u[0], tmp, bytes, cudaMemcpyDeviceToDevice);
+    cudaFree(tmp);
+    if (e1 != cudaSuccess) return fail(NEMO_ERR_CUDA, "adapt: %s", cudaGetErrorString(e1));
+    CK(cudaMemset(g.reg, 0, bytes));
+    CK(cudaMemcpy(&g.ctrl->t[0], &t0, sizeof t0, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(&g.ctrl->steps, &steps, sizeof steps, cudaMemcpyHostToDevice));
+    g.cur = 0;
+    g.has_state = true;
+    g.prepared = false;
+    return NEMO_OK;
+}
+
+int nemo_gpu_amr_flags(double refine_threshold, double coarsen_threshold, int32_t* flags) {
+    int st = ensure_ready();
+    if (st) return st;
+    if (!flags) return fail(NEMO_ERR_ARG, "flags is NULL");
+    int32_t* d = nullptr;
+    CK(cudaMalloc(&d, sizeof(int32_t) * g.E));
+    cudaError_t e1 = launch_amr_flags(g.u[g.cur], g.E, refine_threshold, coarsen_threshold, d, g.stream);
+    if (e1 == cudaSuccess) e1 = cudaMemcpyAsync(flags, d, sizeof(int32_t) * g.E, cudaMemcpyDeviceToHost, g.stream);
+    if (e1 == cudaSuccess) e1 = cudaStreamSynchronize(g.stream);
+    cudaFree(d);
+    if (e1 != cudaSuccess) return fail(NEMO_ERR_CUDA, "amr_flags: %s", cudaGetErrorString(e1));
     return NEMO_OK;
 }
 

@@ -125,6 +125,28 @@ interface
         integer(c_int32_t), value :: len
         integer(c_int) :: st
     end function
+
+    !! Adapt flags of the current state from the device density probe (replaces the probe callbacks
+    !! of mesh_adapt); flags(nquads): +1 refine, -1 coarsen (all 8 of a family), 0 keep.
+    function nemo_gpu_amr_flags(refine_threshold, coarsen_threshold, flags) result(st) &
+            bind(c, name="nemo_gpu_amr_flags")
+        import :: c_int, c_int32_t, c_double
+        real(c_double), value :: refine_threshold, coarsen_threshold
+        integer(c_int32_t), intent(out) :: flags(*)
+        integer(c_int) :: st
+    end function
+
+    !! The adapted forest in set_mesh form plus remap(4, nquads_new) rows (kind, src, depth, offsets)
+    !! with 0-based src (replaces the replace callbacks of mesh_adapt).
+    function nemo_gpu_adapt(nelems, delta, center, nsides, side_quads, side_faceid, side_nquads, boundary, &
+            remap) result(st) bind(c, name="nemo_gpu_adapt")
+        import :: c_int, c_int8_t, c_int32_t, c_int64_t, c_double
+        integer(c_int64_t), value :: nelems, nsides
+        real(c_double), intent(in) :: delta(*), center(*)
+        integer(c_int32_t), intent(in) :: side_quads(*), boundary(*), remap(*)
+        integer(c_int8_t), intent(in) :: side_faceid(*), side_nquads(*)
+        integer(c_int) :: st
+    end function
 end interface
 
 contains

@@ -145,44 +145,19 @@ def ensemble(members, nx):
     return mesh, groups
 
 
-def forest(nb, refine, max_level=2, lo=(0.0, 0.0, 0.0), hi=(1.0, 1.0, 1.0)):
-    """Statically refined periodic forest on an nb^3 base brick (one octree per base element).
+def _children(lev, crd, mask):
+    """Leaves with the masked ones replaced by their 8 children (child c = sx + 2 sy + 4 sz)."""
+    c = np.arange(8)
+    kids = np.stack([c & 1, (c >> 1) & 1, c >> 2], axis=1)
+    c2 = (2 * crd[mask][:, None, :] + kids[None]).reshape(-1, 3)
+    l2 = np.repeat(lev[mask] + 1, 8)
+    return np.concatenate([lev[~mask], l2]), np.concatenate([crd[~mask], c2])
 
-    refine(level, center[n,3], size[n]) -> bool[n] marks leaves of that level to split into 8; it is
-    called for level 0, 1, ..., max_level-1 in turn.  The forest is then 2:1 face-balanced (a leaf whose
-    face neighbour is two or more levels finer is split, repeatedly), the leaves are put in Morton order
-    of their anchors on the finest grid (the p4est order), and the sides are built: conforming sides as
-    in brick(), and one side per 2:1 non-conforming face with the coarse quad on one half and the four
-    fine quads (k = s + 2 t over the face's two tangential axes, lower axis first) on the other."""
-    lo, hi = np.asarray(lo, float), np.asarray(hi, float)
+
+def _balance(nb, max_level, lev, crd):
+    """2:1 face balance on the finest grid: a leaf whose face neighbour is two or more levels finer is
+    split, until none is (level of each finest cell and of its six neighbours, maximum per leaf)."""
     nf = nb << max_level
-    g = np.stack(np.meshgrid(np.arange(nb), np.arange(nb), np.arange(nb), indexing="ij"), -1).reshape(-1, 3)
-    lev = np.zeros(len(g), dtype=np.int64)
-    crd = g.astype(np.int64)
-
-    def split(mask):
-        nonlocal lev, crd
-        kids = np.stack(np.meshgrid([0, 1], [0, 1], [0, 1], indexing="ij"), -1).reshape(8, 3)
-        c2 = (2 * crd[mask][:, None, :] + kids[None]).reshape(-1, 3)
-        l2 = np.repeat(lev[mask] + 1, 8)
-        lev = np.concatenate([lev[~mask], l2])
-        crd = np.concatenate([crd[~mask], c2])
-
-    def geometry():
-        size = (hi - lo)[None, :] / (nb << lev)[:, None]
-        return lo + (crd + 0.5) * size, size
-
-    for level in range(max_level):
-        at = lev == level
-        if not at.any():
-            continue
-        cen, size = geometry()
-        mask = np.zeros(len(lev), dtype=bool)
-        mask[at] = np.asarray(refine(level, cen[at], size[at]), dtype=bool)
-        if mask.any():
-            split(mask)
-
-    # 2:1 face balance on the finest grid: owner level per finest cell, neighbour maximum per leaf
     while True:
         span = 1 << (max_level - lev)
         levgrid = np.empty((nf, nf, nf), dtype=np.int64)
@@ -199,14 +174,51 @@ def forest(nb, refine, max_level=2, lo=(0.0, 0.0, 0.0), hi=(1.0, 1.0, 1.0)):
         np.maximum.at(leafmax, owner.ravel(), nbmax.ravel())
         bad = leafmax > lev + 1
         if not bad.any():
-            break
-        split(bad)
+            return lev, crd
+        lev, crd = _children(lev, crd, bad)
 
+
+def forest(nb, refine, max_level=2, lo=(0.0, 0.0, 0.0), hi=(1.0, 1.0, 1.0)):
+    """Statically refined periodic forest on an nb^3 base brick (one octree per base element).
+
+    refine(level, center[n,3], size[n]) -> bool[n] marks leaves of that level to split into 8; it is
+    called for level 0, 1, ..., max_level-1 in turn.  The forest is then 2:1 face-balanced (a leaf whose
+    face neighbour is two or more levels finer is split, repeatedly), the leaves are put in Morton order
+    of their anchors on the finest grid (the p4est order), and the sides are built: conforming sides as
+    in brick(), and one side per 2:1 non-conforming face with the coarse quad on one half and the four
+    fine quads (k = s + 2 t over the face's two tangential axes, lower axis first) on the other.  The
+    returned mesh keeps its leaves (mesh.tree: level and integer coordinates) for adapt()."""
+    lo, hi = np.asarray(lo, float), np.asarray(hi, float)
+    g = np.stack(np.meshgrid(np.arange(nb), np.arange(nb), np.arange(nb), indexing="ij"), -1).reshape(-1, 3)
+    lev = np.zeros(len(g), dtype=np.int64)
+    crd = g.astype(np.int64)
+    for level in range(max_level):
+        at = lev == level
+        if not at.any():
+            continue
+        size = (hi - lo)[None, :] / (nb << lev[at])[:, None]
+        cen = lo + (crd[at] + 0.5) * size
+        mask = np.zeros(len(lev), dtype=bool)
+        mask[at] = np.asarray(refine(level, cen, size), dtype=bool)
+        if mask.any():
+            lev, crd = _children(lev, crd, mask)
+    lev, crd = _balance(nb, max_level, lev, crd)
+    return forest_mesh(nb, max_level, lev, crd, lo, hi)
+
+
+def forest_mesh(nb, max_level, lev, crd, lo=(0.0, 0.0, 0.0), hi=(1.0, 1.0, 1.0)):
+    """The mesh of a 2:1-balanced leaf set (level, integer coordinates at that level): Morton order of
+    the anchors on the finest grid, sides as described in forest()."""
+    lo, hi = np.asarray(lo, float), np.asarray(hi, float)
+    nf = nb << max_level
+    lev = np.asarray(lev, dtype=np.int64)
+    crd = np.asarray(crd, dtype=np.int64)
     anchor = crd << (max_level - lev)[:, None]
     order = np.argsort(morton3(anchor[:, 0], anchor[:, 1], anchor[:, 2]), kind="stable")
     lev, crd = lev[order], crd[order]
     E = len(lev)
-    cen, size = geometry()
+    size = (hi - lo)[None, :] / (nb << lev)[:, None]
+    cen = lo + (crd + 0.5) * size
 
     key_scale = np.int64(nf)
     def key(l, c):
@@ -263,6 +275,7 @@ def forest(nb, refine, max_level=2, lo=(0.0, 0.0, 0.0), hi=(1.0, 1.0, 1.0)):
             Q.append(q)
     quads, fids, nqs = np.concatenate(Q), np.concatenate(F), np.concatenate(NQ)
     mesh = Mesh(size, cen, quads, fids, nqs, np.zeros(len(quads), dtype=np.int32), level=lev.astype(np.int8))
+    mesh.tree = dict(nb=nb, max_level=max_level, lev=lev, crd=crd, lo=lo, hi=hi)
     return mesh
 
 
@@ -304,3 +317,81 @@ def batched_workload(nb=24, members=256, member_nx=8, seed=11):
     mesh, groups = concat([f] + [one] * members)
     amps = np.random.default_rng(seed).uniform(0.1, 1.0, size=members)
     return mesh, groups, f, one, amps
+
+
+def adapt(mesh, flags, min_level=0):
+    """One adapt step of a forest mesh (made by forest() or adapt()), as mesh_adapt
+    (source/mesh/p4est/mesh_utils_mod.f90:879-1010): coarsen, refine, then restore the 2:1 balance.
+
+    flags[E]: +1 refine (below max_level), -1 coarsen (only complete families of 8 sibling leaves above
+    min_level that are all flagged), 0 keep.  The new leaf set is 2:1-balanced again (balance may
+    refine further, and a coarsening that balance would undo is dropped).  Returns (new mesh, remap) with remap[E_new, 4]
+    int32 rows (kind, src, depth, offsets) for nemo_gpu_adapt:
+      kind 0: copy of old element src;
+      kind 1: refinement of old element src, an ancestor `depth` levels up; offsets = ox | oy << 8 |
+              oz << 16 locate the new element inside it (0 <= o < 2^depth);
+      kind 2: projection of the 8 old children src .. src + 7 (child c = sx + 2 sy + 4 sz).
+    The data movement mirrors kernel_amr_refine / kernel_amr_coarsen
+    (source/kernel/dgsem/weakform/2d/kernel_amr_mod.f90:12-73) in 3D.  Unlike the reference's
+    one-level walk over old and new quads (:980-1005), a leaf that balance refines by more than one
+    level, or a family whose coarsening balance would undo, is handled (deeper interpolation; the
+    coarsening is dropped)."""
+    t = mesh.tree
+    nb, max_level, lo, hi = t["nb"], t["max_level"], t["lo"], t["hi"]
+    lev, crd = t["lev"], t["crd"]
+    flags = np.asarray(flags)
+    old = {(int(l), int(c[0]), int(c[1]), int(c[2])): i for i, (l, c) in enumerate(zip(lev, crd))}
+    # complete coarsening families (8 leaves of one parent, all flagged, consecutive c = sx + 2sy + 4sz)
+    fam = {}
+    for i in np.nonzero((flags < 0) & (lev > max(int(min_level), 0)))[0]:
+        p = (int(lev[i]) - 1, int(crd[i, 0]) >> 1, int(crd[i, 1]) >> 1, int(crd[i, 2]) >> 1)
+        fam.setdefault(p, []).append(int(i))
+    families = {}
+    for p, members in fam.items():
+        if len(members) != 8:
+            continue
+        ch = {}
+        for i in members:
+            c = (int(crd[i, 0]) & 1) | ((int(crd[i, 1]) & 1) << 1) | ((int(crd[i, 2]) & 1) << 2)
+            ch[c] = i
+        first = ch[0]
+        if all(ch[c] == first + c for c in range(8)):
+            families[p] = first
+    refine = (flags > 0) & (lev < max_level)
+    while True:
+        gone = np.zeros(len(lev), dtype=bool)
+        for first in families.values():
+            gone[first:first + 8] = True
+        l_new, c_new = _children(lev[~gone], crd[~gone], refine[~gone])
+        if families:
+            pl = np.array([p[0] for p in families], dtype=np.int64)
+            pc = np.array([p[1:] for p in families], dtype=np.int64)
+            l_new = np.concatenate([l_new, pl])
+            c_new = np.concatenate([c_new, pc])
+        l_bal, c_bal = _balance(nb, max_level, l_new, c_new)
+        present = {(int(l), int(c[0]), int(c[1]), int(c[2])) for l, c in zip(l_bal, c_bal)}
+        undone = [p for p in families if p not in present]
+        if not undone:
+            break
+        for p in undone:
+            del families[p]
+    new = forest_mesh(nb, max_level, l_bal, c_bal, lo, hi)
+    nl, nc = new.tree["lev"], new.tree["crd"]
+    remap = np.zeros((new.E, 4), dtype=np.int32)
+    for e in range(new.E):
+        key = (int(nl[e]), int(nc[e, 0]), int(nc[e, 1]), int(nc[e, 2]))
+        if key in old:
+            remap[e] = (0, old[key], 0, 0)
+            continue
+        if key in families:
+            remap[e] = (2, families[key], 1, 0)
+            continue
+        for depth in range(1, int(nl[e]) + 1):
+            anc = (key[0] - depth, key[1] >> depth, key[2] >> depth, key[3] >> depth)
+            if anc in old:
+                o = [key[1 + a] - (anc[1 + a] << depth) for a in range(3)]
+                remap[e] = (1, old[anc], depth, o[0] | (o[1] << 8) | (o[2] << 16))
+                break
+        else:
+            raise RuntimeError(f"new element {e} has no source in the old forest")
+    return new, remap

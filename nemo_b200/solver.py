@@ -121,6 +121,38 @@ class Solver:
     def set_schedule(self, mode, ctas=0):
         call("nemo_gpu_set_schedule", int(mode), int(ctas))
 
+    def amr_flags(self, refine_threshold, coarsen_threshold):
+        """Adapt flags of the current state from the device density probe (nemo_gpu_amr_flags)."""
+        f = np.empty(self.E, dtype=np.int32)
+        call("nemo_gpu_amr_flags", float(refine_threshold), float(coarsen_threshold), abi.ptr(f))
+        return f
+
+    def adapt(self, flags, min_level=0):
+        """One forest adapt step (mesh.adapt): new mesh, state remapped on the device; returns the
+        new mesh and its remap rows."""
+        from . import mesh as mesh_mod
+        new, remap = mesh_mod.adapt(self.mesh, flags, min_level=min_level)
+        remap = np.ascontiguousarray(remap, dtype=np.int32)
+        if new.E == self.E and not np.any(remap[:, 0]):   # nothing changed
+            return self.mesh, remap
+        call("nemo_gpu_adapt", new.E, abi.ptr(new.delta), abi.ptr(new.center), new.S, abi.ptr(new.side_quads),
+             abi.ptr(new.side_faceid), abi.ptr(new.side_nquads), abi.ptr(new.boundary), abi.ptr(remap))
+        self.mesh, self.E = new, new.E
+        return new, remap
+
+    def run_amr(self, nsteps, every, refine_threshold, coarsen_threshold, min_level=0):
+        """nsteps steps with an adapt before every `every`-th (hook_pre_timestep_300 of the Sedov setup,
+        source/setups/euler/3d/sedov/setup_amr_mod.f90:7-21): device density flags, host forest
+        rebuild, device remap.  Returns (t, number of elements after each adapt)."""
+        sizes, done, t = [], 0, 0.0
+        while done < nsteps:
+            self.adapt(self.amr_flags(refine_threshold, coarsen_threshold), min_level=min_level)
+            sizes.append(self.E)
+            k = min(every, nsteps - done)
+            t, _ = self.run(nsteps=k)
+            done += k
+        return t, sizes
+
     def totals(self):
         out = np.zeros(10)
         call("nemo_gpu_totals", abi.ptr(out))

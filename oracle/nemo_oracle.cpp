@@ -1258,13 +1258,23 @@ void mortar_fluxes(const Ctx& c, const Mesh& M, const double* u, int nthreads) {
         for (int b = 0; b < NN; ++b)
             for (int a = 0; a < NN; ++a)
                 for (int v = 0; v < V; ++v) uc[a + NN * b][v] = u[(v * M.E + qc) * NP + face_node(fc, a, b)];
+        // mean of the coarse trace over the face (LGL weights on [-1/2,1/2]): the admissible state that
+        // replaces a prolonged sub-face trace with an inadmissible node
+        double ucm[VMAX];
+        for (int v = 0; v < V; ++v) {
+            double acc = 0.0;
+            for (int b = 0; b < NN; ++b)
+                for (int a = 0; a < NN; ++a) acc = acc + ((0.5 * op.w[a]) * (0.5 * op.w[b])) * uc[a + NN * b][v];
+            ucm[v] = acc;
+        }
         for (int k = 0; k < 4; ++k) {
             const int s = k & 1, tt = k >> 1;
             const int64_t qf = t[2 + k];
             double* mf = M.mflux + (size_t)(5 * m + 1 + k) * NF * VMAX;
+            double ups[NF][VMAX];
+            bool ok = true;
             for (int j = 0; j < NN; ++j)
                 for (int i = 0; i < NN; ++i) {
-                    double up[VMAX], uf[VMAX], F[VMAX], Gf[VMAX], Gc[VMAX];
                     for (int v = 0; v < V; ++v) {
                         double acc = 0.0;
                         for (int bb = 0; bb < NN; ++bb) {
@@ -1272,7 +1282,15 @@ void mortar_fluxes(const Ctx& c, const Mesh& M, const double* u, int nthreads) {
                             for (int aa = 0; aa < NN; ++aa) in = in + op.pro[s][i * NN + aa] * uc[aa + NN * bb][v];
                             acc = acc + op.pro[tt][j * NN + bb] * in;
                         }
-                        up[v] = acc;
+                        ups[i + NN * j][v] = acc;
+                    }
+                    ok = ok && isvalid_any(c, ups[i + NN * j]);
+                }
+            for (int j = 0; j < NN; ++j)
+                for (int i = 0; i < NN; ++i) {
+                    double up[VMAX], uf[VMAX], F[VMAX], Gf[VMAX], Gc[VMAX];
+                    for (int v = 0; v < V; ++v) {
+                        up[v] = ok ? ups[i + NN * j][v] : ucm[v];
                         uf[v] = u[(v * M.E + qf) * NP + face_node(ff, i, j)];
                     }
                     const double* uL = coarse_left ? up : uf;
@@ -1382,6 +1400,107 @@ void or_mortar_operators(double* pro, double* prj) {
     build_ops(op);
     std::memcpy(pro, op.pro, sizeof op.pro);
     std::memcpy(prj, op.prj, sizeof op.prj);
+}
+
+// Element data of an adapted forest (kernel_amr_refine / kernel_amr_coarsen,
+// source/kernel/dgsem/weakform/2d/kernel_amr_mod.f90:12-73, in 3D as the tensor products of
+// source/setups/euler/3d/sedov/setup_amr_mod.f90:67-125): per new element a remap row (kind, src,
+// depth, offsets): 0 copy, 1 interpolation of ancestor src at the new nodes, 2 sum over the 8 children
+// src..src+7 of their projections.  V variables, SoA [V][E][64].  Where the high-order transfer gives a
+// state that is not admissible, the reference steps down to lower orders until it is
+// (setup_amr_replace_refine / _coarsen, :82-95 / :114-124); here the step down is to the lowest order
+// at once, the mean: every new element of an ancestor with an inadmissible refined element takes the
+// ancestor's mean, an inadmissible coarsened element the mean of its 8 children.  Both conserve.
+static double elem_mean(const Ops& op, const double* ue) {
+    double acc = 0.0;
+    for (int c = 0; c < NN; ++c)
+        for (int b = 0; b < NN; ++b)
+            for (int a = 0; a < NN; ++a) acc = acc + ((op.w[a] * op.w[b]) * op.w[c]) * ue[nidx(a, b, c)];
+    return acc;
+}
+
+void or_remap(int V, int64_t Eo, const double* uo, int64_t En, const int32_t* remap, double kappa, double mu0,
+              double* un) {
+    Ops op;
+    build_ops(op);
+    for (int64_t e = 0; e < En; ++e) {
+        const int32_t* r = remap + 4 * e;
+        const int kind = r[0];
+        const int64_t src = r[1];
+        for (int kk = 0; kk < NN; ++kk)
+            for (int jj = 0; jj < NN; ++jj)
+                for (int ii = 0; ii < NN; ++ii) {
+                    const int n = nidx(ii, jj, kk);
+                    if (kind == 0) {
+                        for (int v = 0; v < V; ++v) un[((int64_t)v * En + e) * NP + n] = uo[((int64_t)v * Eo + src) * NP + n];
+                        continue;
+                    }
+                    if (kind == 1) {
+                        const int depth = r[2], off = r[3];
+                        const int o[3] = {off & 0xff, (off >> 8) & 0xff, (off >> 16) & 0xff};
+                        const int nd[3] = {ii, jj, kk};
+                        double w[3][NN];
+                        for (int d = 0; d < 3; ++d) {
+                            const double xi = -1.0 + (2.0 * (double)o[d] + 1.0 + op.x[nd[d]]) / (double)(1 << depth);
+                            for (int a = 0; a < NN; ++a) w[d][a] = lagrange(NN, op.x, a, xi);
+                        }
+                        for (int v = 0; v < V; ++v) {
+                            const double* ue = uo + ((int64_t)v * Eo + src) * NP;
+                            double acc = 0.0;
+                            for (int c = 0; c < NN; ++c)
+                                for (int b = 0; b < NN; ++b)
+                                    for (int a = 0; a < NN; ++a)
+                                        acc = acc + ((w[0][a] * w[1][b]) * w[2][c]) * ue[nidx(a, b, c)];
+                            un[((int64_t)v * En + e) * NP + n] = acc;
+                        }
+                        continue;
+                    }
+                    for (int v = 0; v < V; ++v) {
+                        double acc = 0.0;
+                        for (int ch = 0; ch < 8; ++ch) {
+                            const double* px = op.prj[ch & 1];
+                            const double* py = op.prj[(ch >> 1) & 1];
+                            const double* pz = op.prj[ch >> 2];
+                            const double* ue = uo + ((int64_t)v * Eo + src + ch) * NP;
+                            for (int c = 0; c < NN; ++c)
+                                for (int b = 0; b < NN; ++b)
+                                    for (int a = 0; a < NN; ++a)
+                                        acc = acc + ((px[ii * NN + a] * py[jj * NN + b]) * pz[kk * NN + c]) * ue[nidx(a, b, c)];
+                        }
+                        un[((int64_t)v * En + e) * NP + n] = acc;
+                    }
+                }
+    }
+    // admissibility of the transferred elements; fall back to the means
+    const MhdPar P{kappa, mu0, 0.0};
+    std::vector<char> bad(Eo + En, 0);
+    for (int64_t e = 0; e < En; ++e) {
+        const int kind = remap[4 * e];
+        if (kind == 0) continue;
+        bool ok = true;
+        for (int n = 0; n < NP; ++n) {
+            double q[9];
+            for (int v = 0; v < V; ++v) q[v] = un[((int64_t)v * En + e) * NP + n];
+            ok = ok && (V == 9 ? m_isvalid(q, P) : e_isvalid(q, kappa));
+        }
+        if (!ok) bad[kind == 1 ? remap[4 * e + 1] : Eo + e] = 1;
+    }
+    for (int64_t e = 0; e < En; ++e) {
+        const int kind = remap[4 * e];
+        const int64_t src = remap[4 * e + 1];
+        if (kind == 0 || !bad[kind == 1 ? src : Eo + e]) continue;
+        for (int v = 0; v < V; ++v) {
+            double m;
+            if (kind == 1) {
+                m = elem_mean(op, uo + ((int64_t)v * Eo + src) * NP) * 0.125;
+            } else {
+                double acc = 0.0;
+                for (int ch = 0; ch < 8; ++ch) acc = acc + elem_mean(op, uo + ((int64_t)v * Eo + src + ch) * NP);
+                m = acc * 0.015625;
+            }
+            for (int n = 0; n < NP; ++n) un[((int64_t)v * En + e) * NP + n] = m;
+        }
+    }
 }
 
 // mortar table [nm][6] of the mesh that the following calls use (nm = 0: conforming mesh)

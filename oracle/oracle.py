@@ -44,6 +44,8 @@ def lib():
         L.or_operators.argtypes = [_dp] * 5
         L.or_mortar_operators.argtypes = [_dp, _dp]
         L.or_set_mortars.argtypes = [ctypes.c_int64, ctypes.c_void_p]
+        L.or_remap.argtypes = [ctypes.c_int, ctypes.c_int64, _dp, ctypes.c_int64, ctypes.c_void_p, ctypes.c_double,
+                               ctypes.c_double, _dp]
         L.or_rk_coeffs.argtypes = [_dp] * 3
         L.or_alpha.argtypes = [ctypes.c_void_p, ctypes.c_int64, _ip, _dp, _dp, _dp, ctypes.c_int]
         L.or_rhs.argtypes = [ctypes.c_void_p, ctypes.c_int64, _ip, _dp, _dp, ctypes.c_void_p, _dp,
@@ -106,6 +108,23 @@ def mortar_operators():
     pro, prj = np.zeros((2, 4, 4)), np.zeros((2, 4, 4))
     lib().or_mortar_operators(_p(pro), _p(prj))
     return pro, prj
+
+
+def amr_flags(u, refine_threshold, coarsen_threshold):
+    """Density probes of the Sedov setup (source/setups/euler/3d/sedov/setup_amr_mod.f90:23-65) per
+    element: +1 if any node's density > refine_threshold, else -1 if none > coarsen_threshold, else 0."""
+    dmax = np.asarray(u)[0].max(axis=1)
+    return np.where(dmax > refine_threshold, 1, np.where(dmax > coarsen_threshold, 0, -1)).astype(np.int32)
+
+
+def remap(u, remap_rows, kappa=1.4, mu0=1.0):
+    """State [V, E_old, 64] -> [V, E_new, 64] by adapt remap rows (mesh.adapt); inadmissible
+    transferred elements fall back to the conservative means (V = 9: GLM-MHD admissibility)."""
+    u = _f64(u)
+    r = np.ascontiguousarray(remap_rows, dtype=np.int32)
+    out = np.zeros((u.shape[0], len(r), 64))
+    lib().or_remap(u.shape[0], u.shape[1], _p(u), len(r), r.ctypes.data, float(kappa), float(mu0), _p(out))
+    return out
 
 
 def lgl(N):

@@ -124,3 +124,33 @@ def test_concat_batch_neighbors():
     for i in range(2):
         blk = nbr[f.E + i * b.E: f.E + (i + 1) * b.E]
         assert blk.min() >= f.E + i * b.E and blk.max() < f.E + (i + 1) * b.E
+
+
+def shocked_coarse_state(m):
+    """A state whose coarse mortar elements hold density P(x) P(y) P(z), P through 1, 1e-3, 1e-3, 1 at
+    the nodes: admissible at every node, but the prolonged trace dips below zero on the sub-faces."""
+    u = setups.smooth_random(m, seed=4)
+    x = orc.lgl(3)[0]
+    p = np.where(np.abs(np.abs(x) - 1.0) < 1e-12, 1.0, 1e-3)
+    rho = np.einsum("k,j,i->kji", p, p, p).ravel()                    # node n = i + 4j + 16k
+    qc = np.unique(m.mortars()[:, 0])
+    u[0, qc] = rho
+    u[1:4, qc] = 0.0
+    u[4, qc] = 2.5
+    return u, qc
+
+
+def test_mortar_trace_guard():
+    m = band_forest(4)
+    u, qc = shocked_coarse_state(m)
+    pro, _ = orc.mortar_operators()
+    face = u[0, qc[0]].reshape(4, 4, 4)[0]                             # the k = 0 face, [j][i]
+    sub = np.einsum("ia,jb,ba->ji", pro[0], pro[0], face)
+    assert sub.min() < 0.0                                               # the plain prolongation fails
+    c = abi.default_cfg(indicator=abi.IND_MODAL, positivity=1)
+    r = orc.Oracle.for_mesh(c, m).rhs(u)
+    assert np.all(np.isfinite(r))
+    o = orc.Oracle.for_mesh(c, m)
+    u2, _, _, _ = o.run(u, nsteps=2)
+    assert np.all(np.isfinite(u2))
+    np.testing.assert_allclose(o.totals(u2), o.totals(u), rtol=1e-13, atol=1e-13)

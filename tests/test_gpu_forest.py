@@ -82,3 +82,20 @@ def test_kh_forest_fp32_and_conservation():
     # the layer starts discontinuous: elements whose FP32 indicator lands on the other side of the
     # alpha_min clip get a different blend, which dominates the difference (1.5e-6 observed)
     assert np.sum(np.abs(u32[0] - u64[0])) / np.sum(np.abs(u64[0])) < 1e-5
+
+
+def test_mortar_trace_guard_bit_exact():
+    """Coarse mortar elements whose prolonged traces have negative density: the guarded mortar kernel
+    against the oracle's, then a short blended run."""
+    from test_forest import shocked_coarse_state
+    m = band_forest(4)
+    u, _ = shocked_coarse_state(m)
+    c = abi.default_cfg(indicator=abi.IND_MODAL, positivity=1)
+    s = Solver(c, m)
+    s.upload(u)
+    o = orc.Oracle.for_mesh(c, m)
+    r = s.rhs()
+    assert np.all(np.isfinite(r)) and np.array_equal(r, o.rhs(u))
+    s.run(nsteps=2)
+    uc, _, _, _ = o.run(u, nsteps=2)
+    assert np.array_equal(s.download(), uc)
