@@ -175,6 +175,21 @@ int nemo_gpu_unpack_elements(const int32_t* idx_dev, int64_t n, const double* bu
 int nemo_gpu_upload_state(const double* host, int64_t elem_stride_bytes);
 int nemo_gpu_download_state(double* host, int64_t elem_stride_bytes);
 
+/* Checkpoint staging (the state that hook_checkpoint_fill writes, source/checkpoint/flash/
+   checkpoint_mod.f90:319-364, and the restart that source/nemo_prog.f90:107-114 leaves as a TODO).
+   nemo_gpu_checkpoint_begin takes a snapshot of the state, of t (group 0) and of the step counter in
+   stream order -- after everything enqueued before it -- into a library-owned device buffer, starts
+   the device->host copy into host (layout as download_state) on a second stream and returns; later
+   steps run while the copy proceeds.  host must stay valid, and should be page-locked for the copy
+   to overlap, until nemo_gpu_checkpoint_wait returns the snapshot's t and step count.  A second
+   begin first waits for the previous copy.  nemo_gpu_set_time restores t (every group) and the step
+   counter after an upload_state, which resets both: upload + set_time is the restart.  alpha_host
+   (optional, nelems doubles) receives the blending coefficients of the last stage (zeros without an
+   indicator), copied with the state. */
+int nemo_gpu_checkpoint_begin(double* host, int64_t elem_stride_bytes, double* alpha_host);
+int nemo_gpu_checkpoint_wait(double* t_out, int64_t* steps_out);
+int nemo_gpu_set_time(double t, int64_t steps);
+
 /* hook_calc_timestep_200: dt = 0.5^(D-1) * cfl / (2*N_NODES-1) * min_e min_d (delta_d / lambda_d),
    lmax = max wave speed.  Device reduction in FP64.  dt_out/lmax_out are host pointers. */
 int nemo_gpu_calc_timestep(double cfl, double* dt_out, double* lmax_out);

@@ -30,6 +30,7 @@ EXPORTS = [
     "nemo_gpu_mlp_train", "nemo_gpu_mlp_grad", "nemo_gpu_mlp_forward", "nemo_gpu_mortar_operators",
     "nemo_gpu_autotune", "nemo_gpu_set_schedule", "nemo_gpu_set_owned", "nemo_gpu_pack_elements",
     "nemo_gpu_unpack_elements", "nemo_gpu_adapt", "nemo_gpu_amr_flags",
+    "nemo_gpu_checkpoint_begin", "nemo_gpu_checkpoint_wait", "nemo_gpu_set_time",
 ]
 
 
@@ -104,6 +105,9 @@ def load(path=LIB_PATH):
         "nemo_gpu_unpack_elements": [vp, i64, vp],
         "nemo_gpu_adapt": [i64, vp, vp, i64, vp, vp, vp, vp, vp],
         "nemo_gpu_amr_flags": [dbl, dbl, vp],
+        "nemo_gpu_checkpoint_begin": [vp, i64, vp],
+        "nemo_gpu_checkpoint_wait": [ctypes.POINTER(dbl), ctypes.POINTER(i64)],
+        "nemo_gpu_set_time": [dbl, i64],
     }
     for name, args in sig.items():
         f = getattr(L, name)

@@ -218,6 +218,16 @@ struct Lib {
     bool timing = false;
     double t_stage_ms = 0.0, t_total_ms = 0.0;
     int64_t n_stage = 0, n_total = 0;
+
+    // checkpoint staging: an AoS copy of the state (and of t, steps) taken in stream order, copied
+    // to the host on its own stream while the library stream computes on
+    double* ckpt = nullptr;
+    int64_t ckpt_bytes = 0;
+    double* ckpt_meta = nullptr;       // device [2]: t of group 0, steps (bits)
+    double* ckpt_meta_host = nullptr;  // pinned [2]
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t ckpt_ready = nullptr, ckpt_done = nullptr;
+    bool ckpt_pending = false;
 };
 
 Lib g;
@@ -248,7 +258,16 @@ void release_graphs() {
         }
 }
 
+void release_checkpoint() {
+    if (g.ckpt_pending) cudaEventSynchronize(g.ckpt_done);
+    g.ckpt_pending = false;
+    free_dev(g.ckpt);
+    g.ckpt = nullptr;
+    g.ckpt_bytes = 0;
+}
+
 void release_mesh() {
+    release_checkpoint();
     release_graphs();
     free_dev(g.u[0]); free_dev(g.u[1]); free_dev(g.reg); free_dev(g.stagebuf);
     free_dev(g.alpha[0]); free_dev(g.alpha[1]); free_dev(g.alpha_used);
@@ -812,6 +831,78 @@ int nemo_gpu_download_state(double* host, int64_t stride) {
     return NEMO_OK;
 }
 
+int nemo_gpu_checkpoint_begin(double* host, int64_t stride, double* alpha_host) {
+    int st = ensure_ready();
+    if (st) return st;
+    if (!host) return fail(NEMO_ERR_ARG, "host is NULL");
+    const size_t row = sizeof(double) * (size_t)g.V * NP;
+    if (stride < (int64_t)row) return fail(NEMO_ERR_ARG, "element stride %lld < %zu bytes", (long long)stride, row);
+    if (g.ckpt_pending) {  // the staging buffer is reused: the previous copy must have left it
+        CK(cudaEventSynchronize(g.ckpt_done));
+        g.ckpt_pending = false;
+    }
+    if (!g.copy_stream) {
+        CK(cudaStreamCreateWithFlags(&g.copy_stream, cudaStreamNonBlocking));
+        CK(cudaEventCreateWithFlags(&g.ckpt_ready, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&g.ckpt_done, cudaEventDisableTiming));
+        CK(cudaMalloc(&g.ckpt_meta, 2 * sizeof(double)));
+        CK(cudaHostAlloc(&g.ckpt_meta_host, 2 * sizeof(double), cudaHostAllocDefault));
+    }
+    const int64_t bytes = (int64_t)row * g.E;
+    const int64_t abytes = (int64_t)sizeof(double) * g.E;   // blending coefficients after the state
+    if (g.ckpt_bytes != bytes + abytes) {
+        free_dev(g.ckpt);
+        g.ckpt = nullptr;
+        g.ckpt_bytes = 0;
+        CK(cudaMalloc(&g.ckpt, (size_t)(bytes + abytes)));
+        g.ckpt_bytes = bytes + abytes;
+    }
+    double* ckpt_alpha = g.ckpt + (size_t)g.V * NP * g.E;
+    if (alpha_host && !blended()) std::fill(alpha_host, alpha_host + g.E, 0.0);
+    // in stream order: the snapshot is the state after everything enqueued so far
+    CK(launch_soa_to_aos(g.u[g.cur], g.ckpt, g.E, g.V, g.stream));
+    CK(cudaMemcpyAsync(g.ckpt_meta, &g.ctrl->t[0], sizeof(double), cudaMemcpyDeviceToDevice, g.stream));
+    CK(cudaMemcpyAsync(g.ckpt_meta + 1, &g.ctrl->steps, sizeof(double), cudaMemcpyDeviceToDevice, g.stream));
+    if (alpha_host && blended())
+        CK(cudaMemcpyAsync(ckpt_alpha, g.alpha_used, (size_t)abytes, cudaMemcpyDeviceToDevice, g.stream));
+    CK(cudaEventRecord(g.ckpt_ready, g.stream));
+    CK(cudaStreamWaitEvent(g.copy_stream, g.ckpt_ready, 0));
+    if (stride == (int64_t)row) CK(cudaMemcpyAsync(host, g.ckpt, (size_t)bytes, cudaMemcpyDeviceToHost, g.copy_stream));
+    else CK(cudaMemcpy2DAsync(host, (size_t)stride, g.ckpt, row, row, (size_t)g.E, cudaMemcpyDeviceToHost, g.copy_stream));
+    if (alpha_host && blended())
+        CK(cudaMemcpyAsync(alpha_host, ckpt_alpha, (size_t)abytes, cudaMemcpyDeviceToHost, g.copy_stream));
+    CK(cudaMemcpyAsync(g.ckpt_meta_host, g.ckpt_meta, 2 * sizeof(double), cudaMemcpyDeviceToHost, g.copy_stream));
+    CK(cudaEventRecord(g.ckpt_done, g.copy_stream));
+    g.ckpt_pending = true;
+    return NEMO_OK;
+}
+
+int nemo_gpu_checkpoint_wait(double* t_out, int64_t* steps_out) {
+    if (!g.ckpt_pending) return fail(NEMO_ERR_STATE, "no checkpoint copy in flight (nemo_gpu_checkpoint_begin)");
+    CK(cudaEventSynchronize(g.ckpt_done));
+    g.ckpt_pending = false;
+    if (t_out) *t_out = g.ckpt_meta_host[0];
+    if (steps_out) {
+        unsigned long long s = 0;
+        std::memcpy(&s, &g.ckpt_meta_host[1], sizeof s);
+        *steps_out = (int64_t)s;
+    }
+    return NEMO_OK;
+}
+
+int nemo_gpu_set_time(double t, int64_t steps) {
+    int st = ensure_ready();
+    if (st) return st;
+    if (!(t >= 0.0) || !std::isfinite(t) || steps < 0) return fail(NEMO_ERR_ARG, "need a finite t >= 0 and steps >= 0");
+    double ts[MAX_GROUPS];
+    for (int i = 0; i < MAX_GROUPS; ++i) ts[i] = t;
+    const unsigned long long s = (unsigned long long)steps;
+    CK(cudaMemcpyAsync(g.ctrl->t, ts, sizeof(double) * g.ngroups, cudaMemcpyHostToDevice, g.stream));
+    CK(cudaMemcpyAsync(&g.ctrl->steps, &s, sizeof s, cudaMemcpyHostToDevice, g.stream));
+    CK(cudaStreamSynchronize(g.stream));
+    return NEMO_OK;
+}
+
 int nemo_gpu_calc_timestep(double cfl, double* dt_out, double* lmax_out) {
     int st = ensure_ready();
     if (st) return st;
@@ -1342,6 +1433,14 @@ int nemo_gpu_finalize(void) {
     free_dev(g.tot);
     free_dev(g.mlp32);
     free_dev(g.mlp64);
+    free_dev(g.ckpt_meta);
+    if (g.ckpt_meta_host) cudaFreeHost(g.ckpt_meta_host);
+    if (g.ckpt_ready) cudaEventDestroy(g.ckpt_ready);
+    if (g.ckpt_done) cudaEventDestroy(g.ckpt_done);
+    if (g.copy_stream) cudaStreamDestroy(g.copy_stream);
+    g.ckpt_meta = g.ckpt_meta_host = nullptr;
+    g.ckpt_ready = g.ckpt_done = nullptr;
+    g.copy_stream = nullptr;
     g.ctrl = nullptr;
     g.tot = nullptr;
     g.mlp32 = nullptr;

@@ -147,6 +147,30 @@ interface
         integer(c_int8_t), intent(in) :: side_faceid(*), side_nquads(*)
         integer(c_int) :: st
     end function
+
+    !! Checkpoint staging: snapshot in stream order, device->host copy on a second stream
+    !! (hook_checkpoint_fill); restart = upload_state + set_time.
+    function nemo_gpu_checkpoint_begin(host, elem_stride_bytes, alpha_host) result(st) &
+            bind(c, name="nemo_gpu_checkpoint_begin")
+        import :: c_int, c_int64_t, c_ptr
+        type(c_ptr), value :: host, alpha_host
+        integer(c_int64_t), value :: elem_stride_bytes
+        integer(c_int) :: st
+    end function
+
+    function nemo_gpu_checkpoint_wait(t_out, steps_out) result(st) bind(c, name="nemo_gpu_checkpoint_wait")
+        import :: c_int, c_int64_t, c_double
+        real(c_double), intent(out) :: t_out
+        integer(c_int64_t), intent(out) :: steps_out
+        integer(c_int) :: st
+    end function
+
+    function nemo_gpu_set_time(t, steps) result(st) bind(c, name="nemo_gpu_set_time")
+        import :: c_int, c_int64_t, c_double
+        real(c_double), value :: t
+        integer(c_int64_t), value :: steps
+        integer(c_int) :: st
+    end function
 end interface
 
 contains

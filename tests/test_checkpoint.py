@@ -1,0 +1,80 @@
+"""FLASH-layout checkpoints (CPU): the block tree (ancestors level by level, then the leaves), the
+datasets' names, shapes and records, the parents' restriction, and write -> read round trips of a
+forest and of a brick (mesh, state, time and step count)."""
+import numpy as np
+
+from nemo_b200 import abi, checkpoint, mesh, setups
+from oracle import oracle as orc
+
+
+def band_forest():
+    return mesh.forest(4, lambda lvl, c, s: np.abs(c[:, 1] - 0.5) < 0.2 / (1 + lvl), max_level=2)
+
+
+def test_block_tree():
+    m = band_forest()
+    t = checkpoint.block_tree(m)
+    nin, nb = t["n_inner"], t["nblocks"]
+    assert nb == nin + m.E
+    assert np.array_equal(t["level"][nin:], m.tree["lev"])            # leaves last, in mesh order
+    assert np.all(np.diff(t["level"][:nin]) >= 0)                     # ancestors level by level
+    for i in range(nb):
+        p = t["parent"][i]
+        if t["level"][i] == 0:
+            assert p == -1 and t["which"][i] == -1
+        else:
+            assert t["children"][p, t["which"][i]] == i
+            assert np.array_equal(t["crd"][p], t["crd"][i] >> 1)
+    assert np.all(t["children"][:nin] >= 0) and np.all(t["children"][nin:] == -1)
+
+
+def test_datasets_and_restriction():
+    m = band_forest()
+    x, y, z = m.node_coords(orc.lgl(3)[0])
+    u = np.stack([1.0 + x + y * y, 0.5 * x * z, y, z, 3.0 + x * y]).copy()   # degree <= 2
+    c = abi.default_cfg()
+    ds = checkpoint.datasets(m, u, 0.25, 17, c, alpha=np.linspace(0, 0.5, m.E))
+    t = checkpoint.block_tree(m)
+    nb, nin = t["nblocks"], t["n_inner"]
+    assert ds["dens"].shape == (nb, 4, 4, 4) and ds["gid"].shape == (nb, 15)
+    assert ds["bounding box"].shape == (nb, 3, 2) and ds["unknown names"].shape == (6, 1)
+    assert [n[0] for n in ds["unknown names"]] == [b"dens", b"momx", b"momy", b"momz", b"ener", b"blnd"]
+    assert np.array_equal(ds["node type"], np.r_[np.full(nin, 2), np.ones(m.E)])
+    iscal = {r["name"]: r["value"] for r in ds["integer scalars"]}
+    assert iscal[b"nstep"] == 17 and iscal[b"globalnumblocks"] == nb
+    assert {r["name"]: r["value"] for r in ds["real scalars"]}[b"time"] == 0.25
+    np.testing.assert_array_equal(ds["dens"][nin:].reshape(m.E, 64), u[0])
+    # parents: the projection reproduces the quadratic at the parent's own nodes
+    xn = orc.lgl(3)[0]
+    for i in range(nin):
+        cen, size = ds["coordinates"][i], ds["block size"][i]
+        X = cen[0] + 0.5 * size[0] * xn[None, None, :]
+        Y = cen[1] + 0.5 * size[1] * xn[None, :, None]
+        np.testing.assert_allclose(ds["dens"][i], np.broadcast_to(1.0 + X + Y * Y, (4, 4, 4)), atol=1e-12)
+    np.testing.assert_array_equal(ds["blnd"][nin:, 0, 0, 0], np.linspace(0, 0.5, m.E))
+
+
+def _round_trip(m, tmp_path):
+    u = setups.smooth_random(m, seed=9)
+    path = str(tmp_path / "chkpt_000000.f5.npz")
+    checkpoint.write(path, checkpoint.datasets(m, u, 0.125, 40, abi.default_cfg()))
+    m2, u2, t, steps = checkpoint.read(path)
+    assert t == 0.125 and steps == 40 and m2.E == m.E
+    np.testing.assert_array_equal(m2.delta, m.delta)
+    np.testing.assert_array_equal(m2.center, m.center)
+    np.testing.assert_array_equal(m2.neighbors(), m.neighbors())
+    np.testing.assert_array_equal(u2, u)
+
+
+def test_round_trip_forest(tmp_path):
+    _round_trip(band_forest(), tmp_path)
+
+
+def test_round_trip_adapted_forest(tmp_path):
+    m = band_forest()
+    f = np.where(m.center[:, 0] < 0.3, 1, np.where(m.center[:, 0] > 0.6, -1, 0))
+    _round_trip(mesh.adapt(m, f)[0], tmp_path)
+
+
+def test_round_trip_brick(tmp_path):
+    _round_trip(mesh.brick(4), tmp_path)
