@@ -28,6 +28,10 @@ constexpr int TPE = 16;         // threads per element, one per line position (a
 constexpr int NT = EPC * TPE;   // 128 threads: a warp holds exactly two elements
 constexpr int V = 5;
 constexpr int NQ = 6;           // FP32 node data: rho, vx, vy, vz, p, beta
+// element stride of the FP32 shared-memory arrays (node data, rhs terms, epilogue scratch): the 6
+// extra words move the second element of a warp onto other banks (fewer shared-memory conflicts
+// in the line accesses; 2.4 % faster per stage than the unpadded 64 on B200)
+constexpr int SP = NP + 6;
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) {
     return static_cast<unsigned>(__cvta_generic_to_shared(p));
@@ -287,7 +291,7 @@ __device__ __forceinline__ void epilogue32(const StageArgs& a, const double* su,
         // modal transforms of rho*p (and, for the features, rho and p) fused over the quantities:
         // x in registers, y and z through shared memory [3][EPC][64] each
         float* t1 = scratch;                 // [3][EPC][64]
-        float* t2 = scratch + 3 * EPC * NP;  // [3][EPC][64]
+        float* t2 = scratch + 3 * EPC * SP;  // [3][EPC][64]
         float tot[3] = {0.f, 0.f, 0.f}, cl1 = 0.f, cl2 = 0.f, Eo[2][6];
 #pragma unroll
         for (int w = 0; w < 2; ++w)
@@ -304,7 +308,7 @@ __device__ __forceinline__ void epilogue32(const StageArgs& a, const double* su,
                         const float qv = w == 0 ? qr[i] * qp[i] : (w == 1 ? qr[i] : qp[i]);
                         s += (float)k.Vinv[o * NN + i] * qv;
                     }
-                    t1[(w * EPC + el) * NP + nidx(o, la, lb)] = s;
+                    t1[(w * EPC + el) * SP + nidx(o, la, lb)] = s;
                 }
             }
         }
@@ -315,8 +319,8 @@ __device__ __forceinline__ void epilogue32(const StageArgs& a, const double* su,
                 for (int o = 0; o < NN; ++o) {
                     float s = 0.f;
 #pragma unroll
-                    for (int j = 0; j < NN; ++j) s += (float)k.Vinv[o * NN + j] * t1[(w * EPC + el) * NP + nidx(la, j, lb)];
-                    t2[(w * EPC + el) * NP + nidx(la, o, lb)] = s;
+                    for (int j = 0; j < NN; ++j) s += (float)k.Vinv[o * NN + j] * t1[(w * EPC + el) * SP + nidx(la, j, lb)];
+                    t2[(w * EPC + el) * SP + nidx(la, o, lb)] = s;
                 }
             }
         }
@@ -328,7 +332,7 @@ __device__ __forceinline__ void epilogue32(const StageArgs& a, const double* su,
                     float s = 0.f;
 #pragma unroll
                     for (int kk = 0; kk < NN; ++kk)
-                        s += (float)k.Vinv[o * NN + kk] * t2[(w * EPC + el) * NP + nidx(la, lb, kk)];
+                        s += (float)k.Vinv[o * NN + kk] * t2[(w * EPC + el) * SP + nidx(la, lb, kk)];
                     const float e2 = s * s;
                     tot[w] += e2;
                     if (w == 0) {
@@ -507,7 +511,7 @@ struct Smem32 {
     uint64_t* bar;     // TMA completion barrier of the state (initialised once per CTA)
     float* s_alpha;    // [EPC]
     int* s_bad;        // [EPC]
-    const float* s_w;  // learned indicator, transposed layout
+    const float* s_w;  // learned indicator, transposed layout (shared memory, or global through L1)
 };
 
 __device__ __forceinline__ void load_mlp32(const StageArgs& a, float* s_w) {
@@ -522,7 +526,7 @@ __device__ __forceinline__ Smem32 smem32(double* smem, uint64_t* bar, float* s_a
     Smem32 S;
     S.su = smem;
     S.sq = reinterpret_cast<float*>(S.su + V * EPC * NP);
-    S.sR = S.sq + NQ * EPC * NP;
+    S.sR = S.sq + NQ * EPC * SP;
     S.bar = bar;
     S.s_alpha = s_alpha;
     S.s_bad = s_bad;
@@ -616,7 +620,7 @@ __device__ __forceinline__ void tile32(const StageArgs& a, const Smem32& S, int6
         epilogue32(a, su, sq, s_w, el, ab, la, lb, active, e, k);
         return;
     }
-    auto SQ = [&](int q, int elx, int n) -> float& { return sq[(q * EPC + elx) * NP + n]; };
+    auto SQ = [&](int q, int elx, int n) -> float& { return sq[(q * EPC + elx) * SP + n]; };
 
     // per-node primitives of the thread's x-line nodes: recovered in FP64, stored in FP32
     if (active) {
@@ -798,7 +802,7 @@ __device__ __forceinline__ void tile32(const StageArgs& a, const Smem32& S, int6
             for (int i = 0; i < NN; ++i)
 #pragma unroll
                 for (int v = 0; v < V; ++v) {
-                    float& R = sR[(vo[v] * EPC + el) * NP + idx[i]];
+                    float& R = sR[(vo[v] * EPC + el) * SP + idx[i]];
                     R = (d == 0 ? 0.0f : R) + cd * t[i][v];
                 }
         }
@@ -819,7 +823,7 @@ __device__ __forceinline__ void tile32(const StageArgs& a, const Smem32& S, int6
 #pragma unroll
             for (int v = 0; v < V; ++v) {
                 const int s = (v * EPC + el) * NP + n;
-                const double rhs = -(double)sR[s];
+                const double rhs = -(double)sR[(v * EPC + el) * SP + n];
                 const int64_t g = ((int64_t)v * E + e) * NP + n;
                 if (RHS_ONLY) {
                     a.rhs_out[g] = rhs;
@@ -873,10 +877,10 @@ __global__ void __launch_bounds__(NT, 4) k_stage_euler32(StageArgs a) {
     __shared__ uint64_t bar[1];
     __shared__ float s_alpha[EPC];
     __shared__ int s_bad[EPC];
-    __shared__ __align__(16) float s_w[MLP_NT];   // learned indicator, transposed layout
     if (!RHS_ONLY && !a.prep_only && a.ctrl->done) return;
-    load_mlp32(a, s_w);
-    const Smem32 S = smem32(smem, bar, s_alpha, s_bad, s_w);
+    // the learned indicator's weights are read through L1 by the epilogue (a CTA handles one tile:
+    // a shared-memory copy of the 6 KB per CTA would cost more L2 reads than it saves)
+    const Smem32 S = smem32(smem, bar, s_alpha, s_bad, a.mlp32t);
     mbar_init32(bar);
     tile32<BLEND, RHS_ONLY, false>(a, S, (int64_t)blockIdx.x, 0u, 0u);
 }
@@ -932,7 +936,7 @@ __global__ void __launch_bounds__(NT, 4) k_stage_euler32p(StageArgs a, MortarArg
 }
 
 int stage_smem_bytes32() {
-    return V * EPC * NP * (int)sizeof(double) + (NQ + V) * EPC * NP * (int)sizeof(float);
+    return V * EPC * NP * (int)sizeof(double) + (NQ + V) * EPC * SP * (int)sizeof(float);
 }
 
 cudaError_t launch_stage_euler32(const StageArgs& a, bool blend, bool rhs_only, cudaStream_t s) {

@@ -159,3 +159,22 @@ def test_sedov_run_with_adapt_every_8_steps_bit_exact():
     assert np.all(np.isfinite(um))
     assert np.array_equal(s.download(), um)
     assert t == to
+
+
+def test_mhd_adapt_bit_exact():
+    """GLM-MHD (HLLD faces): remap of the 9 variables (admissibility with the magnetic pressure) and
+    the continued run against the oracle."""
+    m = base_forest()
+    u = setups.orszag_tang(m)
+    c = abi.default_cfg(eqn=abi.EQN_MHD, n_vars=9, volume_flux=abi.VOLFLUX_EC_MHD, surface_flux=abi.SURFFLUX_HLLD,
+                        kappa=5 / 3, mu0=1.0, glm_ch=0.7, glm_alpha=0.3, indicator=abi.IND_MODAL)
+    s = Solver(c, m)
+    s.upload(u)
+    s.run(nsteps=2)
+    u1 = s.download()
+    new, remap = s.adapt(flags_for(m))
+    want = orc.remap(u1, remap, kappa=5 / 3, mu0=1.0)
+    assert np.array_equal(s.download(), want)
+    s.run(nsteps=2)
+    uo, _, _, _ = orc.Oracle.for_mesh(c, new).run(want, nsteps=2)
+    assert np.array_equal(s.download(), uo)
