@@ -592,23 +592,6 @@ __device__ __forceinline__ void tile32(const StageArgs& a, const Smem32& S, int6
     }
     const bool load_reg = !RHS_ONLY && !a.prep_only && a.stage > 0;
     tile_issue32(su, a.u_in, load_reg ? a.reg : nullptr, E, e0, nel, S.bar);
-    if (!a.prep_only) {
-        // pull the neighbour traces that lie outside the tile into L1 while the tile streams in
-        const int pel = tid >> 4, pab = tid & 15;
-        if (pel < nel) {
-            const int64_t pe = e0 + pel;
-#pragma unroll
-            for (int f = 0; f < 6; ++f) {
-                const int32_t ne = a.nbr[pe * 6 + f];
-                if (ne >= 0 && (ne < e0 || ne >= e0 + nel)) {
-                    const int nn = line_node(f >> 1, pab & 3, pab >> 2, (f & 1) ? 0 : NN - 1);
-#pragma unroll
-                    for (int v = 0; v < V; ++v)
-                        asm volatile("prefetch.global.L1 [%0];" ::"l"(a.u_in + ((int64_t)v * E + ne) * NP + nn));
-                }
-            }
-        }
-    }
     __syncthreads();   // s_alpha / s_bad visible
     if (!tile_wait32(S.bar, phase, ctrl)) return;
 
