@@ -73,6 +73,10 @@ struct OpConsts {
     double w[NN];            // their weights (adapt: element means)
     double pro[2][NN * NN];  // 2:1 mortar prolongation to the lower/upper half, [s][fine i][coarse j]
     double prj[2][NN * NN];  // 2:1 mortar projection from the lower/upper half, [s][coarse a][fine i]
+    // FP32 copies for the FP32 kernels (rounded once here instead of converted at every use)
+    float S32[NN * NN], winv32[NN], Vinv32[NN * NN];
+    float kappa32, km1_32, ikm1_32, c_enth32, hllc_beta32;
+    float ind_k32, ind_T32, alpha_min32, alpha_max32, one_m_alpha_min32;
 };
 
 __host__ __device__ inline int nidx(int i, int j, int k) { return i + NN * (j + NN * k); }

@@ -554,6 +554,21 @@ int nemo_gpu_init(const nemo_cfg* cfg) {
     std::memcpy(o.w, g.hops.w, sizeof o.w);
     std::memcpy(o.pro, g.hops.pro, sizeof o.pro);
     std::memcpy(o.prj, g.hops.prj, sizeof o.prj);
+    for (int i = 0; i < NN * NN; ++i) {
+        o.S32[i] = (float)o.S[i];
+        o.Vinv32[i] = (float)o.Vinv[i];
+    }
+    for (int i = 0; i < NN; ++i) o.winv32[i] = (float)o.winv[i];
+    o.kappa32 = (float)o.kappa;
+    o.km1_32 = (float)o.km1;
+    o.ikm1_32 = (float)(1.0 / o.km1);
+    o.c_enth32 = (float)o.c_enth;
+    o.hllc_beta32 = (float)o.hllc_beta;
+    o.ind_k32 = (float)o.ind_k;
+    o.ind_T32 = (float)o.ind_T;
+    o.alpha_min32 = (float)o.alpha_min;
+    o.alpha_max32 = (float)o.alpha_max;
+    o.one_m_alpha_min32 = (float)o.one_m_alpha_min;
     CK(cudaStreamCreateWithFlags(&g.stream, cudaStreamNonBlocking));
     CK(setup_stage_euler64(o));
     CK(setup_stage_euler32(o));

@@ -135,9 +135,9 @@ __device__ __forceinline__ void xflux32(const P32& q, float* f) {
 // HLLC/HLLE hybrid (source/equations/euler/riemann/hllc/riemann_mod.f90:7-104) in FP32, on
 // primitives recovered in FP64.
 __device__ __forceinline__ void hllc32(const P32& L, const P32& R, float* F, const OpConsts& k) {
-    const float kappa = (float)k.kappa;
-    const float beta = (float)k.hllc_beta;
-    const float km1 = (float)k.km1;
+    const float kappa = k.kappa32;
+    const float beta = k.hllc_beta32;
+    const float km1 = k.km1_32;
     const float cL = sqrtf(kappa * L.p / L.rho);
     const float cR = sqrtf(kappa * R.p / R.rho);
     const float HL = (L.E + L.p) / L.rho;
@@ -186,7 +186,7 @@ __device__ __forceinline__ void hllc32(const P32& L, const P32& R, float* F, con
 
 // Rusanov (source/equations/euler/riemann/rusanov/riemann_mod.f90:7-24) in FP32.
 __device__ __forceinline__ void rusanov32(const P32& L, const P32& R, float* F, const OpConsts& k) {
-    const float kappa = (float)k.kappa;
+    const float kappa = k.kappa32;
     float FL[5], FR[5];
     xflux32(L, FL);
     xflux32(R, FR);
@@ -306,7 +306,7 @@ __device__ __forceinline__ void epilogue32(const StageArgs& a, const double* su,
 #pragma unroll
                     for (int i = 0; i < NN; ++i) {
                         const float qv = w == 0 ? qr[i] * qp[i] : (w == 1 ? qr[i] : qp[i]);
-                        s += (float)k.Vinv[o * NN + i] * qv;
+                        s += k.Vinv32[o * NN + i] * qv;
                     }
                     t1[(w * EPC + el) * SP + nidx(o, la, lb)] = s;
                 }
@@ -319,7 +319,7 @@ __device__ __forceinline__ void epilogue32(const StageArgs& a, const double* su,
                 for (int o = 0; o < NN; ++o) {
                     float s = 0.f;
 #pragma unroll
-                    for (int j = 0; j < NN; ++j) s += (float)k.Vinv[o * NN + j] * t1[(w * EPC + el) * SP + nidx(la, j, lb)];
+                    for (int j = 0; j < NN; ++j) s += k.Vinv32[o * NN + j] * t1[(w * EPC + el) * SP + nidx(la, j, lb)];
                     t2[(w * EPC + el) * SP + nidx(la, o, lb)] = s;
                 }
             }
@@ -332,7 +332,7 @@ __device__ __forceinline__ void epilogue32(const StageArgs& a, const double* su,
                     float s = 0.f;
 #pragma unroll
                     for (int kk = 0; kk < NN; ++kk)
-                        s += (float)k.Vinv[o * NN + kk] * t2[(w * EPC + el) * SP + nidx(la, lb, kk)];
+                        s += k.Vinv32[o * NN + kk] * t2[(w * EPC + el) * SP + nidx(la, lb, kk)];
                     const float e2 = s * s;
                     tot[w] += e2;
                     if (w == 0) {
@@ -353,10 +353,10 @@ __device__ __forceinline__ void epilogue32(const StageArgs& a, const double* su,
         float am;
         {
             const float energy = fmaxf((t0 - c1) / t0, (c1 - c2) / c1);
-            float al = 1.0f / (1.0f + __expf((float)k.ind_k * (energy - (float)k.ind_T)));
-            if (al < (float)k.alpha_min) al = 0.0f;
-            else if (al > (float)k.one_m_alpha_min) al = 1.0f;
-            am = fminf((float)k.alpha_max, al);
+            float al = 1.0f / (1.0f + __expf(k.ind_k32 * (energy - k.ind_T32)));
+            if (al < k.alpha_min32) al = 0.0f;
+            else if (al > k.one_m_alpha_min32) al = 1.0f;
+            am = fminf(k.alpha_max32, al);
         }
         float alpha = am;
         if (a.feat_out) {
@@ -435,8 +435,8 @@ __device__ __forceinline__ void epilogue32(const StageArgs& a, const double* su,
             }
             const float g0 = uacc.x / (1.0f + __expf(-uacc.x)), g1 = uacc.y / (1.0f + __expf(-uacc.y));
             const float z = hsum16(W3[j0] * g0 + W3[j0 + 1] * g1) + W3[32];
-            float al = (float)k.alpha_max / (1.0f + __expf(-z));
-            if (al < (float)k.alpha_min) al = 0.0f;
+            float al = k.alpha_max32 / (1.0f + __expf(-z));
+            if (al < k.alpha_min32) al = 0.0f;
             if (fb) {
                 alpha = am;
                 if (active && ab == 0) s_fb[el] = 1;
@@ -627,8 +627,8 @@ __device__ __forceinline__ void tile32(const StageArgs& a, const Smem32& S, int6
     }
     __syncthreads();
 
-    const float kappa = (float)k.kappa, ikm1 = (float)(1.0 / k.km1);
-    const float c_enth = (float)k.c_enth;
+    const float kappa = k.kappa32, ikm1 = k.ikm1_32;
+    const float c_enth = k.c_enth32;
     for (int d = 0; d < 3; ++d) {
         if (active) {
             const int c0 = d, c1 = (d + 1) % 3, c2 = (d + 2) % 3;
@@ -739,7 +739,7 @@ __device__ __forceinline__ void tile32(const StageArgs& a, const Smem32& S, int6
                         F[3] = F[0] * velz;
                         F[4] = F[0] * enth;
                     }
-                    const float sim = (float)k.S[i * NN + m], smi = (float)k.S[m * NN + i];
+                    const float sim = k.S32[i * NN + m], smi = k.S32[m * NN + i];
 #pragma unroll
                     for (int v = 0; v < V; ++v) {
                         t[i][v] += sim * F[v];
@@ -748,7 +748,7 @@ __device__ __forceinline__ void tile32(const StageArgs& a, const Smem32& S, int6
                 }
             }
             // ---- lift
-            const float w0 = (float)k.winv[0], w3 = (float)k.winv[NN - 1];
+            const float w0 = k.winv32[0], w3 = k.winv32[NN - 1];
 #pragma unroll
             for (int v = 0; v < V; ++v) {
                 t[0][v] -= w0 * Fs[0][v];
@@ -769,7 +769,7 @@ __device__ __forceinline__ void tile32(const StageArgs& a, const Smem32& S, int6
 #pragma unroll
                             for (int v = 0; v < V; ++v) Fr[v] = Fs[1][v];
                         }
-                        const float wi = (float)k.winv[i];
+                        const float wi = k.winv32[i];
 #pragma unroll
                         for (int v = 0; v < V; ++v) {
                             t[i][v] = (1.0f - al) * t[i][v] + al * (wi * (Fr[v] - Fl[v]));
