@@ -79,6 +79,23 @@ struct OpConsts {
     float ind_k32, ind_T32, alpha_min32, alpha_max32, one_m_alpha_min32;
 };
 
+// Operator matrix entries in the arithmetic type R of a kernel (the FP32 copies for float)
+template <typename R>
+__device__ __forceinline__ R op_S(const OpConsts& k, int i) {
+    if constexpr (sizeof(R) == 4) return k.S32[i];
+    else return k.S[i];
+}
+template <typename R>
+__device__ __forceinline__ R op_winv(const OpConsts& k, int i) {
+    if constexpr (sizeof(R) == 4) return k.winv32[i];
+    else return k.winv[i];
+}
+template <typename R>
+__device__ __forceinline__ R op_Vinv(const OpConsts& k, int i) {
+    if constexpr (sizeof(R) == 4) return k.Vinv32[i];
+    else return k.Vinv[i];
+}
+
 __host__ __device__ inline int nidx(int i, int j, int k) { return i + NN * (j + NN * k); }
 
 // node index of line position i on the line (a,b) of direction d

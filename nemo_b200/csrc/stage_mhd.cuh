@@ -152,7 +152,7 @@ __device__ void epilogue_mhd(const StageArgs& a, const double* su, R* scr, unsig
                 const int ai = n % NN, j = (n / NN) % NN, kk = n / NF;
                 R s = R(0.0);
 #pragma unroll
-                for (int i = 0; i < NN; ++i) s = s + (R)k.Vinv[ai * NN + i] * q[pel * NP + nidx(i, j, kk)];
+                for (int i = 0; i < NN; ++i) s = s + op_Vinv<R>(k, ai * NN + i) * q[pel * NP + nidx(i, j, kk)];
                 t1[pel * NP + n] = s;
             }
             __syncthreads();
@@ -161,7 +161,7 @@ __device__ void epilogue_mhd(const StageArgs& a, const double* su, R* scr, unsig
                 const int ai = n % NN, bj = (n / NN) % NN, kk = n / NF;
                 R s = R(0.0);
 #pragma unroll
-                for (int j = 0; j < NN; ++j) s = s + (R)k.Vinv[bj * NN + j] * t1[pel * NP + nidx(ai, j, kk)];
+                for (int j = 0; j < NN; ++j) s = s + op_Vinv<R>(k, bj * NN + j) * t1[pel * NP + nidx(ai, j, kk)];
                 t2[pel * NP + n] = s;
             }
             __syncthreads();
@@ -170,7 +170,7 @@ __device__ void epilogue_mhd(const StageArgs& a, const double* su, R* scr, unsig
                 const int ai = n % NN, bj = (n / NN) % NN, cc = n / NF;
                 R s = R(0.0);
 #pragma unroll
-                for (int kk = 0; kk < NN; ++kk) s = s + (R)k.Vinv[cc * NN + kk] * t2[pel * NP + nidx(ai, bj, kk)];
+                for (int kk = 0; kk < NN; ++kk) s = s + op_Vinv<R>(k, cc * NN + kk) * t2[pel * NP + nidx(ai, bj, kk)];
                 cm[pel * NP + n] = s;
             }
             __syncthreads();
@@ -509,7 +509,7 @@ __global__ void __launch_bounds__(mhd::NT, sizeof(R) == 4 ? 4 : 1) k_stage_mhd(S
                     else m_ec_x(ui, um, F, kap, mu0, ch);
                     m_nc_x(ui, ui, um, Gi, mu0);
                     m_nc_x(um, ui, um, Gm, mu0);
-                    const R sim = (R)k.S[i * NN + m], smi = (R)k.S[m * NN + i];
+                    const R sim = op_S<R>(k, i * NN + m), smi = op_S<R>(k, m * NN + i);
 #pragma unroll
                     for (int v = 0; v < MV; ++v) {
                         t[i][v] = t[i][v] + sim * (F[v] + Gi[v]);
@@ -519,8 +519,8 @@ __global__ void __launch_bounds__(mhd::NT, sizeof(R) == 4 ? 4 : 1) k_stage_mhd(S
             // ---- lift
 #pragma unroll
             for (int v = 0; v < MV; ++v) {
-                t[0][v] = t[0][v] + (R)k.winv[0] * (-Fs[0][v]);
-                t[NN - 1][v] = t[NN - 1][v] + (R)k.winv[NN - 1] * Fs[1][v];
+                t[0][v] = t[0][v] + op_winv<R>(k, 0) * (-Fs[0][v]);
+                t[NN - 1][v] = t[NN - 1][v] + op_winv<R>(k, NN - 1) * Fs[1][v];
             }
             // ---- FV subcells and blend
             if (BLEND) {
@@ -552,7 +552,7 @@ __global__ void __launch_bounds__(mhd::NT, sizeof(R) == 4 ? 4 : 1) k_stage_mhd(S
 #pragma unroll
                             for (int v = 0; v < MV; ++v) FR[v] = Fs[1][v];
                         }
-                        const R wi = (R)k.winv[i];
+                        const R wi = op_winv<R>(k, i);
 #pragma unroll
                         for (int v = 0; v < MV; ++v) t[i][v] = (R(1.0) - al) * t[i][v] + al * (wi * (FR[v] - FL[v]));
                     }
