@@ -400,10 +400,14 @@ __device__ void epilogue_mhd(const StageArgs& a, const double* su, R* scr, unsig
 
 }  // namespace mhd
 
-// FP32 form: 4 CTAs per SM (128 registers; the spills cost less than the lost occupancy would);
-// plain FP64: 1 CTA per SM with the full register file.
+// FP32 form: 3 CTAs per SM (168 registers, a few hundred bytes of spills; 2 % faster on B200 than
+// 4 CTAs at 128 registers with twice the spills, and 2 CTAs without spills is 14 % slower);
+// plain FP64: 1 CTA per SM with the full register file.  The conserved state is read per node pair
+// from the FP64 tile: a shared-memory array of per-node FP32 primitives (20 KB more per CTA) made the
+// pair fluxes cheaper but the stage 4 % slower, as the larger carveout left L1 too small for the
+// neighbour traces and register rows.
 template <typename R, bool BLEND, bool RHS_ONLY>
-__global__ void __launch_bounds__(mhd::NT, sizeof(R) == 4 ? 4 : 1) k_stage_mhd(StageArgs a) {
+__global__ void __launch_bounds__(mhd::NT, sizeof(R) == 4 ? 3 : 1) k_stage_mhd(StageArgs a) {
     constexpr int MEPC = mhd::EPC, MV = mhd::V;
     using mhd::load_rot;
     using mhd::load_rot_global;
