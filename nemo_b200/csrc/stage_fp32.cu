@@ -811,7 +811,8 @@ __device__ __forceinline__ void tile32(const StageArgs& a, const Smem32& S, int6
                 if (RHS_ONLY) {
                     a.rhs_out[g] = rhs;
                 } else {
-                    const double r2 = st == 0 ? rhs : A * a.reg[g] + rhs;
+                    // L2 only (prefetched there at the tile start): L1 stays for the neighbour traces
+                    const double r2 = st == 0 ? rhs : A * __ldcg(a.reg + g) + rhs;
                     a.reg[g] = r2;
                     su[s] = su[s] + cdt * r2;
                 }
@@ -960,10 +961,13 @@ cudaError_t setup_stage_euler32(const OpConsts& ops) {
     cudaError_t err;
     if ((err = set_attrs32(k_stage_euler32p<true>, smem)) != cudaSuccess) return err;
     if ((err = set_attrs32(k_stage_euler32p<false>, smem)) != cudaSuccess) return err;
-    if ((err = set_attrs32(k_stage_euler32<true, true>, smem)) != cudaSuccess) return err;
-    if ((err = set_attrs32(k_stage_euler32<false, true>, smem)) != cudaSuccess) return err;
-    if ((err = set_attrs32(k_stage_euler32<true, false>, smem)) != cudaSuccess) return err;
-    if ((err = set_attrs32(k_stage_euler32<false, false>, smem)) != cudaSuccess) return err;
+    // the grid-schedule kernels leave the shared-memory carveout to the driver: it keeps 4 CTAs per
+    // SM and more L1 than the largest carveout would (1 % faster per stage on B200)
+    const auto dyn = cudaFuncAttributeMaxDynamicSharedMemorySize;
+    if ((err = cudaFuncSetAttribute(k_stage_euler32<true, true>, dyn, smem)) != cudaSuccess) return err;
+    if ((err = cudaFuncSetAttribute(k_stage_euler32<false, true>, dyn, smem)) != cudaSuccess) return err;
+    if ((err = cudaFuncSetAttribute(k_stage_euler32<true, false>, dyn, smem)) != cudaSuccess) return err;
+    if ((err = cudaFuncSetAttribute(k_stage_euler32<false, false>, dyn, smem)) != cudaSuccess) return err;
     return cudaMemcpyToSymbol(c_ops32, &ops, sizeof(OpConsts));
 }
 

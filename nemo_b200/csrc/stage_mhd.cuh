@@ -595,7 +595,9 @@ __global__ void __launch_bounds__(mhd::NT, sizeof(R) == 4 ? 3 : 1) k_stage_mhd(S
                 if (RHS_ONLY) {
                     a.rhs_out[g] = rhs;
                 } else {
-                    const double r2 = st == 0 ? rhs : A * a.reg[g] + rhs;
+                    // FP32 form: the register row from L2 only (0.7 % faster; the FP64 form is not)
+                    const double rg = st == 0 ? 0.0 : (sizeof(R) == 4 ? __ldcg(a.reg + g) : a.reg[g]);
+                    const double r2 = st == 0 ? rhs : A * rg + rhs;
                     a.reg[g] = r2;
                     su[s] = su[s] + cdt * r2;
                 }
