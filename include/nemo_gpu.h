@@ -168,6 +168,15 @@ int nemo_gpu_adapt(int64_t nelems, const double* delta, const double* center, in
 int nemo_gpu_amr_flags(double refine_threshold, double coarsen_threshold, int32_t* flags);
 int nemo_gpu_pack_elements(const int32_t* idx_dev, int64_t n, double* buf_dev);
 int nemo_gpu_unpack_elements(const int32_t* idx_dev, int64_t n, const double* buf_dev);
+/* The face form of the ghost refresh (the reference sends whole payloads; only the traces on the
+   faces that a process's own elements or mortars touch, and the raw blending coefficient, are
+   read from a ghost): for each listed (element idx_dev[i], face face_dev[i]) buf_dev holds a row of
+   n_vars*16 + 1 doubles, the 16 face nodes of every variable (j = a + 4 b over the face's two
+   tangential directions in increasing order) and then the element's raw blending coefficient.
+   Entries outside [0, nelems) x [0, 6) are skipped.  Device pointers; both calls return after the
+   copy has completed. */
+int nemo_gpu_pack_faces(const int32_t* idx_dev, const int32_t* face_dev, int64_t n, double* buf_dev);
+int nemo_gpu_unpack_faces(const int32_t* idx_dev, const int32_t* face_dev, int64_t n, const double* buf_dev);
 
 /* Copy the conserved state host->device.  host points at the first element's state(1,1,1,1);
    consecutive elements are elem_stride_bytes apart (sizeof(quad_t) when the state sits in the

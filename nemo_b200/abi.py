@@ -31,6 +31,7 @@ EXPORTS = [
     "nemo_gpu_autotune", "nemo_gpu_set_schedule", "nemo_gpu_set_owned", "nemo_gpu_pack_elements",
     "nemo_gpu_unpack_elements", "nemo_gpu_adapt", "nemo_gpu_amr_flags",
     "nemo_gpu_checkpoint_begin", "nemo_gpu_checkpoint_wait", "nemo_gpu_set_time",
+    "nemo_gpu_pack_faces", "nemo_gpu_unpack_faces",
 ]
 
 
@@ -108,6 +109,8 @@ def load(path=LIB_PATH):
         "nemo_gpu_checkpoint_begin": [vp, i64, vp],
         "nemo_gpu_checkpoint_wait": [ctypes.POINTER(dbl), ctypes.POINTER(i64)],
         "nemo_gpu_set_time": [dbl, i64],
+        "nemo_gpu_pack_faces": [vp, vp, i64, vp],
+        "nemo_gpu_unpack_faces": [vp, vp, i64, vp],
     }
     for name, args in sig.items():
         f = getattr(L, name)

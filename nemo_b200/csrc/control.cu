@@ -101,7 +101,52 @@ __global__ void k_unpack(double* __restrict__ u, double* __restrict__ alpha, con
     else if (alpha) alpha[e] = buf[i];
 }
 
+// face exchange buffers: per listed (element, face) the V x 16 trace values of that face (node order
+// of line_node) and the element's raw indicator; entries outside [0, E) x [0, 6) are skipped
+__device__ __forceinline__ int face_node(int f, int j) { return line_node(f >> 1, j & 3, j >> 2, (f & 1) ? NN - 1 : 0); }
+
+__global__ void k_pack_faces(const double* __restrict__ u, const double* __restrict__ alpha,
+                             const int32_t* __restrict__ idx, const int32_t* __restrict__ face, int64_t n, int64_t E,
+                             int nv, double* __restrict__ buf) {
+    const int64_t row = (int64_t)nv * NF + 1;
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n * row) return;
+    const int64_t m = i / row, r = i % row;
+    const int64_t e = idx[m];
+    const int f = face[m];
+    if (e < 0 || e >= E || f < 0 || f > 5) return;
+    buf[i] = r < (int64_t)nv * NF ? u[((r / NF) * E + e) * NP + face_node(f, (int)(r % NF))] : (alpha ? alpha[e] : 0.0);
+}
+
+__global__ void k_unpack_faces(double* __restrict__ u, double* __restrict__ alpha, const int32_t* __restrict__ idx,
+                               const int32_t* __restrict__ face, int64_t n, int64_t E, int nv,
+                               const double* __restrict__ buf) {
+    const int64_t row = (int64_t)nv * NF + 1;
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n * row) return;
+    const int64_t m = i / row, r = i % row;
+    const int64_t e = idx[m];
+    const int f = face[m];
+    if (e < 0 || e >= E || f < 0 || f > 5) return;
+    if (r < (int64_t)nv * NF) u[((r / NF) * E + e) * NP + face_node(f, (int)(r % NF))] = buf[i];
+    else if (alpha) alpha[e] = buf[i];
+}
+
 }  // namespace
+
+cudaError_t launch_pack_faces(const double* u, const double* alpha, const int32_t* idx, const int32_t* face, int64_t n,
+                              int64_t E, int nv, double* buf, cudaStream_t s) {
+    const int64_t total = n * ((int64_t)nv * NF + 1);
+    if (total > 0) k_pack_faces<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(u, alpha, idx, face, n, E, nv, buf);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_unpack_faces(double* u, double* alpha, const int32_t* idx, const int32_t* face, int64_t n, int64_t E,
+                                int nv, const double* buf, cudaStream_t s) {
+    const int64_t total = n * ((int64_t)nv * NF + 1);
+    if (total > 0) k_unpack_faces<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(u, alpha, idx, face, n, E, nv, buf);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_pack(const double* u, const double* alpha, const int32_t* idx, int64_t n, int64_t E, int nv,
                         double* buf, cudaStream_t s) {

@@ -94,6 +94,10 @@ cudaError_t mlp_forward_launch(const float* feat, int64_t n, const float* W, flo
 
 // control kernels (control.cu)
 // element exchange (partitioned runs): buf[m] = (state of element idx[m], V x 64, then its raw alpha)
+cudaError_t launch_pack_faces(const double* u, const double* alpha, const int32_t* idx, const int32_t* face, int64_t n,
+                              int64_t E, int nv, double* buf, cudaStream_t s);
+cudaError_t launch_unpack_faces(double* u, double* alpha, const int32_t* idx, const int32_t* face, int64_t n, int64_t E,
+                                int nv, const double* buf, cudaStream_t s);
 cudaError_t launch_pack(const double* u, const double* alpha, const int32_t* idx, int64_t n, int64_t E, int nv,
                         double* buf, cudaStream_t s);
 cudaError_t launch_unpack(double* u, double* alpha, const int32_t* idx, int64_t n, int64_t E, int nv,

@@ -791,6 +791,28 @@ int nemo_gpu_unpack_elements(const int32_t* idx_dev, int64_t n, const double* bu
     return NEMO_OK;
 }
 
+int nemo_gpu_pack_faces(const int32_t* idx_dev, const int32_t* face_dev, int64_t n, double* buf_dev) {
+    int st = ensure_ready();
+    if (st) return st;
+    if (n < 0 || (n > 0 && (!idx_dev || !face_dev || !buf_dev))) return fail(NEMO_ERR_ARG, "bad pack arguments");
+    if ((st = prepare_if_needed())) return st;
+    CK(launch_pack_faces(g.u[g.cur], blended() ? g.alpha[g.cur] : nullptr, idx_dev, face_dev, n, g.E, g.V, buf_dev,
+                         g.stream));
+    CK(cudaStreamSynchronize(g.stream));
+    return NEMO_OK;
+}
+
+int nemo_gpu_unpack_faces(const int32_t* idx_dev, const int32_t* face_dev, int64_t n, const double* buf_dev) {
+    int st = ensure_ready();
+    if (st) return st;
+    if (n < 0 || (n > 0 && (!idx_dev || !face_dev || !buf_dev))) return fail(NEMO_ERR_ARG, "bad unpack arguments");
+    if ((st = prepare_if_needed())) return st;
+    CK(launch_unpack_faces(g.u[g.cur], blended() ? g.alpha[g.cur] : nullptr, idx_dev, face_dev, n, g.E, g.V, buf_dev,
+                           g.stream));
+    CK(cudaStreamSynchronize(g.stream));
+    return NEMO_OK;
+}
+
 int nemo_gpu_set_groups(int32_t ngroups, const int32_t* group_of_elem) {
     if (!g.has_mesh) return fail(NEMO_ERR_STATE, "set the mesh first");
     if (ngroups < 1 || ngroups > MAX_GROUPS) return fail(NEMO_ERR_ARG, "ngroups must be in [1, %d]", MAX_GROUPS);

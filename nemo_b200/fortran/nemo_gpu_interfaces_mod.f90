@@ -171,6 +171,42 @@ interface
         integer(c_int64_t), value :: steps
         integer(c_int) :: st
     end function
+
+    !! Element partition over MPI ranks: owned quads first, then ghosts; ghost refresh before every
+    !! stage around the host's own exchange (mesh_exchange).  idx/face/buf are device pointers.
+    function nemo_gpu_set_owned(n_owned) result(st) bind(c, name="nemo_gpu_set_owned")
+        import :: c_int, c_int64_t
+        integer(c_int64_t), value :: n_owned
+        integer(c_int) :: st
+    end function
+
+    function nemo_gpu_pack_faces(idx_dev, face_dev, n, buf_dev) result(st) bind(c, name="nemo_gpu_pack_faces")
+        import :: c_int, c_int64_t, c_ptr
+        type(c_ptr), value :: idx_dev, face_dev, buf_dev
+        integer(c_int64_t), value :: n
+        integer(c_int) :: st
+    end function
+
+    function nemo_gpu_unpack_faces(idx_dev, face_dev, n, buf_dev) result(st) bind(c, name="nemo_gpu_unpack_faces")
+        import :: c_int, c_int64_t, c_ptr
+        type(c_ptr), value :: idx_dev, face_dev, buf_dev
+        integer(c_int64_t), value :: n
+        integer(c_int) :: st
+    end function
+
+    function nemo_gpu_pack_elements(idx_dev, n, buf_dev) result(st) bind(c, name="nemo_gpu_pack_elements")
+        import :: c_int, c_int64_t, c_ptr
+        type(c_ptr), value :: idx_dev, buf_dev
+        integer(c_int64_t), value :: n
+        integer(c_int) :: st
+    end function
+
+    function nemo_gpu_unpack_elements(idx_dev, n, buf_dev) result(st) bind(c, name="nemo_gpu_unpack_elements")
+        import :: c_int, c_int64_t, c_ptr
+        type(c_ptr), value :: idx_dev, buf_dev
+        integer(c_int64_t), value :: n
+        integer(c_int) :: st
+    end function
 end interface
 
 contains

@@ -13,7 +13,12 @@ its own state and its neighbours' traces, so every owned element evolves exactly
 run.
 
 One exchange per stage, point to point (torch.distributed isend/irecv: NCCL with device buffers on
-GPUs, gloo with host buffers on CPUs), and one minimum reduction of the time step per step.
+GPUs, gloo with host buffers on CPUs), and one minimum reduction of the time step per step.  A
+ghost is only read through the traces on the faces that the rank's sides touch (its conforming
+neighbours' faces and the mortars it belongs to) and through its raw blending coefficient, so the
+exchange moves those faces: one row of V x 16 trace values + the coefficient per (ghost, face),
+a quarter of the element's payload for a ghost with one shared face (the reference exchanges
+whole payloads).  The whole-element form is kept beside it.
 """
 from dataclasses import dataclass, field
 
@@ -32,6 +37,9 @@ class Part:
     glob: np.ndarray                                  # [E_local] global element ids
     send: dict = field(default_factory=dict)          # peer -> local owned indices to send
     recv: dict = field(default_factory=dict)          # peer -> local ghost indices to fill
+    send_f: dict = field(default_factory=dict)        # peer -> (local owned indices, face ids) to send
+    recv_f: dict = field(default_factory=dict)        # peer -> (local ghost indices, face ids) to fill
+    ghost_faces: list = field(default_factory=list)   # (global element, face) read from ghosts
 
 
 def owner_ranges(E, nranks):
@@ -89,7 +97,10 @@ def partition(mesh, nranks):
         gl = glob
         local = Mesh(mesh.delta[gl], mesh.center[gl], np.stack(Q), np.stack(F), np.stack(NQ),
                      np.asarray(B, dtype=np.int32), level=mesh.level[gl])
-        parts.append(Part(rank=r, mesh=local, n_owned=hi - lo, glob=glob))
+        part = Part(rank=r, mesh=local, n_owned=hi - lo, glob=glob)
+        # ghost faces on the included sides: the traces this rank reads from other ranks' elements
+        part.ghost_faces = sorted((int(glob[i]), f) for i, f in covered if i >= hi - lo)
+        parts.append(part)
     # exchange plan: rank r receives its ghosts owned by p; p sends them in the same (global) order
     for r, pr in enumerate(parts):
         ghosts = pr.glob[pr.n_owned:]
@@ -100,18 +111,32 @@ def partition(mesh, nranks):
             pr.recv[p] = (pr.n_owned + sel).astype(np.int32)
             lo_p = ranges[p][0]
             parts[p].send[r] = (ghosts[sel] - lo_p).astype(np.int32)
+    # face plan: rank r receives its ghost faces owned by p; p sends them in the same (global) order
+    for r, pr in enumerate(parts):
+        loc = {int(g): i for i, g in enumerate(pr.glob)}
+        for p in range(nranks):
+            ent = [(g, f) for g, f in pr.ghost_faces if owner[g] == p]
+            if not ent:
+                continue
+            gids = np.array([g for g, _ in ent], dtype=np.int64)
+            fids = np.array([f for _, f in ent], dtype=np.int32)
+            pr.recv_f[p] = (np.array([loc[int(g)] for g in gids], dtype=np.int32), fids)
+            parts[p].send_f[r] = ((gids - ranges[p][0]).astype(np.int32), fids.copy())
     return parts
 
 
-def exchange(part, dist, get_rows, set_rows, make_buffer):
-    """One ghost refresh: get_rows(idx) -> buffer of those local elements, set_rows(idx, buffer);
-    make_buffer(n) -> an empty receive buffer for n elements.  Sends and receives are posted
-    together (batch_isend_irecv) so no ordering between peers is needed."""
+def exchange(part, dist, get_rows, set_rows, make_buffer, faces=False):
+    """One ghost refresh: get_rows(entries) -> buffer of those local entries, set_rows(entries,
+    buffer); make_buffer(n) -> an empty receive buffer for n entries.  Entries are element index
+    arrays, or (element, face) array pairs with faces=True.  Sends and receives are posted together
+    (batch_isend_irecv) so no ordering between peers is needed."""
     ops, incoming = [], []
-    for peer, idx in sorted(part.send.items()):
+    send, recv = (part.send_f, part.recv_f) if faces else (part.send, part.recv)
+    count = (lambda ent: len(ent[0])) if faces else len
+    for peer, idx in sorted(send.items()):
         ops.append(dist.P2POp(dist.isend, get_rows(idx), peer))
-    for peer, idx in sorted(part.recv.items()):
-        buf = make_buffer(len(idx))
+    for peer, idx in sorted(recv.items()):
+        buf = make_buffer(count(idx))
         incoming.append((idx, buf))
         ops.append(dist.P2POp(dist.irecv, buf, peer))
     if ops:
@@ -123,10 +148,11 @@ def exchange(part, dist, get_rows, set_rows, make_buffer):
 
 class PartitionedRun:
     """Advance one rank's share on its GPU: ghosts refreshed before every stage through the library's
-    pack/unpack entry points, Δt = all-reduce minimum of the ranks' CFL bounds.  Euler only (the GLM
-    cleaning speed of MHD would need its own all-reduce of λmax and vmax)."""
+    pack/unpack entry points (the ghost faces by default, whole elements with faces=False),
+    Δt = all-reduce minimum of the ranks' CFL bounds.  Euler only (the GLM cleaning speed of MHD
+    would need its own all-reduce of λmax and vmax)."""
 
-    def __init__(self, cfg, part, dist, host_buffers=None):
+    def __init__(self, cfg, part, dist, host_buffers=None, faces=True):
         import torch
         from . import abi
         from .solver import Solver
@@ -136,32 +162,47 @@ class PartitionedRun:
             raise ValueError("n_vars must be 5")
         self.torch, self.abi, self.dist, self.part = torch, abi, dist, part
         self.cfg = cfg
+        self.faces = faces
         self.s = Solver(cfg, part.mesh)
         abi.call("nemo_gpu_set_owned", int(part.n_owned))
-        self.row = cfg.n_vars * 64 + 1
+        self.row = cfg.n_vars * (16 if faces else 64) + 1
         # gloo moves host tensors, NCCL device tensors
         self.host = (dist.get_backend() != "nccl") if host_buffers is None else host_buffers
         dev = torch.device("cuda", torch.cuda.current_device())
-        self.idx_dev = {}
-        for d in (part.send, part.recv):
-            for peer, idx in d.items():
-                self.idx_dev[id(idx)] = torch.as_tensor(idx, dtype=torch.int32, device=dev)
         self.dev = dev
+        self.idx_dev = {}
+        plans = (part.send_f, part.recv_f) if faces else (part.send, part.recv)
+        for d in plans:
+            for peer, ent in d.items():
+                if faces:
+                    self.idx_dev[id(ent)] = (torch.as_tensor(ent[0], dtype=torch.int32, device=dev),
+                                             torch.as_tensor(ent[1], dtype=torch.int32, device=dev))
+                else:
+                    self.idx_dev[id(ent)] = torch.as_tensor(ent, dtype=torch.int32, device=dev)
+        self.bytes_per_exchange = sum(
+            (len(e[0]) if faces else len(e)) for e in plans[0].values()) * self.row * 8
 
-    def _get(self, idx):
-        t = self.torch
-        i = self.idx_dev[id(idx)]
-        buf = t.empty((len(idx), self.row), dtype=t.float64, device=self.dev)
-        self.abi.call("nemo_gpu_pack_elements", self.abi.ctypes.c_void_p(i.data_ptr()), len(idx),
-                      self.abi.ctypes.c_void_p(buf.data_ptr()))
+    def _get(self, ent):
+        t, vp = self.torch, self.abi.ctypes.c_void_p
+        n = len(ent[0]) if self.faces else len(ent)
+        buf = t.empty((n, self.row), dtype=t.float64, device=self.dev)
+        if self.faces:
+            i, f = self.idx_dev[id(ent)]
+            self.abi.call("nemo_gpu_pack_faces", vp(i.data_ptr()), vp(f.data_ptr()), n, vp(buf.data_ptr()))
+        else:
+            i = self.idx_dev[id(ent)]
+            self.abi.call("nemo_gpu_pack_elements", vp(i.data_ptr()), n, vp(buf.data_ptr()))
         return buf.cpu() if self.host else buf
 
-    def _set(self, idx, buf):
-        i = self.idx_dev[id(idx)]
-        b = buf.to(self.dev) if self.host else buf
-        b = b.contiguous()
-        self.abi.call("nemo_gpu_unpack_elements", self.abi.ctypes.c_void_p(i.data_ptr()), len(idx),
-                      self.abi.ctypes.c_void_p(b.data_ptr()))
+    def _set(self, ent, buf):
+        vp = self.abi.ctypes.c_void_p
+        b = (buf.to(self.dev) if self.host else buf).contiguous()
+        if self.faces:
+            i, f = self.idx_dev[id(ent)]
+            self.abi.call("nemo_gpu_unpack_faces", vp(i.data_ptr()), vp(f.data_ptr()), len(ent[0]), vp(b.data_ptr()))
+        else:
+            i = self.idx_dev[id(ent)]
+            self.abi.call("nemo_gpu_unpack_elements", vp(i.data_ptr()), len(ent), vp(b.data_ptr()))
 
     def _buf(self, n):
         t = self.torch
@@ -171,7 +212,7 @@ class PartitionedRun:
         self.s.upload(u_local)
 
     def exchange(self):
-        exchange(self.part, self.dist, self._get, self._set, self._buf)
+        exchange(self.part, self.dist, self._get, self._set, self._buf, faces=self.faces)
 
     def step(self):
         t = self.torch

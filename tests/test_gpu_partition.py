@@ -35,7 +35,7 @@ def _port():
     return p
 
 
-def _worker(rank, world, port, out_dir, nsteps, precision):
+def _worker(rank, world, port, out_dir, nsteps, precision, faces):
     import torch
     import torch.distributed as dist
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
@@ -46,7 +46,7 @@ def _worker(rank, world, port, out_dir, nsteps, precision):
         u = blast_state(m)
         part = partition.partition(m, world)[rank]
         cfg = abi.default_cfg(indicator=abi.IND_MODAL, positivity=1, precision=precision)
-        run = partition.PartitionedRun(cfg, part, dist)
+        run = partition.PartitionedRun(cfg, part, dist, faces=faces)
         run.upload(np.ascontiguousarray(u[:, part.glob]))
         run.run(nsteps)
         np.save(os.path.join(out_dir, f"rank{rank}.npy"), run.download_owned())
@@ -55,11 +55,12 @@ def _worker(rank, world, port, out_dir, nsteps, precision):
         dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("precision", [abi.PREC_FP64, abi.PREC_FP32])
-def test_two_process_partition_matches_oracle(precision, tmp_path):
+@pytest.mark.parametrize("precision,faces", [(abi.PREC_FP64, True), (abi.PREC_FP64, False), (abi.PREC_FP32, True)])
+def test_two_process_partition_matches_oracle(precision, faces, tmp_path):
+    """Ghost refresh by faces (the default) or whole elements."""
     import torch.multiprocessing as tmp
     nsteps = 3
-    tmp.spawn(_worker, args=(2, _port(), str(tmp_path), nsteps, precision), nprocs=2, join=True)
+    tmp.spawn(_worker, args=(2, _port(), str(tmp_path), nsteps, precision, faces), nprocs=2, join=True)
     got = np.concatenate([np.load(tmp_path / f"rank{r}.npy") for r in range(2)], axis=1)
     m = band_forest()
     u = blast_state(m)

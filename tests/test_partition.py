@@ -116,3 +116,90 @@ def test_partitioned_oracle_run_matches_single_process(world, tmp_path):
     ref, _, n, _ = orc.Oracle.for_mesh(c, m).run(u, nsteps=nsteps)
     assert n == nsteps
     assert np.array_equal(got, ref)
+
+
+def _face_nodes(f):
+    """Node indices of face f (the library's face order: j = a + 4 b over the tangential axes)."""
+    d, end = f >> 1, (3 if f & 1 else 0)
+    out = []
+    for j in range(16):
+        a, b = j & 3, j >> 2
+        out.append([end + 4 * a + 16 * b, a + 4 * end + 16 * b, a + 4 * b + 16 * end][d])
+    return np.array(out)
+
+
+@pytest.mark.parametrize("nranks", [2, 3])
+def test_face_plan(nranks):
+    """Every trace a rank reads from a ghost is in its face plan, sender and receiver list the same
+    (global element, face) in the same order, and the plan moves far less than whole elements."""
+    m = band_forest()
+    parts = partition.partition(m, nranks)
+    for p in parts:
+        lnbr = p.mesh.neighbors()
+        need = set()
+        for e in range(p.n_owned):               # conforming neighbours of owned elements
+            for f in range(6):
+                n = lnbr[e, f]
+                if n >= p.n_owned:
+                    need.add((int(p.glob[n]), f ^ 1))
+        for row in p.mesh.mortars():            # every quad of a local mortar
+            qc, fc = int(row[0]), int(row[1])
+            if qc >= p.n_owned:
+                need.add((int(p.glob[qc]), fc))
+            for q in row[2:]:
+                if q >= p.n_owned:
+                    need.add((int(p.glob[q]), fc ^ 1))
+        got = {(int(p.glob[i]), int(f)) for idx, fs in p.recv_f.values() for i, f in zip(idx, fs)}
+        assert need <= got
+        for peer, (idx, fs) in p.send_f.items():
+            ridx, rfs = parts[peer].recv_f[p.rank]
+            assert np.array_equal(p.glob[idx], parts[peer].glob[ridx]) and np.array_equal(fs, rfs)
+            assert np.all(idx < p.n_owned)
+        nf = sum(len(v[0]) for v in p.send_f.values())
+        ne = sum(len(v) for v in p.send.values())
+        assert nf * (5 * 16 + 1) < 0.35 * ne * (5 * 64 + 1)
+
+
+def _face_worker(rank, world, port, out_dir):
+    import torch
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        m = band_forest()
+        u = blast_state(m)
+        alpha = np.linspace(0.0, 0.5, m.E)
+        part = partition.partition(m, world)[rank]
+        ul = np.zeros((u.shape[0], len(part.glob), 64))
+        ul[:, : part.n_owned] = u[:, part.glob[: part.n_owned]]
+        al = np.zeros(len(part.glob))
+        al[: part.n_owned] = alpha[part.glob[: part.n_owned]]
+        V = u.shape[0]
+
+        def get_rows(ent):
+            idx, fs = ent
+            rows = [np.concatenate([ul[:, i][:, _face_nodes(f)].ravel(), [al[i]]]) for i, f in zip(idx, fs)]
+            return torch.from_numpy(np.array(rows))
+
+        def set_rows(ent, buf):
+            b = buf.numpy()
+            for k, (i, f) in enumerate(zip(*ent)):
+                ul[:, i, _face_nodes(f)] = b[k, : V * 16].reshape(V, 16)
+                al[i] = b[k, -1]
+
+        partition.exchange(part, dist, get_rows, set_rows,
+                           lambda n: torch.empty((n, V * 16 + 1), dtype=torch.float64), faces=True)
+        ok = True
+        for idx, fs in part.recv_f.values():
+            for i, f in zip(idx, fs):
+                g = part.glob[i]
+                ok = ok and np.array_equal(ul[:, i, _face_nodes(f)], u[:, g, _face_nodes(f)]) and al[i] == alpha[g]
+        np.save(os.path.join(out_dir, f"ok{rank}.npy"), np.array([ok]))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_face_exchange_gloo(tmp_path):
+    import torch.multiprocessing as tmp
+    tmp.spawn(_face_worker, args=(3, _free_port(), str(tmp_path)), nprocs=3, join=True)
+    assert all(bool(np.load(tmp_path / f"ok{r}.npy")[0]) for r in range(3))
