@@ -994,7 +994,7 @@ cudaError_t setup_stage_euler32(const OpConsts& ops) {
 namespace nemo {
 #undef NEMO_MHD_OPS
 
-int stage_smem_bytes_mhd32() { return mhd::V * mhd::EPC * NP * (int)(sizeof(double) + sizeof(float)); }
+int stage_smem_bytes_mhd32() { return mhd::V * mhd::EPC * (NP * (int)sizeof(double) + mhd::SPM * (int)sizeof(float)); }
 
 cudaError_t setup_stage_mhd32() {
     const int smem = stage_smem_bytes_mhd32();

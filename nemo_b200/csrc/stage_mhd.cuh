@@ -25,6 +25,9 @@ namespace mhd {
 constexpr int EPC = 8;
 constexpr int NT = 128;
 constexpr int V = 9;
+// element stride of the rhs array: 6 words of padding move the two elements of a warp onto
+// different banks (as in the Euler FP32 stage; 0.7 % faster per FP32 stage at 64^3)
+constexpr int SPM = NP + 6;
 
 __device__ __forceinline__ unsigned su32(const void* p) { return static_cast<unsigned>(__cvta_generic_to_shared(p)); }
 
@@ -83,15 +86,17 @@ __device__ __forceinline__ void load_rot(const double* su, int el, int n, int d,
     }
 }
 
+// an out-of-tile neighbour's trace node, rotated into the frame of direction d (L2 only: each node
+// is read once per CTA, so L1 is kept for the register rows)
 template <typename R>
 __device__ __forceinline__ void load_rot_global(const double* __restrict__ g, int64_t E, int64_t ne, int n, int d, R* r) {
-    r[0] = (R)__ldg(g + ((int64_t)0 * E + ne) * NP + n);
-    r[4] = (R)__ldg(g + ((int64_t)4 * E + ne) * NP + n);
-    r[8] = (R)__ldg(g + ((int64_t)8 * E + ne) * NP + n);
+    r[0] = (R)__ldcg(g + ((int64_t)0 * E + ne) * NP + n);
+    r[4] = (R)__ldcg(g + ((int64_t)4 * E + ne) * NP + n);
+    r[8] = (R)__ldcg(g + ((int64_t)8 * E + ne) * NP + n);
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-        r[1 + c] = (R)__ldg(g + ((int64_t)(1 + (d + c) % 3) * E + ne) * NP + n);
-        r[5 + c] = (R)__ldg(g + ((int64_t)(5 + (d + c) % 3) * E + ne) * NP + n);
+        r[1 + c] = (R)__ldcg(g + ((int64_t)(1 + (d + c) % 3) * E + ne) * NP + n);
+        r[5 + c] = (R)__ldcg(g + ((int64_t)(5 + (d + c) % 3) * E + ne) * NP + n);
     }
 }
 
@@ -568,7 +573,7 @@ __global__ void __launch_bounds__(mhd::NT, sizeof(R) == 4 ? 3 : 1) k_stage_mhd(S
             for (int i = 0; i < NN; ++i)
 #pragma unroll
                 for (int c = 0; c < MV; ++c) {
-                    R& Rv = sR[(unrot(d, c) * MEPC + el) * NP + idx[i]];
+                    R& Rv = sR[(unrot(d, c) * MEPC + el) * mhd::SPM + idx[i]];
                     Rv = (d == 0 ? cd * t[i][c] : Rv + cd * t[i][c]);
                 }
         }
@@ -589,7 +594,7 @@ __global__ void __launch_bounds__(mhd::NT, sizeof(R) == 4 ? 3 : 1) k_stage_mhd(S
 #pragma unroll
             for (int v = 0; v < MV; ++v) {
                 const int s = (v * MEPC + el) * NP + n;
-                double rhs = -(double)sR[s];
+                double rhs = -(double)sR[(v * MEPC + el) * mhd::SPM + n];
                 if (v == 8) rhs = rhs - galpha * su[s];
                 const int64_t g = ((int64_t)v * E + e) * NP + n;
                 if (RHS_ONLY) {
