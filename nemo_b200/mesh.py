@@ -159,13 +159,16 @@ def _balance(nb, max_level, lev, crd):
     split, until none is (level of each finest cell and of its six neighbours, maximum per leaf)."""
     nf = nb << max_level
     while True:
-        span = 1 << (max_level - lev)
         levgrid = np.empty((nf, nf, nf), dtype=np.int64)
         owner = np.empty((nf, nf, nf), dtype=np.int64)
-        for i in range(len(lev)):
-            a = crd[i] * span[i]
-            levgrid[a[0]:a[0] + span[i], a[1]:a[1] + span[i], a[2]:a[2] + span[i]] = lev[i]
-            owner[a[0]:a[0] + span[i], a[1]:a[1] + span[i], a[2]:a[2] + span[i]] = i
+        for lv in np.unique(lev):   # paint the finest cells of all leaves of one level at once
+            sel = np.nonzero(lev == lv)[0]
+            s = 1 << (max_level - int(lv))
+            o = np.arange(s)
+            off = np.stack(np.meshgrid(o, o, o, indexing="ij"), axis=-1).reshape(-1, 3)
+            cells = crd[sel][:, None, :] * s + off[None]
+            levgrid[cells[..., 0], cells[..., 1], cells[..., 2]] = lv
+            owner[cells[..., 0], cells[..., 1], cells[..., 2]] = sel[:, None]
         nbmax = levgrid.copy()
         for d in range(3):
             for sh in (1, -1):
@@ -338,60 +341,83 @@ def adapt(mesh, flags, min_level=0):
     coarsening is dropped)."""
     t = mesh.tree
     nb, max_level, lo, hi = t["nb"], t["max_level"], t["lo"], t["hi"]
-    lev, crd = t["lev"], t["crd"]
+    lev, crd = np.asarray(t["lev"], dtype=np.int64), np.asarray(t["crd"], dtype=np.int64)
     flags = np.asarray(flags)
-    old = {(int(l), int(c[0]), int(c[1]), int(c[2])): i for i, (l, c) in enumerate(zip(lev, crd))}
+    K = nb << max_level
+
+    def key(l, c):   # one integer per (level, x, y, z)
+        return ((l * K + c[:, 0]) * K + c[:, 1]) * K + c[:, 2]
+
+    def lookup(sorted_keys, order, k):
+        """index (in the unsorted list) of each key k, -1 where absent"""
+        if len(sorted_keys) == 0:
+            return np.full(len(k), -1, dtype=np.int64)
+        pos = np.minimum(np.searchsorted(sorted_keys, k), len(sorted_keys) - 1)
+        return np.where(sorted_keys[pos] == k, order[pos], -1)
+
+    ko = key(lev, crd)
+    o_ord = np.argsort(ko, kind="stable")
+    ko_s = ko[o_ord]
     # complete coarsening families (8 leaves of one parent, all flagged, consecutive c = sx + 2sy + 4sz)
-    fam = {}
-    for i in np.nonzero((flags < 0) & (lev > max(int(min_level), 0)))[0]:
-        p = (int(lev[i]) - 1, int(crd[i, 0]) >> 1, int(crd[i, 1]) >> 1, int(crd[i, 2]) >> 1)
-        fam.setdefault(p, []).append(int(i))
-    families = {}
-    for p, members in fam.items():
-        if len(members) != 8:
-            continue
-        ch = {}
-        for i in members:
-            c = (int(crd[i, 0]) & 1) | ((int(crd[i, 1]) & 1) << 1) | ((int(crd[i, 2]) & 1) << 2)
-            ch[c] = i
-        first = ch[0]
-        if all(ch[c] == first + c for c in range(8)):
-            families[p] = first
+    cand = np.nonzero((flags < 0) & (lev > max(int(min_level), 0)))[0]
+    pk = key(lev[cand] - 1, crd[cand] >> 1)
+    cc = (crd[cand, 0] & 1) | ((crd[cand, 1] & 1) << 1) | ((crd[cand, 2] & 1) << 2)
+    srt = np.argsort(pk, kind="stable")
+    pk, cand_s, cc = pk[srt], cand[srt], cc[srt]
+    starts = np.nonzero(np.r_[True, pk[1:] != pk[:-1]])[0]
+    sizes = np.diff(np.r_[starts, len(pk)])
+    first = cand_s - cc                          # equal within a family iff indices are first + c
+    st8 = starts[sizes == 8]
+    same = np.all(first[st8[:, None] + np.arange(8)[None]] == first[st8][:, None], axis=1) if len(st8) else []
+    fam_ok = st8[np.asarray(same, dtype=bool)] if len(st8) else np.zeros(0, dtype=np.int64)
+    fam_key = pk[fam_ok] if len(fam_ok) else np.zeros(0, dtype=np.int64)
+    fam_first = first[fam_ok] if len(fam_ok) else np.zeros(0, dtype=np.int64)
+    fam_lev = (lev[cand_s[fam_ok]] - 1) if len(fam_ok) else np.zeros(0, dtype=np.int64)
+    fam_crd = (crd[cand_s[fam_ok]] >> 1) if len(fam_ok) else np.zeros((0, 3), dtype=np.int64)
     refine = (flags > 0) & (lev < max_level)
     while True:
         gone = np.zeros(len(lev), dtype=bool)
-        for first in families.values():
-            gone[first:first + 8] = True
+        for f0 in fam_first:
+            gone[f0:f0 + 8] = True
         l_new, c_new = _children(lev[~gone], crd[~gone], refine[~gone])
-        if families:
-            pl = np.array([p[0] for p in families], dtype=np.int64)
-            pc = np.array([p[1:] for p in families], dtype=np.int64)
-            l_new = np.concatenate([l_new, pl])
-            c_new = np.concatenate([c_new, pc])
+        l_new = np.concatenate([l_new, fam_lev])
+        c_new = np.concatenate([c_new, fam_crd])
         l_bal, c_bal = _balance(nb, max_level, l_new, c_new)
-        present = {(int(l), int(c[0]), int(c[1]), int(c[2])) for l, c in zip(l_bal, c_bal)}
-        undone = [p for p in families if p not in present]
-        if not undone:
+        keep = np.isin(fam_key, key(np.asarray(l_bal, dtype=np.int64), np.asarray(c_bal, dtype=np.int64)))
+        if keep.all():
             break
-        for p in undone:
-            del families[p]
+        fam_key, fam_first, fam_lev, fam_crd = fam_key[keep], fam_first[keep], fam_lev[keep], fam_crd[keep]
     new = forest_mesh(nb, max_level, l_bal, c_bal, lo, hi)
-    nl, nc = new.tree["lev"], new.tree["crd"]
-    remap = np.zeros((new.E, 4), dtype=np.int32)
-    for e in range(new.E):
-        key = (int(nl[e]), int(nc[e, 0]), int(nc[e, 1]), int(nc[e, 2]))
-        if key in old:
-            remap[e] = (0, old[key], 0, 0)
-            continue
-        if key in families:
-            remap[e] = (2, families[key], 1, 0)
-            continue
-        for depth in range(1, int(nl[e]) + 1):
-            anc = (key[0] - depth, key[1] >> depth, key[2] >> depth, key[3] >> depth)
-            if anc in old:
-                o = [key[1 + a] - (anc[1 + a] << depth) for a in range(3)]
-                remap[e] = (1, old[anc], depth, o[0] | (o[1] << 8) | (o[2] << 16))
-                break
-        else:
-            raise RuntimeError(f"new element {e} has no source in the old forest")
+    nl, nc = np.asarray(new.tree["lev"], dtype=np.int64), np.asarray(new.tree["crd"], dtype=np.int64)
+    kn = key(nl, nc)
+    remap = np.zeros((new.E, 4), dtype=np.int64)
+    done = np.zeros(new.E, dtype=bool)
+    src = lookup(ko_s, o_ord, kn)                # copies
+    m0 = src >= 0
+    remap[m0, 1] = src[m0]
+    done |= m0
+    if len(fam_key):                             # coarsened families
+        f_ord = np.argsort(fam_key, kind="stable")
+        fs = lookup(fam_key[f_ord], f_ord, kn)
+        m2 = ~done & (fs >= 0)
+        remap[m2, 0] = 2
+        remap[m2, 1] = fam_first[fs[m2]]
+        remap[m2, 2] = 1
+        done |= m2
+    for depth in range(1, max_level + 1):       # refinements: the nearest old ancestor
+        todo = np.nonzero(~done & (nl >= depth))[0]
+        if len(todo) == 0:
+            break
+        anc = lookup(ko_s, o_ord, key(nl[todo] - depth, nc[todo] >> depth))
+        hit = anc >= 0
+        e = todo[hit]
+        o = nc[e] - ((nc[e] >> depth) << depth)
+        remap[e, 0] = 1
+        remap[e, 1] = anc[hit]
+        remap[e, 2] = depth
+        remap[e, 3] = o[:, 0] | (o[:, 1] << 8) | (o[:, 2] << 16)
+        done[e] = True
+    if not done.all():
+        raise RuntimeError(f"new element {int(np.nonzero(~done)[0][0])} has no source in the old forest")
+    remap = remap.astype(np.int32)
     return new, remap
