@@ -272,7 +272,23 @@ def run_reference(args, rank, world):
                                    "reference is unbuildable here, this is its C++ FP64 restatement"},
         "e2e": {"value": val, "unit": "DOF-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    line["pid"] = {"cpu": o.nthreads * 1e6 / val, "unit": PID_UNIT, "note": PID_NOTE}
     print(json.dumps(line), flush=True)
+
+
+PID_UNIT = "us per node-stage per device (GPU) or per core (CPU)"
+PID_NOTE = ("performance index of the reference's driver (source/driver_mod.f90:83): wall time x processing "
+            "units / (nodes x time steps x RK stages); for one device 1e6 / (DOF-updates/s per device)")
+
+
+def pid_block(value, e2e, value64, cpu):
+    """The reference's performance index for each measured form (lower is better)."""
+    out = {"chosen": 1e6 / value, "plain_fp64": 1e6 / value64, "unit": PID_UNIT, "note": PID_NOTE}
+    if e2e:
+        out["e2e"] = 1e6 / e2e
+    if cpu:
+        out["cpu_baseline"] = cpu["cores"] * 1e6 / cpu["value"]
+    return out
 
 
 def main():
@@ -441,6 +457,7 @@ def main():
         }
         if cpu:
             line["cpu_baseline"] = cpu
+        line["pid"] = pid_block(value / world, None if e2e_val is None else e2e_val / world, value64 / world, cpu)
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()

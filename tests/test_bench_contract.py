@@ -21,3 +21,5 @@ def test_reference_arm_json_line():
     assert line["e2e"] == {"value": line["value"], "unit": "DOF-updates/s", "h2d_bytes_per_step": 0,
                            "d2h_bytes_per_step": 0}
     assert "workload" in line["config"]
+    # the reference driver's performance index: microseconds per node-stage per core
+    assert abs(line["pid"]["cpu"] - cb["cores"] * 1e6 / line["value"]) < 1e-9 * line["pid"]["cpu"]
