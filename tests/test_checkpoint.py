@@ -78,3 +78,18 @@ def test_round_trip_adapted_forest(tmp_path):
 
 def test_round_trip_brick(tmp_path):
     _round_trip(mesh.brick(4), tmp_path)
+
+
+def test_round_trip_mhd(tmp_path):
+    """GLM-MHD state: the 9 FLASH variable names and a lossless round trip."""
+    m = band_forest()
+    u = setups.orszag_tang(m)
+    c = abi.default_cfg(eqn=abi.EQN_MHD, n_vars=9, kappa=5 / 3)
+    path = str(tmp_path / "mhd.f5.npz")
+    checkpoint.write(path, checkpoint.datasets(m, u, 0.5, 7, c))
+    with np.load(path) as z:
+        assert [n[0] for n in z["unknown names"]] == [n.encode() for n in checkpoint.MHD_NAMES] + [b"blnd"]
+        g = {r["name"]: r["value"] for r in z["real runtime parameters"]}
+        assert abs(g[b"gamma"] - 5 / 3) < 1e-15
+    m2, u2, t, steps = checkpoint.read(path)
+    assert u2.shape == u.shape and np.array_equal(u2, u) and t == 0.5 and steps == 7
