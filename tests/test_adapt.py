@@ -106,3 +106,25 @@ def test_inadmissible_refinement_falls_back_to_the_mean():
     t0 = orc.Oracle(c, m.neighbors(), m.delta, mortars=m.mortars()).totals(u)
     t1 = orc.Oracle(c, n.neighbors(), n.delta, mortars=n.mortars()).totals(got)
     np.testing.assert_allclose(t1, t0, rtol=1e-14, atol=1e-14)
+
+
+def test_coarsening_undone_by_balance_is_dropped():
+    """A family flagged for coarsening whose face neighbours refine at the same time would leave a
+    level jump of 2: the coarsening is dropped (its 8 leaves are copied), the refinement stays; the
+    same family alone coarsens."""
+    m = mesh.forest(2, lambda lvl, c, s: np.full(len(c), lvl < 2), max_level=3)
+    lev, crd = m.tree["lev"], m.tree["crd"]
+    fam = np.nonzero((lev == 2) & np.all(crd >> 1 == 0, axis=1))[0]
+    nbr = np.nonzero((lev == 2) & (crd[:, 0] == 2) & (crd[:, 1] < 2) & (crd[:, 2] < 2))[0]
+    assert len(fam) == 8 and len(nbr) == 4
+    f = np.zeros(m.E, np.int32)
+    f[fam] = -1
+    f[nbr] = 1
+    n, r = mesh.adapt(m, f)
+    assert not np.any(r[:, 0] == 2) and np.sum(r[:, 0] == 1) == 32
+    assert set(fam) <= set(r[r[:, 0] == 0, 1])
+    for row in n.mortars():
+        assert np.all(n.level[row[2:]] == n.level[row[0]] + 1)
+    f[nbr] = 0
+    n2, r2 = mesh.adapt(m, f)
+    assert n2.E == m.E - 7 and np.sum(r2[:, 0] == 2) == 1 and r2[r2[:, 0] == 2][0, 1] == fam[0]
