@@ -878,13 +878,13 @@ int nemo_gpu_checkpoint_begin(double* host, int64_t stride, double* alpha_host) 
         CK(cudaEventSynchronize(g.ckpt_done));
         g.ckpt_pending = false;
     }
-    if (!g.copy_stream) {
-        CK(cudaStreamCreateWithFlags(&g.copy_stream, cudaStreamNonBlocking));
-        CK(cudaEventCreateWithFlags(&g.ckpt_ready, cudaEventDisableTiming));
-        CK(cudaEventCreateWithFlags(&g.ckpt_done, cudaEventDisableTiming));
-        CK(cudaMalloc(&g.ckpt_meta, 2 * sizeof(double)));
-        CK(cudaHostAlloc(&g.ckpt_meta_host, 2 * sizeof(double), cudaHostAllocDefault));
-    }
+    // first call: the copy stream, its events and the time/step staging (each piece on its own, so a
+    // failed set-up is completed by the next call)
+    if (!g.copy_stream) CK(cudaStreamCreateWithFlags(&g.copy_stream, cudaStreamNonBlocking));
+    if (!g.ckpt_ready) CK(cudaEventCreateWithFlags(&g.ckpt_ready, cudaEventDisableTiming));
+    if (!g.ckpt_done) CK(cudaEventCreateWithFlags(&g.ckpt_done, cudaEventDisableTiming));
+    if (!g.ckpt_meta) CK(cudaMalloc(&g.ckpt_meta, 2 * sizeof(double)));
+    if (!g.ckpt_meta_host) CK(cudaHostAlloc(&g.ckpt_meta_host, 2 * sizeof(double), cudaHostAllocDefault));
     const int64_t bytes = (int64_t)row * g.E;
     const int64_t abytes = (int64_t)sizeof(double) * g.E;   // blending coefficients after the state
     if (g.ckpt_bytes != bytes + abytes) {
