@@ -128,3 +128,31 @@ def test_coarsening_undone_by_balance_is_dropped():
     f[nbr] = 0
     n2, r2 = mesh.adapt(m, f)
     assert n2.E == m.E - 7 and np.sum(r2[:, 0] == 2) == 1 and r2[r2[:, 0] == 2][0, 1] == fam[0]
+
+
+def test_inadmissible_coarsening_falls_back_to_the_mean():
+    """Children with rough but positive densities whose projection undershoots below zero: the
+    coarsened element takes the mean of its 8 children (conservative and admissible)."""
+    m = mesh.forest(2, lambda lvl, c, s: np.full(len(c), lvl < 1), max_level=2)
+    lev, crd = m.tree["lev"], m.tree["crd"]
+    fam = np.nonzero((lev == 1) & np.all(crd >> 1 == 0, axis=1))[0]
+    u = np.zeros((5, m.E, 64))
+    u[0], u[4] = 1.0, 2.5
+    rng = np.random.default_rng(1)
+    for c in fam:
+        u[0, c] = np.where(rng.random(64) < 0.5, 1e-3, 3.0)
+    # the plain projection (sum of the children's L2 projections) is not admissible
+    _, prj = orc.mortar_operators()
+    plain = sum(np.einsum("ai,bj,ck,kji->cba", prj[c & 1], prj[(c >> 1) & 1], prj[c >> 2],
+                          u[0, fam[c]].reshape(4, 4, 4)) for c in range(8))
+    assert plain.min() < 0
+    f = np.zeros(m.E, np.int32)
+    f[fam] = -1
+    n, r = mesh.adapt(m, f)
+    got = orc.remap(u, r)
+    e2 = int(np.nonzero(r[:, 0] == 2)[0][0])
+    wq = orc.lgl(3)[1]
+    w = np.einsum("a,b,c->cba", wq, wq, wq).ravel()
+    for v in range(5):
+        np.testing.assert_allclose(got[v, e2], np.mean([w @ u[v, c] / 8.0 for c in fam]), rtol=1e-14, atol=1e-15)
+    assert np.all(got[0] > 0)
