@@ -55,51 +55,48 @@ def partition(mesh, nranks):
     owner = np.empty(E, dtype=np.int64)
     for r, (lo, hi) in enumerate(ranges):
         owner[lo:hi] = r
-    # quads of every side (1, 2 or 5 of them)
-    side_elems = []
-    for s in range(mesh.S):
-        q = []
-        for h in range(2):
-            n = int(mesh.side_nquads[s, h])
-            q.extend(int(x) for x in mesh.side_quads[s, h, :n])
-        side_elems.append(q)
+    # quads of every side (1, 2 or 5 of them), -1 where unused
+    sq = np.asarray(mesh.side_quads, dtype=np.int64)
+    nq = np.asarray(mesh.side_nquads, dtype=np.int64)
+    valid = np.arange(4)[None, None, :] < nq[:, :, None]
+    qv = np.where(valid, sq, -1)
+    fid = np.asarray(mesh.side_faceid, dtype=np.int64)
     parts = []
     for r, (lo, hi) in enumerate(ranges):
-        sides = [s for s in range(mesh.S) if any(lo <= e < hi for e in side_elems[s])]
-        need = sorted({e for s in sides for e in side_elems[s] if not lo <= e < hi},
-                      key=lambda e: (owner[e], e))
-        glob = np.concatenate([np.arange(lo, hi), np.asarray(need, dtype=np.int64)])
-        loc = {int(g): i for i, g in enumerate(glob)}
-        Q, F, NQ, B = [], [], [], []
-        covered = set()
-        for s in sides:
-            q = np.full((2, 4), -1, dtype=np.int32)
-            for h in range(2):
-                n = int(mesh.side_nquads[s, h])
-                for k in range(n):
-                    gq = int(mesh.side_quads[s, h, k])
-                    q[h, k] = loc[gq]
-                    covered.add((loc[gq], int(mesh.side_faceid[s, h])))
-            Q.append(q)
-            F.append(mesh.side_faceid[s])
-            NQ.append(mesh.side_nquads[s])
-            B.append(mesh.boundary[s])
+        mine = (qv >= lo) & (qv < hi)
+        sides = np.nonzero(mine.any(axis=(1, 2)))[0]
+        qs = qv[sides]
+        other = qs[(qs >= 0) & ((qs < lo) | (qs >= hi))]
+        need = np.unique(other)                 # ghosts, ascending (= by owner, then id)
+        glob = np.concatenate([np.arange(lo, hi), need]).astype(np.int64)
+        loc = np.full(E, -1, dtype=np.int64)
+        loc[glob] = np.arange(len(glob))
+        Q = np.where(qs >= 0, loc[np.maximum(qs, 0)], -1).astype(np.int32)
+        F = fid[sides].astype(np.int8)
+        NQ = nq[sides].astype(np.int8)
+        B = np.asarray(mesh.boundary, dtype=np.int32)[sides]
+        # (local element, face) pairs on the included sides
+        vmask = qs >= 0
+        ce = Q.astype(np.int64)[vmask]
+        cf = np.broadcast_to(F.astype(np.int64)[:, :, None], qs.shape)[vmask]
+        nown, nloc = hi - lo, len(glob)
+        cov = np.zeros((nloc, 6), dtype=bool)
+        cov[ce, cf] = True
         # faces of ghosts that no included side covers: boundary sides (mirrored state, never used)
-        for i in range(hi - lo, len(glob)):
-            for f in range(6):
-                if (i, f) not in covered:
-                    q = np.full((2, 4), -1, dtype=np.int32)
-                    q[0, 0] = i
-                    Q.append(q)
-                    F.append(np.array([f, f ^ 1], dtype=np.int8))
-                    NQ.append(np.array([1, 0], dtype=np.int8))
-                    B.append(1 + f)
-        gl = glob
-        local = Mesh(mesh.delta[gl], mesh.center[gl], np.stack(Q), np.stack(F), np.stack(NQ),
-                     np.asarray(B, dtype=np.int32), level=mesh.level[gl])
-        part = Part(rank=r, mesh=local, n_owned=hi - lo, glob=glob)
+        gi, gf = np.nonzero(~cov[nown:])
+        gi = gi + nown
+        if len(gi):
+            qb = np.full((len(gi), 2, 4), -1, dtype=np.int32)
+            qb[:, 0, 0] = gi
+            Q = np.concatenate([Q, qb])
+            F = np.concatenate([F, np.stack([gf, gf ^ 1], axis=1).astype(np.int8)])
+            NQ = np.concatenate([NQ, np.tile(np.array([1, 0], dtype=np.int8), (len(gi), 1))])
+            B = np.concatenate([B, (1 + gf).astype(np.int32)])
+        local = Mesh(mesh.delta[glob], mesh.center[glob], Q, F, NQ, B, level=mesh.level[glob])
+        part = Part(rank=r, mesh=local, n_owned=nown, glob=glob)
         # ghost faces on the included sides: the traces this rank reads from other ranks' elements
-        part.ghost_faces = sorted((int(glob[i]), f) for i, f in covered if i >= hi - lo)
+        hi_i, hi_f = np.nonzero(cov[nown:])
+        part.ghost_faces = [(int(glob[i + nown]), int(f)) for i, f in zip(hi_i, hi_f)]
         parts.append(part)
     # exchange plan: rank r receives its ghosts owned by p; p sends them in the same (global) order
     for r, pr in enumerate(parts):
