@@ -102,13 +102,14 @@ def _restrict(tree, leaf_data):
     out = np.zeros((nb, V, 4, 4, 4))
     out[nin:] = leaf_data.transpose(1, 0, 2).reshape(-1, V, 4, 4, 4)
     _, prj = abi.mortar_operators()
-    for i in sorted(range(nin), key=lambda i: -tree["level"][i]):
-        acc = np.zeros((V, 4, 4, 4))
+    lev_in = tree["level"][:nin]
+    for lv in sorted(set(lev_in.tolist()), reverse=True):   # children (one level finer) are done
+        par = np.nonzero(lev_in == lv)[0]
+        acc = np.zeros((len(par), V, 4, 4, 4))
         for c in range(8):
-            ch = tree["children"][i, c]
             px, py, pz = prj[c & 1], prj[(c >> 1) & 1], prj[c >> 2]
-            acc += np.einsum("ai,bj,ck,vkji->vcba", px, py, pz, out[ch])
-        out[i] = acc
+            acc += np.einsum("ai,bj,ck,nvkji->nvcba", px, py, pz, out[tree["children"][par, c]], optimize=True)
+        out[par] = acc
     return out
 
 
