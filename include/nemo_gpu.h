@@ -267,15 +267,22 @@ int nemo_gpu_mlp_forward(const float* feat, int64_t nsamp, const float* weights,
    without allocating anything.  No counterpart in the reference: it serves hosts that cannot
    allocate device memory at this point (device arrays owned by a Fortran/OpenACC pool sized at
    start-up, or a fixed device-memory budget where a cudaMalloc/cudaFree would fail or synchronise
-   the device).  u_dev: [nvars][nelems][64] FP64 (the library's layout); delta_dev: [nelems][3];
-   out_dev: nvars doubles; all device pointers.  stream: a cudaStream_t as an integer (0 = the
-   legacy default stream); the call only enqueues work on it.  Limits: 1 <= nelems <= 65536 and
-   1 <= nvars <= 9 (larger sizes are rejected with NEMO_ERR_ARG): the per-element partial sums live
-   in a fixed 4.5 MiB device array inside the library, held by every GPU that loads it until exit.
-   The first call on a device looks up that array's address (make it before any stream capture).
-   Every call overwrites the array, so calls that overlap on the GPU (other streams) race. */
-int nemo_gpu_totals_noalloc(const double* u_dev, const double* delta_dev, int64_t nelems, int32_t nvars,
-                            double* out_dev, uint64_t stream);
+   the device).  u_dev: [nvars][elem_stride][64] FP64 (the library's layout); delta_dev:
+   [elem_stride][3]; only the first nelems elements are summed, so a partitioned state passes its
+   element count as elem_stride and its owned count as nelems (its ghost copies after the owned
+   elements are left out, as nemo_gpu_totals leaves them out); out_dev: nvars doubles; all device
+   pointers.  stream: a cudaStream_t as an integer (0 = the legacy default stream); the call only
+   enqueues work on it.  Limits: 1 <= nelems <= 65536, nelems <= elem_stride and 1 <= nvars <= 9
+   (anything else is rejected with NEMO_ERR_ARG): the per-element partial sums live in a fixed
+   4.5 MiB device array inside the library, held by every GPU that loads it until exit.  The first
+   call on a device looks up that array's address with cudaGetSymbolAddress and caches it; under
+   lazy module loading that look-up may load the library's device code, which can itself allocate,
+   so make the first call at start-up (and before any stream capture).  The cached address belongs
+   to the device context: after a cudaDeviceReset by the host it is stale, so do not call this
+   entry point again in that process.  Every call overwrites the array, so calls that overlap on
+   the GPU (other streams) race. */
+int nemo_gpu_totals_noalloc(const double* u_dev, const double* delta_dev, int64_t elem_stride, int64_t nelems,
+                            int32_t nvars, double* out_dev, uint64_t stream);
 
 int nemo_gpu_finalize(void);
 
@@ -304,6 +311,14 @@ int nemo_gpu_kernel_timing(double* stage_ms, int64_t* stage_launches, double* to
 /* The library's CUDA stream (cudaStream_t as an integer), for callers that record their own
    events on it. */
 int nemo_gpu_stream(uint64_t* stream_out);
+
+/* Measured arithmetic peaks of the current device for the roofline of the stage kernels (no
+   counterpart in the reference, which reports only its wall-time performance index,
+   source/driver_mod.f90:83): out[0] FP64 and out[1] FP32 fused-multiply-add throughput in
+   TFLOP/s (2 flops per FMA, independent chains on every SM, best of 3 timed launches of about
+   10 ms), out[2] the SM count, out[3] the maximum SM clock in MHz.  Allocates and frees a 2 KB
+   buffer and a stream; call it outside timed regions. */
+int nemo_gpu_measure_peaks(double* out);
 
 #ifdef __cplusplus
 }

@@ -31,7 +31,7 @@ EXPORTS = [
     "nemo_gpu_autotune", "nemo_gpu_set_schedule", "nemo_gpu_set_owned", "nemo_gpu_pack_elements",
     "nemo_gpu_unpack_elements", "nemo_gpu_adapt", "nemo_gpu_amr_flags",
     "nemo_gpu_checkpoint_begin", "nemo_gpu_checkpoint_wait", "nemo_gpu_set_time",
-    "nemo_gpu_pack_faces", "nemo_gpu_unpack_faces",
+    "nemo_gpu_pack_faces", "nemo_gpu_unpack_faces", "nemo_gpu_measure_peaks",
 ]
 
 
@@ -91,7 +91,8 @@ def load(path=LIB_PATH):
         "nemo_gpu_kernel_timing": [ctypes.POINTER(dbl), ctypes.POINTER(i64), ctypes.POINTER(dbl),
                                    ctypes.POINTER(i64)],
         "nemo_gpu_stream": [ctypes.POINTER(ctypes.c_uint64)],
-        "nemo_gpu_totals_noalloc": [vp, vp, i64, i32, vp, ctypes.c_uint64],
+        "nemo_gpu_measure_peaks": [vp],
+        "nemo_gpu_totals_noalloc": [vp, vp, i64, i64, i32, vp, ctypes.c_uint64],
         "nemo_gpu_set_mlp": [vp, i32, vp, vp],
         "nemo_gpu_features": [vp, vp],
         "nemo_gpu_indicator_stats": [ctypes.POINTER(i64), ctypes.POINTER(i64), ctypes.POINTER(dbl)],
@@ -136,6 +137,27 @@ def call(name, *args):
 def default_cfg(**kw):
     c = NemoCfg()
     call("nemo_gpu_default_cfg", ctypes.byref(c))
+    for k, v in kw.items():
+        if not hasattr(c, k):
+            raise AttributeError(k)
+        setattr(c, k, v)
+    return c
+
+
+def measure_peaks():
+    """Measured FP64 / FP32 FMA peaks of the current device: dict with TFLOP/s, SM count and clock."""
+    out = np.zeros(4)
+    call("nemo_gpu_measure_peaks", out.ctypes.data)
+    return {"fp64_tflops": float(out[0]), "fp32_tflops": float(out[1]), "sms": int(out[2]),
+            "sm_max_mhz": float(out[3])}
+
+
+def cfg_struct(**kw):
+    """A NemoCfg with the defaults of nemo_gpu_default_cfg, built without loading the library (for
+    callers that only drive the oracle)."""
+    c = NemoCfg(n_nodes=4, n_vars=5, eqn=EQN_EULER, volume_flux=VOLFLUX_CHANDRASHEKAR, surface_flux=SURFFLUX_HLLC,
+                precision=PREC_FP64, indicator=IND_NONE, alpha_smoothing=1, positivity=0, kappa=1.4, mu0=1.0,
+                cfl=0.5, alpha_max=0.5, alpha_min=0.001, repair_decr=0.01)
     for k, v in kw.items():
         if not hasattr(c, k):
             raise AttributeError(k)

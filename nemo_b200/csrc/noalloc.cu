@@ -29,10 +29,12 @@ struct Weights {
     double wt[NN];
 };
 
+// part[v][e] for the first n elements of a state with element stride E (n <= E; elements [n, E) are
+// ghost copies of a partitioned run and are not summed)
 __global__ void k_totals_elem64_static(const double* __restrict__ u, const double* __restrict__ delta, int64_t E,
-                                       int nv, Weights w, double* __restrict__ part) {
+                                       int64_t n, int nv, Weights w, double* __restrict__ part) {
     const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= E) return;
+    if (e >= n) return;
     const double vol = delta[e * 3 + 0] * delta[e * 3 + 1] * delta[e * 3 + 2];
     for (int v = 0; v < nv; ++v) {
         double s = 0.0;
@@ -40,7 +42,7 @@ __global__ void k_totals_elem64_static(const double* __restrict__ u, const doubl
         for (int kk = 0; kk < NN; ++kk)
             for (int j = 0; j < NN; ++j)
                 for (int i = 0; i < NN; ++i) s = s + w.wt[i] * w.wt[j] * w.wt[kk] * ue[nidx(i, j, kk)];
-        part[(int64_t)v * E + e] = vol * s;
+        part[(int64_t)v * n + e] = vol * s;
     }
 }
 
@@ -54,6 +56,8 @@ __global__ void k_totals_sum64_static(const double* __restrict__ part, int64_t E
 
 constexpr int MAX_DEVICES = 64;
 double* g_scratch_ptr[MAX_DEVICES] = {};
+Weights g_weights;          // quadrature weights on [-1/2, 1/2], built with the first scratch look-up
+bool g_have_weights = false;
 
 }  // namespace
 
@@ -66,8 +70,8 @@ using namespace nemo;
 extern "C" int nemo_gpu_operators(int32_t n, double* nodes, double* weights, double* dmat, double* smat,
                                   double* vinv);
 
-extern "C" int nemo_gpu_totals_noalloc(const double* u_dev, const double* delta_dev, int64_t nelems, int32_t nvars,
-                                       double* out_dev, uint64_t stream) {
+extern "C" int nemo_gpu_totals_noalloc(const double* u_dev, const double* delta_dev, int64_t elem_stride,
+                                       int64_t nelems, int32_t nvars, double* out_dev, uint64_t stream) {
     auto fail = [](int code, const char* msg) {
         set_last_error(msg);
         return code;
@@ -77,6 +81,12 @@ extern "C" int nemo_gpu_totals_noalloc(const double* u_dev, const double* delta_
         char buf[160];
         std::snprintf(buf, sizeof buf, "nemo_gpu_totals_noalloc: nelems = %lld outside [1, %lld] (the size of its fixed scratch)",
                       (long long)nelems, (long long)NOALLOC_MAX_ELEMS);
+        return fail(NEMO_ERR_ARG, buf);
+    }
+    if (elem_stride < nelems) {
+        char buf[160];
+        std::snprintf(buf, sizeof buf, "nemo_gpu_totals_noalloc: elem_stride = %lld below nelems = %lld",
+                      (long long)elem_stride, (long long)nelems);
         return fail(NEMO_ERR_ARG, buf);
     }
     if (nvars < 1 || nvars > NOALLOC_MAX_VARS) return fail(NEMO_ERR_ARG, "nemo_gpu_totals_noalloc: nvars outside [1, 9]");
@@ -90,13 +100,16 @@ extern "C" int nemo_gpu_totals_noalloc(const double* u_dev, const double* delta_
         if (err != cudaSuccess || !ptr) return fail(NEMO_ERR_CUDA, "nemo_gpu_totals_noalloc: cudaGetSymbolAddress failed");
         g_scratch_ptr[dev] = ptr;
     }
-    Weights w;
-    double x[NN], wl[NN];
-    nemo_gpu_operators(NN, x, wl, nullptr, nullptr, nullptr);
-    for (int i = 0; i < NN; ++i) w.wt[i] = 0.5 * wl[i];
+    if (!g_have_weights) {
+        double x[NN], wl[NN];
+        if (nemo_gpu_operators(NN, x, wl, nullptr, nullptr, nullptr) != NEMO_OK)
+            return fail(NEMO_ERR_ARG, "nemo_gpu_totals_noalloc: quadrature weights could not be built");
+        for (int i = 0; i < NN; ++i) g_weights.wt[i] = 0.5 * wl[i];
+        g_have_weights = true;
+    }
     cudaStream_t s = (cudaStream_t)(uintptr_t)stream;
-    k_totals_elem64_static<<<(unsigned)((nelems + 127) / 128), 128, 0, s>>>(u_dev, delta_dev, nelems, nvars, w,
-                                                                           g_scratch_ptr[dev]);
+    k_totals_elem64_static<<<(unsigned)((nelems + 127) / 128), 128, 0, s>>>(u_dev, delta_dev, elem_stride, nelems,
+                                                                           nvars, g_weights, g_scratch_ptr[dev]);
     k_totals_sum64_static<<<1, 32, 0, s>>>(g_scratch_ptr[dev], nelems, nvars, out_dev);
     cudaError_t err = cudaGetLastError();
     if (err != cudaSuccess) return fail(NEMO_ERR_CUDA, cudaGetErrorString(err));
