@@ -17,7 +17,6 @@ import json
 import os
 import subprocess
 import sys
-import threading
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
@@ -56,10 +55,12 @@ def load_peaks():
         return 6650.0, "fallback"
 
 
-def make_state(wl):
-    """(mesh, state, groups or None)."""
+def make_state(wl, nx=None):
+    """(mesh, state, groups or None); nx overrides the elements per direction (smaller samples)."""
     from nemo_b200 import mesh, setups
-    w = WORKLOADS[wl]
+    w = dict(WORKLOADS[wl])
+    if nx:
+        w["nx"] = nx
     if w["setup"] == "batch":
         m, g, f, one, amps = mesh.batched_workload(nb=w["nx"])
         u = np.concatenate([setups.kelvin_helmholtz(f)] + [setups.gaussian_blob(one, a) for a in amps], axis=1)
@@ -76,15 +77,17 @@ def make_state(wl):
     return m, u, None
 
 
-def make_cfg(wl, precision=0, learned=False):
+def make_cfg(wl, precision=0, learned=False, host_only=False):
+    """Configuration of a workload; host_only builds it without loading the CUDA library (oracle runs)."""
     from nemo_b200 import abi
     w = WORKLOADS[wl]
+    make = abi.cfg_struct if host_only else abi.default_cfg
     ind = abi.IND_LEARNED if (learned and w["indicator"]) else w["indicator"]
     if w.get("mhd"):
-        return abi.default_cfg(indicator=ind, positivity=w["positivity"], cfl=0.5, precision=precision,
-                               eqn=abi.EQN_MHD, n_vars=9, volume_flux=abi.VOLFLUX_EC_MHD,
-                               surface_flux=abi.SURFFLUX_HLLD, kappa=5.0 / 3.0, mu0=1.0)
-    return abi.default_cfg(indicator=ind, positivity=w["positivity"], cfl=0.5, precision=precision)
+        return make(indicator=ind, positivity=w["positivity"], cfl=0.5, precision=precision,
+                    eqn=abi.EQN_MHD, n_vars=9, volume_flux=abi.VOLFLUX_EC_MHD,
+                    surface_flux=abi.SURFFLUX_HLLD, kappa=5.0 / 3.0, mu0=1.0)
+    return make(indicator=ind, positivity=w["positivity"], cfl=0.5, precision=precision)
 
 
 def make_solver(wl, m, precision, learned=False, groups=None):
@@ -177,7 +180,7 @@ def cpu_baseline(wl, u, m, nthreads=None, sample_stages=5):
     """The oracle (C++ FP64 restatement, OpenMP) on the host cores, on a bounded sample of the same
     workload: sample_stages RK stages of the full state (one common time step for all elements)."""
     from oracle import oracle as orc
-    c = make_cfg(wl)
+    c = make_cfg(wl, host_only=True)
     o = orc.Oracle.for_mesh(c, m, nthreads=nthreads)
     uu, reg = u.copy(), np.zeros_like(u)
     dt, _ = o.timestep(uu)
@@ -193,15 +196,28 @@ def cpu_baseline(wl, u, m, nthreads=None, sample_stages=5):
                       f"{o.nthreads} OpenMP threads, {el:.2f} s"}
 
 
+FORMS = {
+    # key: (precision, learned indicator)
+    "fp64_modal": (0, False),      # the plain path: bit-identical to the FP64 oracle
+    "fp32_modal": (1, False),      # the chosen form
+    "fp64_learned": (0, True),
+    "fp32_learned": (1, True),
+}
+GATE = 1e-6   # relative L1 density error of a form against the plain FP64 (oracle) run at t_end
+
+
 def accuracy_check(wl, m, u, abi, Solver, t_end=0.05, groups=None):  # noqa: C901
-    """All forms to t_end.  The chosen form (FP32 bulk + learned indicator) against the FP64 form of
-    the same method (learned indicator evaluated in FP64 from the same BF16 weights; that plain
-    path reproduces the FP64 oracle bit for bit, see tests/test_gpu_learned.py), and both against
-    the plain FP64 modal-indicator run."""
+    """Every form to t_end.  The gate compares density at t_end with the plain FP64 run of the modal
+    method, which reproduces the FP64 oracle bit for bit (tests/test_gpu_parity.py,
+    tests/test_gpu_baseline_sizes.py): the chosen form (FP32 bulk + modal indicator) must stay within
+    1e-6 relative L1.  The learned-indicator forms are reported against the same oracle run (a
+    different indicator is a different method, so they do not meet the gate) and against the FP64
+    run of their own method."""
     import ctypes
     res = {}
-    for key, prec, learned in (("fp64_modal", abi.PREC_FP64, False), ("fp64_learned", abi.PREC_FP64, True),
-                               ("fp32_learned", abi.PREC_FP32, True)):
+    for key, (prec, learned) in FORMS.items():
+        if learned and not WORKLOADS[wl]["indicator"]:
+            continue
         s = make_solver(wl, m, prec, learned, groups)
         s.upload(u)
         if prec == abi.PREC_FP32:
@@ -221,19 +237,27 @@ def accuracy_check(wl, m, u, abi, Solver, t_end=0.05, groups=None):  # noqa: C90
     def l1(a, b):
         return float(np.sum(np.abs(a - b)) / np.sum(np.abs(b)))
 
+    def linf(a, b):
+        return float(np.max(np.abs(a - b)) / np.max(np.abs(b)))
+
     r = res
-    return {"t_end": t_end, "steps": {k: v["steps"] for k, v in r.items()},
-            "rel_l1_density_chosen_vs_fp64_same_method": l1(r["fp32_learned"]["rho"], r["fp64_learned"]["rho"]),
-            "rel_linf_density_chosen_vs_fp64_same_method": float(
-                np.max(np.abs(r["fp32_learned"]["rho"] - r["fp64_learned"]["rho"])) / np.max(np.abs(r["fp64_learned"]["rho"]))),
-            "rel_l1_density_learned_vs_modal_fp64": l1(r["fp64_learned"]["rho"], r["fp64_modal"]["rho"]),
-            "indicator_judge": {k: {"fallback_elements": v["fallback"], "judged_elements": v["judged"],
-                                    "mean_abs_alpha_learned_minus_modal": v["judge_mae"]}
-                                for k, v in r.items() if k != "fp64_modal"},
-            "repair_failures": {k: v["nbad"] for k, v in r.items()},
-            "wall_s_to_t_end": {k: v["wall"] for k, v in r.items()},
-            **({"div_b_l2_linf": {"t0": divb(m, u, abi), **{k: v["divb"] for k, v in r.items()}}}
-               if WORKLOADS[wl].get("mhd") else {})}
+    ref = r["fp64_modal"]["rho"]
+    out = {"t_end": t_end, "gate": GATE,
+           "gate_reference": "plain FP64 GPU run of the modal method (bit-identical to the FP64 oracle)",
+           "steps": {k: v["steps"] for k, v in r.items()},
+           "rel_l1_density_vs_fp64_oracle": {k: l1(v["rho"], ref) for k, v in r.items() if k != "fp64_modal"},
+           "rel_linf_density_vs_fp64_oracle": {k: linf(v["rho"], ref) for k, v in r.items() if k != "fp64_modal"},
+           "repair_failures": {k: v["nbad"] for k, v in r.items()},
+           "wall_s_to_t_end": {k: v["wall"] for k, v in r.items()}}
+    out["chosen_form_passes_gate"] = out["rel_l1_density_vs_fp64_oracle"]["fp32_modal"] <= GATE
+    if "fp64_learned" in r:
+        out["rel_l1_density_fp32_learned_vs_fp64_learned"] = l1(r["fp32_learned"]["rho"], r["fp64_learned"]["rho"])
+        out["indicator_judge"] = {k: {"fallback_elements": v["fallback"], "judged_elements": v["judged"],
+                                      "mean_abs_alpha_learned_minus_modal": v["judge_mae"]}
+                                  for k, v in r.items() if k.endswith("learned")}
+    if WORKLOADS[wl].get("mhd"):
+        out["div_b_l2_linf"] = {"t0": divb(m, u, abi), **{k: v["divb"] for k, v in r.items()}}
+    return out
 
 
 def divb(m, u, abi):
@@ -242,16 +266,24 @@ def divb(m, u, abi):
     return setups.divergence_b(m, u, D, w)
 
 
+def workload_config(wl, m, u):
+    """The `config` block, identical in both arms: the workload only."""
+    return {"workload": WORKLOADS[wl]["desc"], "elements": int(m.E), "nodes": int(m.E * 64), "stages_per_step": 5,
+            "l2": f"working set (u in/out + register, 3 x {u.nbytes / 1e6:.0f} MB) larger than L2"
+                  if 3 * u.nbytes > 126e6 else "working set fits in L2 (126 MB): HBM figures are L2-assisted"}
+
+
 def run_reference(args, rank, world):
     """--impl reference: the reference's CPU implementation of the path.  The Fortran reference
     cannot be built here (no Fortran compiler / MPI / p4est / HDF5), so this times the C++ FP64
-    restatement of it (oracle/) on all host cores; each step is one full time step (5 stages)."""
+    restatement of it (oracle/) on all host cores; each step is one full time step (5 stages).  It
+    loads only the oracle (the configuration struct is filled on the host)."""
     if rank != 0:
         return
     from oracle import oracle as orc
     orc.build()
     m, u, groups = make_state(args.workload)
-    c = make_cfg(args.workload)
+    c = make_cfg(args.workload, host_only=True)
     o = orc.Oracle.for_mesh(c, m)
     uu = u.copy()
     for _ in range(args.warmup):
@@ -265,8 +297,8 @@ def run_reference(args, rank, world):
         "impl": "reference", "metric": "DOF-updates/s per RK stage", "value": val, "unit": "DOF-updates/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOADS[args.workload]["desc"], "elements": m.E, "nodes": m.E * 64,
-                   "stages_per_step": 5},
+        "config": workload_config(args.workload, m, u),
+        "form": "reference CPU path: FP64, modal indicator (C++ restatement of the Fortran, OpenMP)",
         "cpu_baseline": {"value": val, "unit": "DOF-updates/s", "cores": o.nthreads, "kind": "port",
                          "sample": f"{args.steps} full time steps, {o.nthreads} OpenMP threads; the Fortran "
                                    "reference is unbuildable here, this is its C++ FP64 restatement"},
@@ -281,17 +313,34 @@ PID_NOTE = ("performance index of the reference's driver (source/driver_mod.f90:
             "units / (nodes x time steps x RK stages); for one device 1e6 / (DOF-updates/s per device)")
 
 
-def pid_block(value, e2e, value64, cpu):
-    """The reference's performance index for each measured form (lower is better)."""
-    out = {"chosen": 1e6 / value, "plain_fp64": 1e6 / value64, "unit": PID_UNIT, "note": PID_NOTE}
-    if e2e:
-        out["e2e"] = 1e6 / e2e
-    if cpu:
-        out["cpu_baseline"] = cpu["cores"] * 1e6 / cpu["value"]
+def load_flops(wl):
+    """Algorithmic flops per DOF-update of the workload (profiles/roofline.json, from the counting
+    build of the oracle: python -m oracle.count_flops)."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "roofline.json")) as f:
+            return float(json.load(f)["workloads"][wl]["flops_per_dof_update"])
+    except Exception:
+        return None
+
+
+def roofline_of(bytes_per_launch, flops_per_launch, avg_s, hbm_gbs, peak_tflops, arith):
+    """Both rooflines of a stage kernel and the binding one (the larger ideal time)."""
+    t_hbm = bytes_per_launch / (hbm_gbs * 1e9)
+    out = {"hbm": {"achieved_gbs": bytes_per_launch / avg_s / 1e9, "peak_gbs": hbm_gbs,
+                   "frac": t_hbm / avg_s}}
+    bound, frac = "hbm", t_hbm / avg_s
+    if flops_per_launch and peak_tflops:
+        t_fl = flops_per_launch / (peak_tflops * 1e12)
+        out["flop"] = {"arith": arith, "achieved_tflops": flops_per_launch / avg_s / 1e12, "peak_tflops": peak_tflops,
+                       "frac": t_fl / avg_s, "flops_per_launch": flops_per_launch}
+        if t_fl > t_hbm:
+            bound, frac = arith, t_fl / avg_s
+    out["binding"] = bound
+    out["binding_frac"] = frac
     return out
 
 
-def main():
+def main():  # noqa: C901
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
@@ -301,6 +350,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
     ap.add_argument("--no-accuracy", action="store_true", help="skip the run to t_end that checks the L1 error")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned-indicator form (profiling runs)")
     ap.add_argument("--schedule", default="auto", choices=["auto", "grid", "persistent"],
                     help="FP32 stage schedule: autotuned (default) or fixed (profiling runs)")
     args = ap.parse_args()
@@ -330,41 +380,58 @@ def main():
     dof_per_step = m.E * 64 * 5
     V = nvars(args.workload)
     mhd = bool(WORKLOADS[args.workload].get("mhd"))
-
-    # ---- the plain FP64 form (the comparison point of the metric)
-    s = Solver(make_cfg(args.workload, abi.PREC_FP64), m, groups)
-    s.upload(u)
-    stream_ptr = ctypes.c_uint64()
-    abi.call("nemo_gpu_stream", ctypes.byref(stream_ptr))
-    stream = torch.cuda.ExternalStream(stream_ptr.value)
-    s.run(nsteps=args.warmup)
-    ms64, st64, n64, tot64, ntot64, _, _ = timed_run(s, args.steps, stream, dist, torch, ctypes, abi)
-    value64 = world * dof_per_step * args.steps / (ms64 * 1e-3)
-    s.finalize()
-
-    # ---- the chosen form: FP32 bulk + learned indicator, FP64 state/register/update/repair/reductions
-    s = make_solver(args.workload, m, abi.PREC_FP32, learned=True, groups=groups)
-    s.upload(u)
-    if args.schedule == "auto":
-        tune_mode, tune_ctas, tune_ms = s.autotune(nsteps=3)   # restores the state it times
-    else:
-        import torch as _t
-        nsm = _t.cuda.get_device_properties(local).multi_processor_count
-        tune_mode, tune_ctas, tune_ms = (0, 0, [-1.0] * 5) if args.schedule == "grid" else (1, 4 * nsm, [-1.0] * 5)
-        s.set_schedule(tune_mode, tune_ctas)
-    abi.call("nemo_gpu_stream", ctypes.byref(stream_ptr))
-    stream = torch.cuda.ExternalStream(stream_ptr.value)
-    s.run(nsteps=args.warmup)
-    with ClockSampler(local) as clk:
-        ms, st_ms_v, st_n_v, tot_ms_v, tot_n_v, t_sim, nst = timed_run(s, args.steps, stream, dist, torch, ctypes,
-                                                                        abi)
-    value = world * dof_per_step * args.steps / (ms * 1e-3)
-
-    # ---- roofline of the stage kernel (HBM): algorithmic bytes per launch / avg launch time
+    has_ind = bool(WORKLOADS[args.workload]["indicator"])
+    peaks = abi.measure_peaks()
+    hbm, hbm_kind = load_peaks()
+    flops_dof = load_flops(args.workload)
     bytes_per_launch = sum(m.E * 64 * V * 8 * (3 if st == 0 else 4) for st in range(5)) / 5.0
-    avg_stage_s = st_ms_v * 1e-3 / max(st_n_v, 1)
-    peak, peak_kind = load_peaks()
-    achieved = bytes_per_launch / avg_stage_s / 1e9
+    flops_per_launch = flops_dof * m.E * 64 if flops_dof else None
+    stream_ptr = ctypes.c_uint64()
+
+    def measure(key, clocks=False):
+        """Time one form: warm-up, K steps with per-kernel events; returns a result dict."""
+        prec, learned = FORMS[key]
+        s = make_solver(args.workload, m, prec, learned, groups)
+        s.upload(u)
+        sched = None
+        if prec == abi.PREC_FP32:
+            if args.schedule == "auto":
+                mode, ctas, tms = s.autotune(nsteps=3)   # restores the state it times
+            else:
+                mode, ctas, tms = (0, 0, [-1.0] * 5) if args.schedule == "grid" else (1, 4 * peaks["sms"], [-1.0] * 5)
+                s.set_schedule(mode, ctas)
+            sched = {"chosen": "persistent" if mode == 1 else "grid", "persistent_ctas": ctas,
+                     "autotune_ms_per_step": {"grid": tms[0], "persistent_1_per_sm": tms[1],
+                                              "persistent_2_per_sm": tms[2], "persistent_3_per_sm": tms[3],
+                                              "persistent_4_per_sm": tms[4]}}
+        abi.call("nemo_gpu_stream", ctypes.byref(stream_ptr))
+        stream = torch.cuda.ExternalStream(stream_ptr.value)
+        s.run(nsteps=args.warmup)
+        clk = ClockSampler(local) if clocks else None
+        if clk:
+            clk.__enter__()
+        ms, st_ms, st_n, tot_ms, tot_n, t_sim, nst = timed_run(s, args.steps, stream, dist, torch, ctypes, abi)
+        if clk:
+            clk.__exit__(None, None, None)
+        avg_s = st_ms * 1e-3 / max(st_n, 1)
+        arith = "fp32" if prec == abi.PREC_FP32 else "fp64"
+        peak_t = peaks["fp32_tflops"] if prec == abi.PREC_FP32 else peaks["fp64_tflops"]
+        r = {"value": world * dof_per_step * args.steps / (ms * 1e-3), "ms": ms, "avg_stage_ms": avg_s * 1e3,
+             "stage_launches": st_n, "launches": tot_n, "t_sim": t_sim, "steps": nst, "schedule": sched,
+             "clocks": clk.summary() if clk else None, "solver": s, "stream": stream,
+             "roofline": roofline_of(bytes_per_launch, flops_per_launch, avg_s, hbm, peak_t, arith)}
+        return r
+
+    res = {"fp64_modal": measure("fp64_modal")}
+    res["fp64_modal"]["solver"].finalize()
+    if has_ind and not args.no_learned:
+        res["fp32_learned"] = measure("fp32_learned")
+        res["fp32_learned"]["solver"].finalize()
+    chosen = res["fp32_modal"] = measure("fp32_modal", clocks=True)
+    s, stream = chosen["solver"], chosen["stream"]
+    value, ms = chosen["value"], chosen["ms"]
+    kname = ("k_stage_mhd<float>" if mhd else ("k_stage_euler32p" if chosen["schedule"]["chosen"] == "persistent"
+                                               else "k_stage_euler32"))
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "stage_traffic.json")
     if os.path.exists(tpath):
@@ -412,6 +479,7 @@ def main():
         cpu = cpu_baseline(args.workload, u, m)
 
     if rank == 0:
+        rf = chosen["roofline"]
         line = {
             "metric": "DOF-updates/s per RK stage",
             "value": value,
@@ -425,39 +493,47 @@ def main():
             "vs_baseline": None,
             "dtype": "f32 flux bulk, f64 state/register/update",
             "data": "synthetic",
-            "config": {"workload": WORKLOADS[args.workload]["desc"], "elements": m.E, "nodes": m.E * 64,
-                       "stages_per_step": 5,
-                       "form": "chosen: FP32 bulk + FP64 accumulation, learned indicator with modal fallback",
-                       "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
-                       "schedule": {"chosen": "persistent" if tune_mode == 1 else "grid", "persistent_ctas": tune_ctas,
-                                    "autotune_ms_per_step": {"grid": tune_ms[0], "persistent_1_per_sm": tune_ms[1],
-                                                             "persistent_2_per_sm": tune_ms[2],
-                                                             "persistent_3_per_sm": tune_ms[3],
-                                                             "persistent_4_per_sm": tune_ms[4]}},
-                       "groups": int(groups.max()) + 1 if groups is not None else 1,
-                       "l2": f"working set (u in/out + register, 3 x {u.nbytes / 1e6:.0f} MB) larger than L2"},
-            "clocks": clk.summary(),
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
-                         "kernel": "k_stage_mhd<float>" if mhd else "k_stage_euler32",
-                         "algorithmic_bytes_per_launch": bytes_per_launch,
-                         "avg_launch_ms": avg_stage_s * 1e3},
+            "config": workload_config(args.workload, m, u),
+            "form": "chosen: FP32 bulk + FP64 state/register/update/repair/reductions, modal indicator",
+            "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
+            "schedule": chosen["schedule"],
+            "groups": int(groups.max()) + 1 if groups is not None else 1,
+            "clocks": chosen["clocks"],
+            "roofline": {"bound": "hbm", "achieved": rf["hbm"]["achieved_gbs"], "peak": hbm, "unit": "GB/s",
+                         "frac": rf["hbm"]["frac"], "traffic": traffic, "peak_source": hbm_kind,
+                         "kernel": kname, "algorithmic_bytes_per_launch": bytes_per_launch,
+                         "avg_launch_ms": chosen["avg_stage_ms"], "flop": rf.get("flop"),
+                         "binding": rf["binding"], "binding_frac": rf["binding_frac"]},
+            "arith_peaks": {"fp64_tflops": peaks["fp64_tflops"], "fp32_tflops": peaks["fp32_tflops"],
+                            "source": "measured in this run (nemo_gpu_measure_peaks: FMA chains on every SM)"},
+            "flops_per_dof_update": flops_dof,
             "e2e": None if e2e_val is None else {
                     "value": e2e_val, "unit": "DOF-updates/s", "h2d_bytes_per_step": nbytes,
                     "d2h_bytes_per_step": nbytes,
                     "note": "per step: upload of the full state from pinned host memory, one time step, "
                             "download of the full state"},
-            "gpu_launches": int(tot_n_v),
-            "sim": {"t": t_sim, "steps": nst},
-            "plain_fp64": {"value": value64, "unit": "DOF-updates/s", "ms_per_step": ms64 / args.steps,
-                           "avg_stage_ms": st64 / max(n64, 1),
-                           "kernel": "k_stage_mhd<double>" if mhd else "k_stage_euler64",
-                           "speedup_of_chosen_form": value / value64},
-            "accuracy": accuracy,
+            "gpu_launches": int(chosen["launches"]),
+            "sim": {"t": chosen["t_sim"], "steps": chosen["steps"]},
         }
+        forms = {}
+        for key, r in res.items():
+            if key == "fp32_modal":
+                continue
+            forms[key] = {"value": r["value"], "unit": "DOF-updates/s", "ms_per_step": r["ms"] / args.steps,
+                          "avg_stage_ms": r["avg_stage_ms"], "schedule": r["schedule"],
+                          "roofline": r["roofline"], "chosen_form_speedup": value / r["value"]}
+        forms["fp64_modal"]["kernel"] = "k_stage_mhd<double>" if mhd else "k_stage_euler64"
+        line["plain_fp64"] = forms.pop("fp64_modal")
+        line["other_forms"] = forms
+        line["accuracy"] = accuracy
         if cpu:
             line["cpu_baseline"] = cpu
-        line["pid"] = pid_block(value / world, None if e2e_val is None else e2e_val / world, value64 / world, cpu)
+        line["pid"] = {"chosen": 1e6 * world / value, "plain_fp64": 1e6 * world / line["plain_fp64"]["value"],
+                       "unit": PID_UNIT, "note": PID_NOTE}
+        if e2e_val:
+            line["pid"]["e2e"] = 1e6 * world / e2e_val
+        if cpu:
+            line["pid"]["cpu_baseline"] = cpu["cores"] * 1e6 / cpu["value"]
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()

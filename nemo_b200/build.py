@@ -23,6 +23,7 @@ SOURCES = {
     "noalloc.cu": ["-fmad=false"],
     "mlp.cu": ["--use_fast_math"],
     "mortar.cu": ["-fmad=false"],
+    "peaks.cu": [],
 }
 
 

@@ -209,7 +209,20 @@ constexpr double LN2_HI = 0x1.62e42feep-1;
 constexpr double LN2_LO = 0x1.a39ef35793c76p-33;
 constexpr double INV_LN2 = 0x1.71547652b82fep+0;
 
+// Build variants (oracle/Makefile): liboracle_libm.so (-DORACLE_LIBM) takes log and exp from the C
+// library, the arithmetic the reference's Fortran gets from its intrinsics, to measure how far the
+// shared IEEE-only construction moves a run; liboracle_count.so (opcount.cpp) counts each call as
+// one operation.
+#ifndef ORACLE_COUNT_LOG
+#define ORACLE_COUNT_LOG()
+#define ORACLE_COUNT_EXP()
+#endif
+
 double own_log(double x) {
+    ORACLE_COUNT_LOG();
+#ifdef ORACLE_LIBM
+    return std::log(x);
+#endif
     if (!(x > 0.0)) return x == 0.0 ? -HUGE_VAL : std::nan("");
     if (std::isinf(x)) return x;
     int shift = 0;
@@ -233,6 +246,10 @@ double own_log(double x) {
 }
 
 double own_exp(double y) {
+    ORACLE_COUNT_EXP();
+#ifdef ORACLE_LIBM
+    return std::exp(y);
+#endif
     if (y != y) return y;
     if (y > 709.78) return HUGE_VAL;
     if (y < -745.2) return 0.0;

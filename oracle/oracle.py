@@ -17,70 +17,87 @@ _dp = ctypes.POINTER(ctypes.c_double)
 _ip = ctypes.POINTER(ctypes.c_int32)
 
 
+# Build variants of the oracle (oracle/Makefile): "" the oracle, "libm" with the C library's log/exp
+# (the reference's intrinsic arithmetic), "count" with the algorithmic operation counter.
+VARIANTS = {"": "liboracle.so", "libm": "liboracle_libm.so", "count": "liboracle_count.so"}
+_VLIB = {}
+
+
 def build(force=False):
-    so = os.path.join(_HERE, "liboracle.so")
-    src = os.path.join(_HERE, "nemo_oracle.cpp")
-    if force or not os.path.exists(so) or os.path.getmtime(so) < os.path.getmtime(src):
+    srcs = [os.path.join(_HERE, f) for f in ("nemo_oracle.cpp", "opcount.cpp", "Makefile")]
+    newest = max(os.path.getmtime(f) for f in srcs)
+    sos = [os.path.join(_HERE, f) for f in VARIANTS.values()]
+    if force or any(not os.path.exists(so) or os.path.getmtime(so) < newest for so in sos):
         subprocess.run(["make", "-C", _HERE, "-B" if force else "all"], check=True,
                        stdout=subprocess.DEVNULL)
-    return so
+    return sos[0]
 
 
-def lib():
+def lib(variant=""):
+    """The oracle's shared library (variant "" / "libm" / "count", see VARIANTS)."""
     global _LIB
+    if variant:
+        if variant not in _VLIB:
+            _VLIB[variant] = _load(os.path.join(_HERE, VARIANTS[variant]))
+        return _VLIB[variant]
     if _LIB is None:
-        so = os.path.join(_HERE, "liboracle.so")
-        if not os.path.exists(so):
-            build()
-        L = ctypes.CDLL(so)
-        L.or_logmean.restype = ctypes.c_double
-        L.or_logmean.argtypes = [ctypes.c_double, ctypes.c_double]
-        L.or_pressure.restype = ctypes.c_double
-        L.or_pressure.argtypes = [_dp, ctypes.c_double]
-        L.or_flux.argtypes = [ctypes.c_int, _dp, _dp, ctypes.c_double]
-        L.or_riemann.argtypes = [ctypes.c_int, ctypes.c_int, _dp, _dp, _dp, ctypes.c_double]
-        L.or_twopoint.argtypes = [ctypes.c_int, ctypes.c_int, _dp, _dp, _dp, ctypes.c_double]
-        L.or_lgl.argtypes = [ctypes.c_int, _dp, _dp]
-        L.or_operators.argtypes = [_dp] * 5
-        L.or_mortar_operators.argtypes = [_dp, _dp]
-        L.or_set_mortars.argtypes = [ctypes.c_int64, ctypes.c_void_p]
-        L.or_remap.argtypes = [ctypes.c_int, ctypes.c_int64, _dp, ctypes.c_int64, ctypes.c_void_p, ctypes.c_double,
-                               ctypes.c_double, _dp]
-        L.or_rk_coeffs.argtypes = [_dp] * 3
-        L.or_alpha.argtypes = [ctypes.c_void_p, ctypes.c_int64, _ip, _dp, _dp, _dp, ctypes.c_int]
-        L.or_rhs.argtypes = [ctypes.c_void_p, ctypes.c_int64, _ip, _dp, _dp, ctypes.c_void_p, _dp,
-                             ctypes.c_int]
-        L.or_timestep.restype = ctypes.c_double
-        L.or_timestep.argtypes = [ctypes.c_void_p, ctypes.c_int64, _dp, _dp, _dp]
-        L.or_stage.restype = ctypes.c_int64
-        L.or_stage.argtypes = [ctypes.c_void_p, ctypes.c_int64, _ip, _dp, ctypes.c_int,
-                               ctypes.c_double, _dp, _dp, ctypes.c_int]
-        L.or_run.restype = ctypes.c_int64
-        L.or_run.argtypes = [ctypes.c_void_p, ctypes.c_int64, _ip, _dp, _dp, ctypes.c_int64,
-                             ctypes.c_double, _dp, ctypes.POINTER(ctypes.c_int64), ctypes.c_int]
-        L.or_totals.argtypes = [ctypes.c_void_p, ctypes.c_int64, _dp, _dp, _dp]
-        L.or_max_threads.restype = ctypes.c_int
-        L.or_log.restype = ctypes.c_double
-        L.or_log.argtypes = [ctypes.c_double]
-        L.or_exp.restype = ctypes.c_double
-        L.or_exp.argtypes = [ctypes.c_double]
-        L.or_set_mlp.argtypes = [_dp, _dp, _dp]
-        L.or_mhd_flux.argtypes = [ctypes.c_int, _dp, _dp, ctypes.c_double, ctypes.c_double, ctypes.c_double]
-        L.or_mhd_riemann.argtypes = [ctypes.c_int, ctypes.c_int, _dp, _dp, _dp, ctypes.c_double, ctypes.c_double, ctypes.c_double]
-        L.or_mhd_twopoint.argtypes = [ctypes.c_int, ctypes.c_int, _dp, _dp, _dp, ctypes.c_double, ctypes.c_double,
-                                      ctypes.c_double]
-        L.or_mhd_nc.argtypes = [ctypes.c_int, _dp, _dp, _dp, _dp, ctypes.c_double, ctypes.c_double]
-        L.or_mhd_pressure.restype = ctypes.c_double
-        L.or_mhd_pressure.argtypes = [_dp, ctypes.c_double, ctypes.c_double]
-        L.or_timestep2.restype = ctypes.c_double
-        L.or_timestep2.argtypes = [ctypes.c_void_p, ctypes.c_int64, _dp, _dp, _dp, _dp]
-        L.or_features.argtypes = [ctypes.c_void_p, ctypes.c_int64, _dp, _dp, ctypes.c_void_p, ctypes.c_int]
-        L.or_mlp_alpha.restype = ctypes.c_double
-        L.or_mlp_alpha.argtypes = [ctypes.c_void_p, _dp]
-        L.or_repair.restype = ctypes.c_int
-        L.or_repair.argtypes = [ctypes.c_void_p, _dp]
-        _LIB = L
+        _LIB = _load(os.path.join(_HERE, VARIANTS[""]))
     return _LIB
+
+
+def _load(so):
+    if not os.path.exists(so):
+        build()
+    L = ctypes.CDLL(so)
+    L.or_logmean.restype = ctypes.c_double
+    L.or_logmean.argtypes = [ctypes.c_double, ctypes.c_double]
+    L.or_pressure.restype = ctypes.c_double
+    L.or_pressure.argtypes = [_dp, ctypes.c_double]
+    L.or_flux.argtypes = [ctypes.c_int, _dp, _dp, ctypes.c_double]
+    L.or_riemann.argtypes = [ctypes.c_int, ctypes.c_int, _dp, _dp, _dp, ctypes.c_double]
+    L.or_twopoint.argtypes = [ctypes.c_int, ctypes.c_int, _dp, _dp, _dp, ctypes.c_double]
+    L.or_lgl.argtypes = [ctypes.c_int, _dp, _dp]
+    L.or_operators.argtypes = [_dp] * 5
+    L.or_mortar_operators.argtypes = [_dp, _dp]
+    L.or_set_mortars.argtypes = [ctypes.c_int64, ctypes.c_void_p]
+    L.or_remap.argtypes = [ctypes.c_int, ctypes.c_int64, _dp, ctypes.c_int64, ctypes.c_void_p, ctypes.c_double,
+                           ctypes.c_double, _dp]
+    L.or_rk_coeffs.argtypes = [_dp] * 3
+    L.or_alpha.argtypes = [ctypes.c_void_p, ctypes.c_int64, _ip, _dp, _dp, _dp, ctypes.c_int]
+    L.or_rhs.argtypes = [ctypes.c_void_p, ctypes.c_int64, _ip, _dp, _dp, ctypes.c_void_p, _dp,
+                         ctypes.c_int]
+    L.or_timestep.restype = ctypes.c_double
+    L.or_timestep.argtypes = [ctypes.c_void_p, ctypes.c_int64, _dp, _dp, _dp]
+    L.or_stage.restype = ctypes.c_int64
+    L.or_stage.argtypes = [ctypes.c_void_p, ctypes.c_int64, _ip, _dp, ctypes.c_int,
+                           ctypes.c_double, _dp, _dp, ctypes.c_int]
+    L.or_run.restype = ctypes.c_int64
+    L.or_run.argtypes = [ctypes.c_void_p, ctypes.c_int64, _ip, _dp, _dp, ctypes.c_int64,
+                         ctypes.c_double, _dp, ctypes.POINTER(ctypes.c_int64), ctypes.c_int]
+    L.or_totals.argtypes = [ctypes.c_void_p, ctypes.c_int64, _dp, _dp, _dp]
+    L.or_max_threads.restype = ctypes.c_int
+    L.or_log.restype = ctypes.c_double
+    L.or_log.argtypes = [ctypes.c_double]
+    L.or_exp.restype = ctypes.c_double
+    L.or_exp.argtypes = [ctypes.c_double]
+    L.or_set_mlp.argtypes = [_dp, _dp, _dp]
+    L.or_mhd_flux.argtypes = [ctypes.c_int, _dp, _dp, ctypes.c_double, ctypes.c_double, ctypes.c_double]
+    L.or_mhd_riemann.argtypes = [ctypes.c_int, ctypes.c_int, _dp, _dp, _dp, ctypes.c_double, ctypes.c_double, ctypes.c_double]
+    L.or_mhd_twopoint.argtypes = [ctypes.c_int, ctypes.c_int, _dp, _dp, _dp, ctypes.c_double, ctypes.c_double,
+                                  ctypes.c_double]
+    L.or_mhd_nc.argtypes = [ctypes.c_int, _dp, _dp, _dp, _dp, ctypes.c_double, ctypes.c_double]
+    L.or_mhd_pressure.restype = ctypes.c_double
+    L.or_mhd_pressure.argtypes = [_dp, ctypes.c_double, ctypes.c_double]
+    L.or_timestep2.restype = ctypes.c_double
+    L.or_timestep2.argtypes = [ctypes.c_void_p, ctypes.c_int64, _dp, _dp, _dp, _dp]
+    L.or_features.argtypes = [ctypes.c_void_p, ctypes.c_int64, _dp, _dp, ctypes.c_void_p, ctypes.c_int]
+    L.or_mlp_alpha.restype = ctypes.c_double
+    L.or_mlp_alpha.argtypes = [ctypes.c_void_p, _dp]
+    L.or_repair.restype = ctypes.c_int
+    L.or_repair.argtypes = [ctypes.c_void_p, _dp]
+    if hasattr(L, "or_opcount_read"):
+        L.or_opcount_read.argtypes = [ctypes.POINTER(ctypes.c_uint64)]
+    return L
 
 
 def _p(a, t=_dp):
@@ -229,29 +246,30 @@ class Oracle:
     """Oracle bound to one configuration and mesh (nbr = per-element face neighbours with the mortar
     encoding of Mesh.neighbors(); mortars = Mesh.mortars() for a 2:1 forest)."""
 
-    def __init__(self, cfg, nbr, delta, nthreads=None, mortars=None):
+    def __init__(self, cfg, nbr, delta, nthreads=None, mortars=None, variant=""):
+        self.lib = lib(variant)              # "": the oracle; "libm" / "count": its build variants
         self.cfg = cfg                       # a nemo_b200.abi.NemoCfg (ctypes struct)
         self.nbr = np.ascontiguousarray(nbr, dtype=np.int32)
         self.delta = _f64(delta)
         self.E = self.nbr.shape[0]
         self.V = int(cfg.n_vars)
-        self.nthreads = nthreads or nthreads_default()
+        self.nthreads = nthreads or int(self.lib.or_max_threads())
         self.mortars = np.ascontiguousarray(np.zeros((0, 6)) if mortars is None else mortars, dtype=np.int32)
         if (self.nbr <= -2).any() and len(self.mortars) == 0:
             raise ValueError("mesh has mortar faces: pass mortars=mesh.mortars()")
 
     @classmethod
-    def for_mesh(cls, cfg, mesh, nthreads=None):
-        return cls(cfg, mesh.neighbors(), mesh.delta, nthreads=nthreads, mortars=mesh.mortars())
+    def for_mesh(cls, cfg, mesh, nthreads=None, variant=""):
+        return cls(cfg, mesh.neighbors(), mesh.delta, nthreads=nthreads, mortars=mesh.mortars(), variant=variant)
 
     def _c(self):
-        lib().or_set_mortars(len(self.mortars), self.mortars.ctypes.data)
+        self.lib.or_set_mortars(len(self.mortars), self.mortars.ctypes.data)
         return ctypes.byref(self.cfg)
 
     def alpha(self, u):
         u = _f64(u)
         a = np.zeros(self.E)
-        lib().or_alpha(self._c(), self.E, _p(self.nbr, _ip), _p(self.delta), _p(u), _p(a), self.nthreads)
+        self.lib.or_alpha(self._c(), self.E, _p(self.nbr, _ip), _p(self.delta), _p(u), _p(a), self.nthreads)
         return a
 
     def rhs(self, u, alpha=None):
@@ -261,37 +279,46 @@ class Oracle:
         if alpha is not None:
             alpha = _f64(alpha)
             ap = alpha.ctypes.data
-        lib().or_rhs(self._c(), self.E, _p(self.nbr, _ip), _p(self.delta), _p(u), ap, _p(r), self.nthreads)
+        self.lib.or_rhs(self._c(), self.E, _p(self.nbr, _ip), _p(self.delta), _p(u), ap, _p(r), self.nthreads)
         return r
 
     def timestep(self, u):
         u = _f64(u)
         lm = ctypes.c_double(0)
-        dt = lib().or_timestep(self._c(), self.E, _p(self.delta), _p(u), ctypes.byref(lm))
+        dt = self.lib.or_timestep(self._c(), self.E, _p(self.delta), _p(u), ctypes.byref(lm))
         return dt, lm.value
 
     def timestep2(self, u):
         """dt, max wave speed, max velocity component (MHD cleaning speed inputs)."""
         u = _f64(u)
         lm, vm = ctypes.c_double(0), ctypes.c_double(0)
-        dt = lib().or_timestep2(self._c(), self.E, _p(self.delta), _p(u), ctypes.byref(lm), ctypes.byref(vm))
+        dt = self.lib.or_timestep2(self._c(), self.E, _p(self.delta), _p(u), ctypes.byref(lm), ctypes.byref(vm))
         return dt, lm.value, vm.value
 
     def stage(self, u, reg, stage, dt):
         """In place on u and reg (float64 C-contiguous); stage is 0-based."""
-        return lib().or_stage(self._c(), self.E, _p(self.nbr, _ip), _p(self.delta), stage, dt, _p(u), _p(reg),
+        return self.lib.or_stage(self._c(), self.E, _p(self.nbr, _ip), _p(self.delta), stage, dt, _p(u), _p(reg),
                               self.nthreads)
 
     def run(self, u, nsteps=0, t_end=0.0, t0=0.0):
         u = _f64(u).copy()
         t = ctypes.c_double(t0)
         nbad = ctypes.c_int64(0)
-        steps = lib().or_run(self._c(), self.E, _p(self.nbr, _ip), _p(self.delta), _p(u), int(nsteps),
+        steps = self.lib.or_run(self._c(), self.E, _p(self.nbr, _ip), _p(self.delta), _p(u), int(nsteps),
                              float(t_end), ctypes.byref(t), ctypes.byref(nbad), self.nthreads)
         return u, t.value, int(steps), int(nbad.value)
 
     def totals(self, u):
         u = _f64(u)
         out = np.zeros(10)
-        lib().or_totals(self._c(), self.E, _p(self.delta), _p(u), _p(out))
+        self.lib.or_totals(self._c(), self.E, _p(self.delta), _p(u), _p(out))
         return out[: self.V]
+
+    def opcounts(self):
+        """Counted operations since the last reset (variant "count" only): dict by kind."""
+        out = (ctypes.c_uint64 * 6)()
+        self.lib.or_opcount_read(out)
+        return dict(zip(("add", "mul", "div", "sqrt", "log", "exp"), [int(x) for x in out]))
+
+    def opcount_reset(self):
+        self.lib.or_opcount_reset()

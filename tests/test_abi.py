@@ -100,3 +100,10 @@ def test_mesh_generator_invariants():
     mb = mesh.brick(3, 3, 3, periodic=(False, True, False))
     nb = mb.neighbors()
     assert (nb[:, 0] == -1).sum() == 9 and (nb[:, 1] == -1).sum() == 9 and (nb[:, 2] >= 0).all()
+
+
+def test_host_only_cfg_matches_library_defaults(lib):
+    """abi.cfg_struct (used where only the oracle runs) equals nemo_gpu_default_cfg field by field."""
+    a, b = abi.cfg_struct(), abi.default_cfg()
+    for name, _ in abi.NemoCfg._fields_:
+        assert getattr(a, name) == getattr(b, name), name

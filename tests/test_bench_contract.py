@@ -23,3 +23,14 @@ def test_reference_arm_json_line():
     assert "workload" in line["config"]
     # the reference driver's performance index: microseconds per node-stage per core
     assert abs(line["pid"]["cpu"] - cb["cores"] * 1e6 / line["value"]) < 1e-9 * line["pid"]["cpu"]
+
+
+def test_reference_arm_does_not_load_the_cuda_library():
+    """The reference arm runs the oracle only: libnemo_gpu.so must not be mapped into its process."""
+    code = (
+        "import sys, types; sys.argv = ['bench.py', '--impl', 'reference', '--workload', 'wave16', '--steps', '1',"
+        " '--warmup', '0']; sys.path.insert(0, '.'); import bench; bench.main();"
+        " maps = open('/proc/self/maps').read(); print('LOADED' if 'libnemo_gpu.so' in maps else 'CLEAN')")
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=600, cwd=ROOT)
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert r.stdout.strip().splitlines()[-1] == "CLEAN"
