@@ -220,6 +220,26 @@ int nemo_gpu_run(int64_t nsteps, double t_end, double* t_out, int64_t* steps_out
    state, without updating it (source/kernel/mcfv/3d/kernel_flux_mod.f90:280-500). */
 int nemo_gpu_rhs(double* rhs_host);
 
+/* AMR operator matrices for hosts that transfer quad payloads themselves (the setups' replace
+   callbacks, source/setups/euler/3d/sedov/setup_amr_mod.f90:67-125, through kernel_share_mod's
+   refineMat / coarseMat): Fortran-layout arrays (n, n, 3, 8, 0:qmax), first index fastest.
+   refine(:,:,d,f,q) maps a parent's nodal values along direction d to child f's (f = cx + 2 cy +
+   4 cz, 0-based here, p4est child order) after truncating the parent to its Legendre modes 0..q
+   in that direction; coarsen(:,:,d,f,q) maps child f's nodal values to its L2 projection onto the
+   parent (Gauss-Lobatto quadrature), truncated the same way; summing blockmulXYZ(coarsen(..f..))
+   over the 8 children gives the parent.  At q = n-1 these are the interpolation and projection of
+   nemo_gpu_adapt; q = 0 gives element means.  0 <= qmax <= n-1; either output may be NULL. */
+int nemo_gpu_amr_operators(int32_t n, int32_t qmax, double* refine, double* coarsen);
+
+/* Positivity repair of n element states held by the host (kernel_repair of a per-quad host shim,
+   source/kernel/mcfv/3d/kernel_validate_mod.f90:27-157): each element [n_vars][64] at a byte
+   stride from the previous one (sizeof(quad_t) for quad%pld%hydro%state) is checked and, if a node
+   is inadmissible, repaired on the device by the stage kernels' dgfv_repair_3d; the states are
+   written back in place and ok_host[e] = 1 if element e is admissible afterwards.  Returns
+   NEMO_ERR_REPAIR if any element stays inadmissible (as the reference raises an error).  Needs
+   nemo_gpu_init; allocates and frees a device buffer per call (a slow path, not for the stage). */
+int nemo_gpu_repair_states(double* host, int64_t n, int64_t elem_stride_bytes, int32_t* ok_host);
+
 /* Blending coefficient alpha per element (host array [E]) of the current state. */
 int nemo_gpu_alpha(double* alpha_host);
 

@@ -31,7 +31,8 @@ EXPORTS = [
     "nemo_gpu_autotune", "nemo_gpu_set_schedule", "nemo_gpu_set_owned", "nemo_gpu_pack_elements",
     "nemo_gpu_unpack_elements", "nemo_gpu_adapt", "nemo_gpu_amr_flags",
     "nemo_gpu_checkpoint_begin", "nemo_gpu_checkpoint_wait", "nemo_gpu_set_time",
-    "nemo_gpu_pack_faces", "nemo_gpu_unpack_faces", "nemo_gpu_measure_peaks",
+    "nemo_gpu_pack_faces", "nemo_gpu_unpack_faces", "nemo_gpu_measure_peaks", "nemo_gpu_amr_operators",
+    "nemo_gpu_repair_states",
 ]
 
 
@@ -92,6 +93,8 @@ def load(path=LIB_PATH):
                                    ctypes.POINTER(i64)],
         "nemo_gpu_stream": [ctypes.POINTER(ctypes.c_uint64)],
         "nemo_gpu_measure_peaks": [vp],
+        "nemo_gpu_amr_operators": [i32, i32, vp, vp],
+        "nemo_gpu_repair_states": [vp, i64, i64, vp],
         "nemo_gpu_totals_noalloc": [vp, vp, i64, i64, i32, vp, ctypes.c_uint64],
         "nemo_gpu_set_mlp": [vp, i32, vp, vp],
         "nemo_gpu_features": [vp, vp],
@@ -150,6 +153,17 @@ def measure_peaks():
     call("nemo_gpu_measure_peaks", out.ctypes.data)
     return {"fp64_tflops": float(out[0]), "fp32_tflops": float(out[1]), "sms": int(out[2]),
             "sm_max_mhz": float(out[3])}
+
+
+def amr_operators(qmax=3):
+    """(refine, coarsen) as [q][f][d][i][j] numpy arrays (the C side writes the Fortran layout
+    (n, n, 3, 8, 0:qmax), i fastest)."""
+    n = 4
+    r = np.zeros((qmax + 1) * 8 * 3 * n * n)
+    c = np.zeros_like(r)
+    call("nemo_gpu_amr_operators", n, int(qmax), r.ctypes.data, c.ctypes.data)
+    shape = (qmax + 1, 8, 3, n, n)   # C order of the Fortran (i, j, d, f, q) array is (q, f, d, j, i)
+    return r.reshape(shape).transpose(0, 1, 2, 4, 3), c.reshape(shape).transpose(0, 1, 2, 4, 3)
 
 
 def cfg_struct(**kw):

@@ -71,6 +71,8 @@ cudaError_t launch_stage_euler64(const StageArgs& a, bool blend, bool ind, bool 
 cudaError_t launch_totals64(const double* u, const double* delta, int64_t E, int64_t n, int nv, double* part,
                             double* out, cudaStream_t s);
 int stage_smem_bytes64();
+// positivity repair of element states [n][nv][64] (one element per warp), ok[e] = admissible after
+cudaError_t launch_repair_states64(double* st, int64_t n, int nv, int mhd, int32_t* ok, cudaStream_t s);
 
 // FP32-bulk Euler path (stage_fp32.cu)
 cudaError_t setup_stage_euler32(const OpConsts& ops);

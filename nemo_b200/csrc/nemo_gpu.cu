@@ -476,6 +476,68 @@ int nemo_gpu_mortar_operators(int32_t n, double* prolong, double* project) {
     return NEMO_OK;
 }
 
+int nemo_gpu_amr_operators(int32_t n, int32_t qmax, double* refine, double* coarsen) {
+    if (n != NN) return fail(NEMO_ERR_ARG, "only n = %d Gauss-Lobatto nodes are compiled (got %d)", NN, n);
+    if (qmax < 0 || qmax > NN - 1) return fail(NEMO_ERR_ARG, "qmax must be in [0, %d] (got %d)", NN - 1, qmax);
+    HostOps h;
+    build_host_ops(h);
+    for (int q = 0; q <= qmax; ++q) {
+        // nodal filter to the Legendre modes 0..q of one direction: P = V diag(m <= q) Vinv
+        double P[NN * NN];
+        for (int i = 0; i < NN; ++i)
+            for (int j = 0; j < NN; ++j) {
+                double acc = 0.0;
+                for (int m = 0; m <= q; ++m) acc = acc + h.V[i * NN + m] * h.Vinv[m * NN + j];
+                P[i * NN + j] = acc;
+            }
+        for (int f = 0; f < 8; ++f)
+            for (int d = 0; d < 3; ++d) {
+                const int s = (f >> d) & 1;   // child f = cx + 2 cy + 4 cz: its half in direction d
+                for (int i = 0; i < NN; ++i)
+                    for (int j = 0; j < NN; ++j) {
+                        double r = 0.0, c = 0.0;
+                        for (int m = 0; m < NN; ++m) {
+                            r = r + h.pro[s][i * NN + m] * P[m * NN + j];
+                            c = c + P[i * NN + m] * h.prj[s][m * NN + j];
+                        }
+                        // Fortran layout (N, N, 3, 8, 0:qmax), first index fastest
+                        const size_t o = (size_t)i + NN * ((size_t)j + NN * ((size_t)d + 3 * ((size_t)f + 8 * (size_t)q)));
+                        if (refine) refine[o] = r;
+                        if (coarsen) coarsen[o] = c;
+                    }
+            }
+    }
+    return NEMO_OK;
+}
+
+int nemo_gpu_repair_states(double* host, int64_t n, int64_t stride, int32_t* ok_host) {
+    if (!g.inited) return fail(NEMO_ERR_STATE, "call nemo_gpu_init first");
+    if (n < 0 || (n > 0 && (!host || !ok_host))) return fail(NEMO_ERR_ARG, "bad repair arguments");
+    if (n == 0) return NEMO_OK;
+    const size_t row = sizeof(double) * (size_t)g.V * NP;
+    if (stride < (int64_t)row) return fail(NEMO_ERR_ARG, "element stride %lld < %zu bytes", (long long)stride, row);
+    double* dst = nullptr;
+    int32_t* dok = nullptr;
+    cudaError_t err = cudaMalloc(&dst, row * (size_t)n);
+    if (err == cudaSuccess) err = cudaMalloc(&dok, sizeof(int32_t) * (size_t)n);
+    if (err == cudaSuccess)
+        err = cudaMemcpy2DAsync(dst, row, host, (size_t)stride, row, (size_t)n, cudaMemcpyHostToDevice, g.stream);
+    if (err == cudaSuccess) err = launch_repair_states64(dst, n, g.V, is_mhd() ? 1 : 0, dok, g.stream);
+    if (err == cudaSuccess)
+        err = cudaMemcpy2DAsync(host, (size_t)stride, dst, row, row, (size_t)n, cudaMemcpyDeviceToHost, g.stream);
+    if (err == cudaSuccess)
+        err = cudaMemcpyAsync(ok_host, dok, sizeof(int32_t) * (size_t)n, cudaMemcpyDeviceToHost, g.stream);
+    if (err == cudaSuccess) err = cudaStreamSynchronize(g.stream);
+    if (dst) cudaFree(dst);
+    if (dok) cudaFree(dok);
+    if (err != cudaSuccess) return fail(NEMO_ERR_CUDA, "%s", cudaGetErrorString(err));
+    int64_t nbad = 0;
+    for (int64_t e = 0; e < n; ++e) nbad += ok_host[e] ? 0 : 1;
+    if (nbad) return fail(NEMO_ERR_REPAIR, "%lld of %lld elements stay inadmissible after the repair", (long long)nbad,
+                          (long long)n);
+    return NEMO_OK;
+}
+
 int nemo_gpu_operators(int32_t n, double* nodes, double* weights, double* dmat, double* smat, double* vinv) {
     if (n != NN) return fail(NEMO_ERR_ARG, "only n = %d Gauss-Lobatto nodes are compiled (got %d)", NN, n);
     HostOps h;

@@ -650,6 +650,43 @@ cudaError_t setup_stage_mhd64() {
     return cudaFuncSetAttribute(k_stage_mhd<double, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
 }
 
+// Positivity repair of element states held outside the library (the per-quad kernel_repair of a
+// host, source/kernel/mcfv/3d/kernel_validate_mod.f90:27-157): one warp per element [nv][64] (the
+// Fortran state(n,n,n,nv) layout); if a node is inadmissible, lanes 0..15 run the cooperative
+// dgfv_repair_3d of the stage kernels on it.  ok[e] = 1 if the element is admissible afterwards.
+__global__ void __launch_bounds__(32) k_repair_states64(double* __restrict__ st, int64_t n, int nv, int is_mhd,
+                                                        int32_t* __restrict__ ok) {
+    __shared__ double su[VMAX * NP];
+    const OpConsts& k = c_ops64;
+    const int64_t e = blockIdx.x;
+    const int lane = threadIdx.x;
+    double* g = st + e * (int64_t)nv * NP;
+    for (int p = lane; p < nv * NP; p += 32) su[p] = g[p];
+    __syncwarp();
+    bool valid = true;
+    for (int p = lane; p < NP; p += 32) {
+        double q[VMAX];
+        for (int v = 0; v < nv; ++v) q[v] = su[v * NP + p];
+        valid = valid && (is_mhd ? m_isvalid<double>(q, k.kappa, k.mu0) : isvalid64(q, k));
+    }
+    bool good = __all_sync(0xffffffffu, valid);
+    if (!good) {
+        bool rep = false;
+        if (lane < 16) rep = is_mhd ? repair_elem16_mhd<1>(su, 0, lane, k) : repair_elem16<1>(su, 0, lane, k);
+        good = __shfl_sync(0xffffffffu, rep, 0);
+        __syncwarp();
+        for (int p = lane; p < nv * NP; p += 32) g[p] = su[p];
+    }
+    if (lane == 0) ok[e] = good ? 1 : 0;
+}
+
+cudaError_t launch_repair_states64(double* st, int64_t n, int nv, int mhd, int32_t* ok, cudaStream_t s) {
+    if (n <= 0) return cudaSuccess;
+    if (n > 0x7fffffffLL) return cudaErrorInvalidValue;
+    k_repair_states64<<<(unsigned)n, 32, 0, s>>>(st, n, nv, mhd, ok);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_stage_mhd64(const StageArgs& a, bool blend, bool rhs_only, cudaStream_t s) {
     const int grid = (int)((a.E_own + mhd::EPC - 1) / mhd::EPC);
     const int smem = stage_smem_bytes_mhd64();

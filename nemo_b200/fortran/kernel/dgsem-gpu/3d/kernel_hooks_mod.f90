@@ -15,7 +15,8 @@ subroutine hook_init_400
 
     use iso_c_binding
     use nemo_gpu_interfaces_mod
-    use kernel_share_mod, only: nodes, weights, gpu_cfg
+    use kernel_share_mod, only: nodes, weights, gpu_cfg, kernel_share_amr_operators
+    use kernel_config_mod, only: repair_decr
     use setup_config_mod, only: kappa, CFL
 
     real(c_double) :: x(N_NODES), w(N_NODES), dmat(N_NODES**2), smat(N_NODES**2), vinv(N_NODES**2)
@@ -23,6 +24,7 @@ subroutine hook_init_400
     call nemo_gpu_check(nemo_gpu_default_cfg(gpu_cfg), 'default_cfg')
     gpu_cfg%kappa = kappa
     gpu_cfg%cfl = CFL
+    gpu_cfg%repair_decr = repair_decr
 # ifdef PP_KERNEL_GPU_PRECISION
     gpu_cfg%precision = PP_KERNEL_GPU_PRECISION
 # endif
@@ -36,6 +38,8 @@ subroutine hook_init_400
     call nemo_gpu_check(nemo_gpu_operators(int(N_NODES,c_int), x, w, dmat, smat, vinv), 'operators')
     nodes = 0.5_dp * x
     weights = 0.5_dp * w
+
+    call kernel_share_amr_operators()
 
 end subroutine
 
@@ -62,7 +66,8 @@ subroutine hook_pre_rk_timestep_300
 
 end subroutine
 
-!! The setups' analyze and checkpoint hooks read quad%pld%hydro%state: bring it back first.
+!! The setups' analyze and checkpoint hooks read quad%pld%hydro%state (and aux%hydro%blend): bring
+!! them back first.
 subroutine hook_analyze_100
 
     use kernel_share_mod, only: kernel_share_download
@@ -73,10 +78,44 @@ end subroutine
 
 subroutine hook_checkpoint_100
 
-    use kernel_share_mod, only: kernel_share_download
+    use kernel_share_mod, only: kernel_share_download, kernel_share_blend
 
     call kernel_share_download()
+    call kernel_share_blend()
 
 end subroutine
+
+# ifdef PP_KERNEL_GPU_AMR_SYNC
+!! Setups that adapt the forest with their own replace callbacks on the host (hook_pre_timestep_300,
+!! source/setups/euler/3d/sedov/setup_amr_mod.f90:7-21, every amr_each_ntimesteps steps): the state
+!! comes back to the quads before, and the new forest and its state go to the device after.  Setups
+!! that adapt through nemo_gpu_amr_flags / nemo_gpu_adapt leave PP_KERNEL_GPU_AMR_SYNC undefined.
+subroutine hook_pre_timestep_290
+
+    use share_mod, only: rt => runtime
+    use setup_config_mod, only: amr_each_ntimesteps
+    use kernel_share_mod, only: kernel_share_download
+
+    if (mod(rt%timesteps,amr_each_ntimesteps) == 0) call kernel_share_download()
+
+end subroutine
+
+subroutine hook_pre_timestep_310
+
+    use iso_c_binding
+    use share_mod, only: rt => runtime
+    use setup_config_mod, only: amr_each_ntimesteps
+    use kernel_share_mod, only: kernel_share_set_mesh, kernel_share_upload
+    use nemo_gpu_interfaces_mod
+
+    if (mod(rt%timesteps,amr_each_ntimesteps) == 0) then
+        call kernel_share_set_mesh()
+        call kernel_share_upload()
+        !! the upload starts a new run on the device: carry the time over
+        call nemo_gpu_check(nemo_gpu_set_time(real(rt%simtime,c_double), int(rt%timesteps,c_int64_t)), 'set_time')
+    end if
+
+end subroutine
+# endif
 
 end module

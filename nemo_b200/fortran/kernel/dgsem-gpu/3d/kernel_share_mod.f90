@@ -1,13 +1,22 @@
 !! GPU kernel module, shared data: the symbols other modules import from kernel_share_mod
-!! (nodes, weights, dtmin, lmax) plus the host<->device synchronisation of the quad states.
+!! (nodes, weights, dtmin, lmax, refineMat, coarseMat) plus the host<->device synchronisation of the
+!! quad states.
 
 module kernel_share_mod
 
 use constants_mod
+use kernel_const_mod, only: DGFV_QMAX
 use nemo_gpu_interfaces_mod, only: nemo_cfg_t
 
 real(dp), save :: nodes(N_NODES)
 real(dp), save :: weights(N_NODES)
+
+!! AMR transfer operators of the setups' replace callbacks (nemo_gpu_amr_operators): for child f
+!! (p4est order) and direction d, refineMat(:,:,d,f,q) maps the parent's nodal values to the child's
+!! after truncating the parent to its Legendre modes 0..q; coarseMat(:,:,d,f,q) maps the child's
+!! nodal values to its projection onto the parent, truncated the same way.
+real(dp), save :: refineMat(N_NODES,N_NODES,3,8,0:DGFV_QMAX)
+real(dp), save :: coarseMat(N_NODES,N_NODES,3,8,0:DGFV_QMAX)
 
 real(dp), save :: dtmin
 real(dp), save :: lmax
@@ -15,6 +24,34 @@ real(dp), save :: lmax
 type(nemo_cfg_t), save :: gpu_cfg
 
 contains
+
+subroutine kernel_share_amr_operators
+
+    use iso_c_binding
+    use nemo_gpu_interfaces_mod
+
+    call nemo_gpu_check(nemo_gpu_amr_operators(int(N_NODES,c_int32_t), int(DGFV_QMAX,c_int32_t), &
+        refineMat, coarseMat), 'amr_operators')
+
+end subroutine
+
+!! The quads' blending coefficients (aux%hydro%blend) from the device, for the setups' output.
+subroutine kernel_share_blend
+
+    use iso_c_binding
+    use share_mod, only: mesh
+    use nemo_gpu_interfaces_mod
+
+    real(c_double), allocatable :: alpha(:)
+    integer(kind=8) :: i
+
+    allocate(alpha(mesh%nquads))
+    call nemo_gpu_check(nemo_gpu_alpha(alpha), 'alpha')
+    do i = 1,mesh%nquads
+        mesh%quads(i)%aux%hydro%blend = alpha(i)
+    end do
+
+end subroutine
 
 !! side_t / quad_t -> the C side arrays (0-based ids and face ids, source/mesh/p4est/mesh_types_mod.f90:30-77)
 subroutine kernel_share_set_mesh

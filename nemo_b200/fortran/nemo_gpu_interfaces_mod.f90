@@ -207,6 +207,31 @@ interface
         integer(c_int64_t), value :: n
         integer(c_int) :: st
     end function
+
+    !! Blending coefficient per quad of the current state (host array alpha(nquads)).
+    function nemo_gpu_alpha(alpha) result(st) bind(c, name="nemo_gpu_alpha")
+        import :: c_int, c_double
+        real(c_double), intent(out) :: alpha(*)
+        integer(c_int) :: st
+    end function
+
+    !! refineMat / coarseMat (n, n, 3, 8, 0:qmax) of kernel_share_mod for the setups' replace callbacks.
+    function nemo_gpu_amr_operators(n, qmax, refine, coarsen) result(st) bind(c, name="nemo_gpu_amr_operators")
+        import :: c_int, c_int32_t, c_double
+        integer(c_int32_t), value :: n, qmax
+        real(c_double), intent(out) :: refine(*), coarsen(*)
+        integer(c_int) :: st
+    end function
+
+    !! Positivity repair of host-held quad states (n of them, elem_stride_bytes apart), in place on the
+    !! device; ok(e) = 1 if quad e is admissible afterwards (kernel_repair).
+    function nemo_gpu_repair_states(host, n, elem_stride_bytes, ok) result(st) bind(c, name="nemo_gpu_repair_states")
+        import :: c_int, c_int32_t, c_int64_t, c_ptr
+        type(c_ptr), value :: host
+        integer(c_int64_t), value :: n, elem_stride_bytes
+        integer(c_int32_t), intent(out) :: ok(*)
+        integer(c_int) :: st
+    end function
 end interface
 
 contains

@@ -107,3 +107,40 @@ def test_host_only_cfg_matches_library_defaults(lib):
     a, b = abi.cfg_struct(), abi.default_cfg()
     for name, _ in abi.NemoCfg._fields_:
         assert getattr(a, name) == getattr(b, name), name
+
+
+def test_amr_operators_are_the_adapt_interpolation_and_projection(lib):
+    """refineMat/coarseMat for hosts' replace callbacks: at q = N the 1D factors are the mortar
+    prolongation/projection of the child's half; lower q truncate to Legendre modes 0..q (q = 0:
+    the element mean)."""
+    R, C = abi.amr_operators(3)
+    pro, prj = abi.mortar_operators()
+    x, w, D, S, Vi = abi.operators()
+    V = np.linalg.inv(Vi)
+    for f in range(8):
+        for d in range(3):
+            s = (f >> d) & 1
+            np.testing.assert_allclose(R[3, f, d], pro[s], atol=1e-14)
+            np.testing.assert_allclose(C[3, f, d], prj[s], atol=1e-14)
+            for q in range(4):
+                P = V[:, : q + 1] @ Vi[: q + 1, :]
+                np.testing.assert_allclose(R[q, f, d], pro[s] @ P, atol=1e-13)
+                np.testing.assert_allclose(C[q, f, d], P @ prj[s], atol=1e-13)
+    # refining then projecting back keeps the integral (Gauss-Lobatto quadrature is exact to degree 5
+    # on each half) and constants (the projection is not the identity: the quadrature is not exact
+    # for the degree-6 products of the projection)
+    back = C[3, 0, 0] @ R[3, 0, 0] + C[3, 1, 0] @ R[3, 1, 0]
+    np.testing.assert_allclose(w @ back, w, atol=1e-14)
+    np.testing.assert_allclose(back @ np.ones(4), np.ones(4), atol=1e-14)
+    mean = np.outer(np.ones(4), w / 2.0)
+    np.testing.assert_allclose(R[0, 5, 1], mean, atol=1e-14)
+    rc = lib.nemo_gpu_amr_operators(4, 4, None, None)
+    assert rc == 1 and "qmax" in abi.last_error()
+
+
+def test_repair_states_needs_init(lib):
+    ok = np.zeros(1, dtype=np.int32)
+    st = np.zeros((1, 5, 64))
+    abi.call("nemo_gpu_finalize")
+    rc = lib.nemo_gpu_repair_states(abi.ptr(st), 1, 5 * 64 * 8, abi.ptr(ok))
+    assert rc == 2 and "init" in abi.last_error()
