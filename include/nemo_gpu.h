@@ -178,11 +178,49 @@ int nemo_gpu_unpack_elements(const int32_t* idx_dev, int64_t n, const double* bu
 int nemo_gpu_pack_faces(const int32_t* idx_dev, const int32_t* face_dev, int64_t n, double* buf_dev);
 int nemo_gpu_unpack_faces(const int32_t* idx_dev, const int32_t* face_dev, int64_t n, const double* buf_dev);
 
+/* A stage in two parts, so that a partitioned host overlaps its ghost exchange with work: with the
+   owned elements ordered so that [0, n_interior) read no ghost data (neither a conforming neighbour
+   nor a quad of a 2:1 mortar is a ghost), nemo_gpu_stage_interior enqueues the stage for those
+   elements and returns at once; the host refreshes the ghosts (its own exchange, then
+   nemo_gpu_unpack_faces / _elements), and nemo_gpu_stage_boundary advances the rest, waits, and
+   reports as nemo_gpu_stage.  The two parts give the results of nemo_gpu_stage bit for bit (each
+   element's update reads only its own state and its neighbours' traces).  n_interior = 0 (the
+   default, and after nemo_gpu_set_owned) runs everything in the boundary part.  Needs the grid
+   stage schedule.  The reference exchanges first and then computes
+   (source/mesh/p4est/mesh_utils_mod.f90:650-664, source/timedisc/rungekutta/timedisc_evolve_mod.f90:20-84). */
+int nemo_gpu_set_interior(int64_t n_interior);
+int nemo_gpu_stage_interior(int32_t stage, double dt);
+int nemo_gpu_stage_boundary(int32_t stage, double dt, int32_t* nbad_out);
+
+/* GLM-MHD on partitioned hosts: the wave-speed and velocity maxima of the state's CFL evaluation
+   (after nemo_gpu_calc_timestep) and the cleaning speed / damping of the coming step, which a
+   partitioned host sets from the all-reduced maxima, c_h = 2 |lmax - vmax|, alpha = c_h / 0.18
+   (source/kernel/mcfv/3d/kernel_timestep_mod.f90:48-52, :338-344). */
+int nemo_gpu_glm_speeds(double* lmax_out, double* vmax_out);
+int nemo_gpu_set_glm(double ch, double alpha);
+
 /* Copy the conserved state host->device.  host points at the first element's state(1,1,1,1);
    consecutive elements are elem_stride_bytes apart (sizeof(quad_t) when the state sits in the
    reference's quad_t array, n^3*V*8 for a packed [E][V][n^3] array).  Resets the RK register. */
 int nemo_gpu_upload_state(const double* host, int64_t elem_stride_bytes);
 int nemo_gpu_download_state(double* host, int64_t elem_stride_bytes);
+
+/* Asynchronous form of nemo_gpu_upload_state for hosts that stream independent states through the
+   library (ensemble members, parameter sweeps, a state per step): the host->device copy runs on the
+   library's upload stream into one of two staging slots and returns at once; the library stream
+   takes the new state in stream order (work enqueued before the call still sees the old state, work
+   enqueued after it the new one, as a new run: time 0, register cleared).  So the copy of the next
+   state overlaps the stage work of the current one and, with nemo_gpu_checkpoint_begin as the
+   asynchronous download, the copy of its result.  host must be pinned (cudaHostAlloc or
+   cudaHostRegister) for the copy to be asynchronous, and must not be modified before
+   nemo_gpu_upload_wait returns (or before the second-next call of this function, which reuses the
+   slot).  Same layout and stride rules as nemo_gpu_upload_state.  No reference counterpart: the
+   reference's state lives in host memory. */
+int nemo_gpu_upload_state_async(const double* host, int64_t elem_stride_bytes);
+
+/* Wait until the host->device copies of every asynchronous upload have finished (their host
+   buffers may then be reused). */
+int nemo_gpu_upload_wait(void);
 
 /* Checkpoint staging (the state that hook_checkpoint_fill writes, source/checkpoint/flash/
    checkpoint_mod.f90:319-364, and the restart that source/nemo_prog.f90:107-114 leaves as a TODO).
@@ -207,6 +245,18 @@ int nemo_gpu_calc_timestep(double cfl, double* dt_out, double* lmax_out);
    state, register update, state update, positivity repair.  stage is 1..5 as rt%rkstage.
    nbad_out (may be NULL) receives the number of elements whose repair failed. */
 int nemo_gpu_stage(int32_t stage, double dt, double t_stage, int32_t* nbad_out);
+
+/* Enqueue nsteps full time steps with the device-side dt (as nemo_gpu_run without an end time) on
+   the library stream and return without waiting: with nemo_gpu_upload_state_async before and
+   nemo_gpu_checkpoint_begin after it, a host streams states through the library with the copies of
+   one state overlapping the steps of another.  Errors the device reports while these steps run
+   (bounded waits, a non-finite dt) come back from the next nemo_gpu_sync or nemo_gpu_run; repair
+   failures are counted in nemo_gpu_status.  Not in timing mode.  No reference counterpart. */
+int nemo_gpu_run_async(int64_t nsteps);
+
+/* Wait for all work the library has enqueued (steps, asynchronous uploads and checkpoint copies)
+   and return the status the device reported for it. */
+int nemo_gpu_sync(void);
 
 /* One full time step (5 stages) with the given dt, replayed from a captured CUDA graph. */
 int nemo_gpu_step(double dt);

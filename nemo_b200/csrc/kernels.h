@@ -11,7 +11,9 @@ namespace nemo {
 
 struct StageArgs {
     int64_t E;                // element stride of the SoA arrays
-    int64_t E_own;            // elements processed: [0, E_own); [E_own, E) are ghost copies (neighbour data)
+    int64_t E_begin;          // first element of this launch (0, or the first partition-boundary element)
+    int64_t E_own;            // end of this launch's elements, at most the owned count ([owned, E) are
+                              // ghost copies: neighbour data only)
     const double* u_in;       // [V][E][64]
     double* u_out;            // [V][E][64]
     double* reg;              // [V][E][64] LSRK register (FP64)
@@ -31,6 +33,7 @@ struct StageArgs {
     int32_t surface_flux;
     int32_t volume_flux;
     int32_t prep_only;        // only the epilogue on u_in (indicator and CFL bound of a state)
+    int32_t tick;             // this launch advances t and the step counter after the last stage
     const double* mlp64;      // learned indicator (FP64 values of the BF16 weights) or null
     const float* mlp32;       // same, FP32
     const float* mlp32t;      // FP32, W1 and W2 transposed (MLP_NT floats, 16-byte aligned)

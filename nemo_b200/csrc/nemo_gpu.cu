@@ -178,6 +178,9 @@ struct Lib {
 
     int64_t E = 0;
     int64_t E_own = 0;            // elements advanced by this process; [E_own, E) are ghost copies
+    int64_t n_interior = 0;       // owned elements [0, n_interior) read no ghost data (0: no split)
+    bool split_open = false;      // a stage's interior part is enqueued, its boundary part not yet
+    unsigned long long nbad_mark = 0;  // repair-failure count before the open split stage (host copy)
     int V = 5;
     bool has_mesh = false, has_state = false;
     int ngroups = 1;
@@ -228,6 +231,17 @@ struct Lib {
     cudaStream_t copy_stream = nullptr;
     cudaEvent_t ckpt_ready = nullptr, ckpt_done = nullptr;
     bool ckpt_pending = false;
+
+    // asynchronous uploads (nemo_gpu_upload_state_async): two AoS staging slots filled on their
+    // own stream, consumed in stream order by the library stream; per slot a pinned control block
+    cudaStream_t in_stream = nullptr;
+    double* in_stage[2] = {nullptr, nullptr};
+    int64_t in_bytes = 0;
+    cudaEvent_t in_done[2] = {nullptr, nullptr};   // host->device copy of the slot finished
+    cudaEvent_t in_free[2] = {nullptr, nullptr};   // the library stream has consumed the slot
+    bool in_used[2] = {false, false};
+    int in_next = 0;
+    Control* in_ctrl = nullptr;                    // pinned [2]
 };
 
 Lib g;
@@ -266,8 +280,19 @@ void release_checkpoint() {
     g.ckpt_bytes = 0;
 }
 
+void release_uploads() {
+    for (int i = 0; i < 2; ++i) {
+        if (g.in_used[i]) cudaEventSynchronize(g.in_free[i]);
+        g.in_used[i] = false;
+        free_dev(g.in_stage[i]);
+        g.in_stage[i] = nullptr;
+    }
+    g.in_bytes = 0;
+}
+
 void release_mesh() {
     release_checkpoint();
+    release_uploads();
     release_graphs();
     free_dev(g.u[0]); free_dev(g.u[1]); free_dev(g.reg); free_dev(g.stagebuf);
     free_dev(g.alpha[0]); free_dev(g.alpha[1]); free_dev(g.alpha_used);
@@ -294,7 +319,9 @@ int mlp_t_offset() { return (MLP_NPACK + 3) / 4 * 4; }
 StageArgs stage_args(int st, bool rhs_only) {
     StageArgs a{};
     a.E = g.E;
+    a.E_begin = 0;
     a.E_own = g.E_own;
+    a.tick = 1;
     a.u_in = g.u[g.cur];
     a.u_out = g.u[g.cur ^ 1];
     a.reg = g.reg;
@@ -380,6 +407,19 @@ cudaError_t launch_stage(int st, cudaStream_t s) {
     return e;
 }
 
+// One part of a stage over owned elements [begin, end) of u[cur] (u[cur] stays current: the caller
+// toggles after the last part).  The mortar rows are recomputed for every part: a part that follows
+// a ghost refresh sees the fresh traces, and the rows the earlier part used are rewritten with the
+// same values where they read no ghost.  tick: this part advances t and the step counter.
+cudaError_t launch_stage_part(int st, int64_t begin, int64_t end, bool tick, cudaStream_t s) {
+    StageArgs a = stage_args(st, false);
+    a.E_begin = begin;
+    a.E_own = end;
+    a.tick = tick ? 1 : 0;
+    if (end <= begin && g.nm == 0) return cudaSuccess;
+    return launch_stage_any(a, false, s);
+}
+
 // Indicator (and, if dt_cand, the CFL bound) of the state in u[cur]: the stage kernel's epilogue
 // on the loaded state.
 cudaError_t launch_prepare(bool dt_cand, cudaStream_t s, float* feat = nullptr, double* alpha_modal = nullptr) {
@@ -435,6 +475,17 @@ int build_graph(int start) {
     cudaGraphDestroy(graph);
     if (e3 != cudaSuccess) return fail(NEMO_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e3));
     return NEMO_OK;
+}
+
+// The control block of a new run (time 0, counters reset, the configuration's GLM values).
+Control fresh_control() {
+    Control c{};
+    c.ngroups = g.ngroups;
+    c.dt_factor = 0.25 * g.cfg.cfl / (double)(2 * NN - 1);
+    c.glm_ch = g.cfg.glm_ch;
+    c.glm_alpha = g.cfg.glm_alpha;
+    c.mhd = is_mhd() ? 1 : 0;
+    return c;
 }
 
 }  // namespace
@@ -828,6 +879,7 @@ int nemo_gpu_set_owned(int64_t n_owned) {
     if (!g.has_mesh) return fail(NEMO_ERR_STATE, "set the mesh first");
     if (n_owned < 1 || n_owned > g.E) return fail(NEMO_ERR_ARG, "n_owned must be in [1, %lld]", (long long)g.E);
     g.E_own = n_owned;
+    g.n_interior = 0;
     release_graphs();
     g.prepared = false;
     return NEMO_OK;
@@ -904,16 +956,62 @@ int nemo_gpu_upload_state(const double* host, int64_t stride) {
     CK(launch_aos_to_soa(g.stagebuf, g.u[0], g.E, g.V, g.stream));
     CK(cudaMemsetAsync(g.reg, 0, row * g.E, g.stream));
     // reset the simulation time and counters
-    Control c{};
-    c.ngroups = g.ngroups;
-    c.dt_factor = 0.25 * g.cfg.cfl / (double)(2 * NN - 1);
-    c.glm_ch = g.cfg.glm_ch;
-    c.glm_alpha = g.cfg.glm_alpha;
-    c.mhd = is_mhd() ? 1 : 0;
+    const Control c = fresh_control();
     CK(cudaMemcpyAsync(g.ctrl, &c, sizeof c, cudaMemcpyHostToDevice, g.stream));
     CK(cudaStreamSynchronize(g.stream));
     g.has_state = true;
     g.prepared = false;
+    return NEMO_OK;
+}
+
+int nemo_gpu_upload_state_async(const double* host, int64_t stride) {
+    if (!g.has_mesh) return fail(NEMO_ERR_STATE, "set the mesh first");
+    if (!host) return fail(NEMO_ERR_ARG, "host is NULL");
+    const size_t row = sizeof(double) * (size_t)g.V * NP;
+    if (stride < (int64_t)row) return fail(NEMO_ERR_ARG, "element stride %lld < %zu bytes", (long long)stride, row);
+    // first call: stream, events, pinned control blocks (each piece on its own, so that a failed
+    // set-up is completed by the next call)
+    if (!g.in_stream) CK(cudaStreamCreateWithFlags(&g.in_stream, cudaStreamNonBlocking));
+    for (int i = 0; i < 2; ++i) {
+        if (!g.in_done[i]) CK(cudaEventCreateWithFlags(&g.in_done[i], cudaEventDisableTiming));
+        if (!g.in_free[i]) CK(cudaEventCreateWithFlags(&g.in_free[i], cudaEventDisableTiming));
+    }
+    if (!g.in_ctrl) CK(cudaHostAlloc((void**)&g.in_ctrl, 2 * sizeof(Control), cudaHostAllocDefault));
+    const int64_t bytes = (int64_t)row * g.E;
+    if (g.in_bytes != bytes) {
+        release_uploads();
+        for (int i = 0; i < 2; ++i) CK(cudaMalloc(&g.in_stage[i], (size_t)bytes));
+        g.in_bytes = bytes;
+    }
+    const int s = g.in_next;
+    // the slot's previous upload must have been consumed before its staging buffer and control
+    // block are written again (two uploads ago: in a pipelined loop this has long happened)
+    if (g.in_used[s]) CK(cudaEventSynchronize(g.in_free[s]));
+    g.in_ctrl[s] = fresh_control();
+    if (stride == (int64_t)row)
+        CK(cudaMemcpyAsync(g.in_stage[s], host, (size_t)bytes, cudaMemcpyHostToDevice, g.in_stream));
+    else
+        CK(cudaMemcpy2DAsync(g.in_stage[s], row, host, (size_t)stride, row, (size_t)g.E, cudaMemcpyHostToDevice,
+                             g.in_stream));
+    CK(cudaEventRecord(g.in_done[s], g.in_stream));
+    // consumed in stream order by the library stream: the work enqueued so far still sees the old
+    // state, the work enqueued after this call sees the new one
+    CK(cudaStreamWaitEvent(g.stream, g.in_done[s], 0));
+    g.cur = 0;
+    CK(launch_aos_to_soa(g.in_stage[s], g.u[0], g.E, g.V, g.stream));
+    CK(cudaMemsetAsync(g.reg, 0, row * g.E, g.stream));
+    CK(cudaMemcpyAsync(g.ctrl, &g.in_ctrl[s], sizeof(Control), cudaMemcpyHostToDevice, g.stream));
+    CK(cudaEventRecord(g.in_free[s], g.stream));
+    g.in_used[s] = true;
+    g.in_next = s ^ 1;
+    g.has_state = true;
+    g.prepared = false;
+    return NEMO_OK;
+}
+
+int nemo_gpu_upload_wait(void) {
+    for (int i = 0; i < 2; ++i)
+        if (g.in_used[i]) CK(cudaEventSynchronize(g.in_done[i]));
     return NEMO_OK;
 }
 
@@ -1059,6 +1157,98 @@ int nemo_gpu_step(double dt) {
     CK(launch_ctrl_set_dt(g.ctrl, dt, g.stream));
     for (int s = 0; s < 5; ++s) CK(launch_stage(s, g.stream));
     return check_ctrl_error();
+}
+
+int nemo_gpu_set_interior(int64_t n_interior) {
+    if (!g.has_mesh) return fail(NEMO_ERR_STATE, "set the mesh first");
+    if (n_interior < 0 || n_interior > g.E_own)
+        return fail(NEMO_ERR_ARG, "n_interior must be in [0, %lld]", (long long)g.E_own);
+    g.n_interior = n_interior;
+    return NEMO_OK;
+}
+
+int nemo_gpu_stage_interior(int32_t stage, double dt) {
+    int st = ensure_ready();
+    if (st) return st;
+    if (stage < 1 || stage > 5) return fail(NEMO_ERR_ARG, "stage must be 1..5");
+    if (!(dt >= 0.0) || !std::isfinite(dt)) return fail(NEMO_ERR_ARG, "dt must be finite and >= 0");
+    if (g.tune_mode == 1) return fail(NEMO_ERR_STATE, "split stages need the grid schedule (nemo_gpu_set_schedule 0)");
+    if ((st = prepare_if_needed())) return st;
+    CK(cudaMemcpyAsync(&g.nbad_mark, &g.ctrl->nbad, 8, cudaMemcpyDeviceToHost, g.stream));
+    CK(launch_ctrl_set_dt(g.ctrl, dt, g.stream));
+    // the interior part advances the clock only when there is no boundary part
+    CK(launch_stage_part(stage - 1, 0, g.n_interior, g.n_interior == g.E_own, g.stream));
+    g.split_open = true;
+    return NEMO_OK;
+}
+
+int nemo_gpu_stage_boundary(int32_t stage, double dt, int32_t* nbad_out) {
+    int st = ensure_ready();
+    if (st) return st;
+    (void)dt;
+    if (!g.split_open) return fail(NEMO_ERR_STATE, "nemo_gpu_stage_interior of this stage first");
+    g.split_open = false;
+    if (g.E_own > g.n_interior) CK(launch_stage_part(stage - 1, g.n_interior, g.E_own, true, g.stream));
+    g.cur ^= 1;
+    unsigned long long nb1 = 0;
+    CK(cudaMemcpyAsync(&nb1, &g.ctrl->nbad, 8, cudaMemcpyDeviceToHost, g.stream));
+    if ((st = check_ctrl_error())) return st;
+    if (nbad_out) *nbad_out = (int32_t)(nb1 - g.nbad_mark);
+    if (nb1 > g.nbad_mark) return fail(NEMO_ERR_REPAIR, "positivity repair failed on %llu elements", nb1 - g.nbad_mark);
+    return NEMO_OK;
+}
+
+int nemo_gpu_glm_speeds(double* lmax_out, double* vmax_out) {
+    int st = ensure_ready();
+    if (st) return st;
+    unsigned long long b[2] = {0, 0};
+    CK(cudaMemcpyAsync(&b[0], &g.ctrl->lmax_bits[0], 8, cudaMemcpyDeviceToHost, g.stream));
+    CK(cudaMemcpyAsync(&b[1], &g.ctrl->vmax_bits, 8, cudaMemcpyDeviceToHost, g.stream));
+    CK(cudaStreamSynchronize(g.stream));
+    if (lmax_out) std::memcpy(lmax_out, &b[0], 8);
+    if (vmax_out) std::memcpy(vmax_out, &b[1], 8);
+    return NEMO_OK;
+}
+
+int nemo_gpu_set_glm(double ch, double alpha) {
+    int st = ensure_ready();
+    if (st) return st;
+    if (!is_mhd()) return fail(NEMO_ERR_STATE, "GLM cleaning needs the MHD equations");
+    if (!std::isfinite(ch) || ch < 0.0 || !std::isfinite(alpha) || alpha < 0.0)
+        return fail(NEMO_ERR_ARG, "GLM speed and damping must be finite and >= 0");
+    const double v[2] = {ch, alpha};
+    CK(cudaMemcpyAsync(&g.ctrl->glm_ch, &v[0], 8, cudaMemcpyHostToDevice, g.stream));
+    CK(cudaMemcpyAsync(&g.ctrl->glm_alpha, &v[1], 8, cudaMemcpyHostToDevice, g.stream));
+    CK(cudaStreamSynchronize(g.stream));
+    return NEMO_OK;
+}
+
+int nemo_gpu_run_async(int64_t nsteps) {
+    int st = ensure_ready();
+    if (st) return st;
+    if (nsteps <= 0) return fail(NEMO_ERR_ARG, "nsteps must be > 0");
+    if (g.timing) return fail(NEMO_ERR_STATE, "timing mode runs synchronously (nemo_gpu_run)");
+    g.prepared = false;  // the CFL bound must belong to the current state
+    if ((st = prepare_if_needed())) return st;
+    // no end time (t_end = 0.0 is all-zero bits), not done
+    CK(cudaMemsetAsync(&g.ctrl->t_end, 0, sizeof(double), g.stream));
+    CK(cudaMemsetAsync(&g.ctrl->done, 0, sizeof(int32_t), g.stream));
+    for (int s = 0; s < 2; ++s)
+        if (!g.graph[s] && (st = build_graph(s))) return st;
+    for (int64_t i = 0; i < nsteps; ++i) {
+        CK(cudaGraphLaunch(g.graph[g.cur], g.stream));
+        g.cur ^= 1;
+    }
+    return NEMO_OK;
+}
+
+int nemo_gpu_sync(void) {
+    if (!g.inited) return fail(NEMO_ERR_STATE, "nemo_gpu_init has not been called");
+    if (g.in_stream) CK(cudaStreamSynchronize(g.in_stream));
+    if (g.copy_stream) CK(cudaStreamSynchronize(g.copy_stream));
+    CK(cudaStreamSynchronize(g.stream));
+    if (g.has_mesh) return check_ctrl_error();
+    return NEMO_OK;
 }
 
 int nemo_gpu_run(int64_t nsteps, double t_end, double* t_out, int64_t* steps_out) {
@@ -1540,6 +1730,16 @@ int nemo_gpu_finalize(void) {
     g.ckpt_meta = g.ckpt_meta_host = nullptr;
     g.ckpt_ready = g.ckpt_done = nullptr;
     g.copy_stream = nullptr;
+    for (int i = 0; i < 2; ++i) {   // release_mesh released the staging slots
+        if (g.in_done[i]) cudaEventDestroy(g.in_done[i]);
+        if (g.in_free[i]) cudaEventDestroy(g.in_free[i]);
+        g.in_done[i] = g.in_free[i] = nullptr;
+    }
+    if (g.in_ctrl) cudaFreeHost(g.in_ctrl);
+    if (g.in_stream) cudaStreamDestroy(g.in_stream);
+    g.in_ctrl = nullptr;
+    g.in_stream = nullptr;
+    g.in_next = 0;
     g.ctrl = nullptr;
     g.tot = nullptr;
     g.mlp32 = nullptr;

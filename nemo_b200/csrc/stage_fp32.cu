@@ -584,7 +584,7 @@ __device__ __forceinline__ void tile32(const StageArgs& a, const Smem32& S, int6
     const float* s_w = S.s_w;
     const int tid = threadIdx.x;
     const int64_t E = a.E;
-    const int64_t e0 = tile * EPC;
+    const int64_t e0 = a.E_begin + tile * EPC;
     const int nel = (int)min((int64_t)EPC, a.E_own - e0);
 
     if (tid < EPC) {
@@ -860,7 +860,7 @@ __device__ __forceinline__ void tile32(const StageArgs& a, const Smem32& S, int6
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncthreads();
     if (tid == 0) tile_store32(su, a.u_out, E, e0, nel);
-    if (st == 4 && tile == 0 && tid == 0) {
+    if (st == 4 && a.tick && tile == 0 && tid == 0) {
         for (int g = 0; g < ctrl->ngroups; ++g) ctrl->t[g] = ctrl->t[g] + ctrl->dt[g];
         ctrl->steps += 1;
     }
@@ -904,7 +904,7 @@ __global__ void __launch_bounds__(NT, 4) k_stage_euler32p(StageArgs a, MortarArg
     load_mlp32(a, s_w);
     const Smem32 S = smem32(smem, bar, s_alpha, s_bad, s_w);
     mbar_init32(bar);
-    const int64_t ntiles = (a.E_own + EPC - 1) / EPC;
+    const int64_t ntiles = (a.E_own - a.E_begin + EPC - 1) / EPC;
     const int64_t npairs = (ma.nm + mortar::MPB - 1) / mortar::MPB;
     unsigned phase = 0;
     for (;;) {
@@ -939,7 +939,8 @@ int stage_smem_bytes32() {
 }
 
 cudaError_t launch_stage_euler32(const StageArgs& a, bool blend, bool rhs_only, cudaStream_t s) {
-    const int grid = (int)((a.E_own + EPC - 1) / EPC);
+    const int grid = (int)((a.E_own - a.E_begin + EPC - 1) / EPC);
+    if (grid <= 0) return cudaSuccess;
     const int smem = stage_smem_bytes32();
     if (rhs_only) {
         if (blend) k_stage_euler32<true, true><<<grid, NT, smem, s>>>(a);
@@ -1006,7 +1007,8 @@ cudaError_t setup_stage_mhd32() {
 }
 
 cudaError_t launch_stage_mhd32(const StageArgs& a, bool blend, bool rhs_only, cudaStream_t s) {
-    const int grid = (int)((a.E_own + mhd::EPC - 1) / mhd::EPC);
+    const int grid = (int)((a.E_own - a.E_begin + mhd::EPC - 1) / mhd::EPC);
+    if (grid <= 0) return cudaSuccess;
     const int smem = stage_smem_bytes_mhd32();
     if (rhs_only) {
         if (blend) k_stage_mhd<float, true, true><<<grid, mhd::NT, smem, s>>>(a);

@@ -1,6 +1,6 @@
 // stage_fp64.cu -- plain FP64 path: one fused kernel per LSRK stage (compiled with -fmad=false).
 //
-// One CTA owns EPC = 8 consecutive elements (a 2x2x2 block on a Morton-ordered brick) and runs
+// One CTA owns EPC = 4 consecutive elements (a 2x2x1 block on a Morton-ordered brick) and runs
 // 48 threads per element, one per (direction d, line (a,b)).  Per stage and element it does what
 // the reference spreads over hook_pre_rk_timestep_300 and hook_mid_rk_timestep_500:
 //   1. TMA bulk copy (cp.async.bulk, mbarrier) of the 8 elements' SoA state into shared memory;
@@ -29,16 +29,20 @@ __constant__ OpConsts c_ops64;
 namespace {
 
 // Tile shape (compile-time knobs for tuning builds): elements per CTA and the minimum number of
-// resident CTAs per SM that __launch_bounds__ asks the register allocator for.
+// resident CTAs per SM that __launch_bounds__ asks the register allocator for.  Measured on B200
+// (Sedov 32^3, plain FP64 stage, bit-identical results in every case): 8 elements x 1 CTA/SM at 168
+// registers 0.890 ms; 4 x 3 CTAs/SM at 96 registers 0.735 ms; 2 x 6 at 96 registers 0.764 ms;
+// 2 x 5 0.784 ms.  Three independent 192-thread CTAs per SM overlap one another's tile loads,
+// barriers and epilogues, which one 384-thread CTA cannot (barrier stalls were 2.0 per issue).
 #ifndef NEMO_FP64_EPC
-#define NEMO_FP64_EPC 8
+#define NEMO_FP64_EPC 4
 #endif
 #ifndef NEMO_FP64_MINB
-#define NEMO_FP64_MINB 1
+#define NEMO_FP64_MINB 3
 #endif
 constexpr int EPC = NEMO_FP64_EPC;   // elements per CTA
 constexpr int TPE = 48;              // threads per element
-constexpr int NT = EPC * TPE;        // 384 threads at 8 elements per CTA
+constexpr int NT = EPC * TPE;        // 192 threads at 4 elements per CTA
 constexpr int V = 5;
 static_assert(NT / 32 >= EPC, "the repair runs one element per warp");
 
@@ -303,7 +307,7 @@ __global__ void __launch_bounds__(NT, NEMO_FP64_MINB) k_stage_euler64(StageArgs 
 
     const int tid = threadIdx.x;
     const int64_t E = a.E;
-    const int64_t e0 = (int64_t)blockIdx.x * EPC;
+    const int64_t e0 = a.E_begin + (int64_t)blockIdx.x * EPC;
     const int nel = (int)min((int64_t)EPC, a.E_own - e0);
 
     if (tid < EPC) {
@@ -361,51 +365,6 @@ __global__ void __launch_bounds__(NT, NEMO_FP64_MINB) k_stage_euler64(StageArgs 
 
     double t[NN][V];  // direction-d contribution per line node, rotated frame
     if (active) {
-        // ---- surface fluxes at the two ends of the line (faces 2d, 2d+1 at (la,lb))
-        double Fs[2][V];
-#pragma unroll
-        for (int side = 0; side < 2; ++side) {
-            const int f = 2 * d + side;
-            const int own = line_node(d, la, lb, side ? NN - 1 : 0);
-            double uo[V], un[V];
-            uo[0] = su[(0 * EPC + el) * NP + own];
-            uo[1] = su[((1 + c0) * EPC + el) * NP + own];
-            uo[2] = su[((1 + c1) * EPC + el) * NP + own];
-            uo[3] = su[((1 + c2) * EPC + el) * NP + own];
-            uo[4] = su[(4 * EPC + el) * NP + own];
-            const int32_t ne = a.nbr[e * 6 + f];
-            if (ne <= -2) {  // 2:1 mortar face: flux row of the mortar kernel
-                const double* mf = a.mflux + (int64_t)(-2 - ne) * V * NF + ab;
-#pragma unroll
-                for (int v = 0; v < V; ++v) Fs[side][v] = mf[v * NF];
-                continue;
-            }
-            if (ne >= 0) {
-                const int nn = line_node(d, la, lb, side ? 0 : NN - 1);
-                const int64_t nl = (int64_t)ne - e0;
-                if (nl >= 0 && nl < nel) {
-                    const int nli = (int)nl;
-                    un[0] = su[(0 * EPC + nli) * NP + nn];
-                    un[1] = su[((1 + c0) * EPC + nli) * NP + nn];
-                    un[2] = su[((1 + c1) * EPC + nli) * NP + nn];
-                    un[3] = su[((1 + c2) * EPC + nli) * NP + nn];
-                    un[4] = su[(4 * EPC + nli) * NP + nn];
-                } else {
-                    const double* g = a.u_in;
-                    un[0] = __ldg(g + ((int64_t)0 * E + ne) * NP + nn);
-                    un[1] = __ldg(g + ((int64_t)(1 + c0) * E + ne) * NP + nn);
-                    un[2] = __ldg(g + ((int64_t)(1 + c1) * E + ne) * NP + nn);
-                    un[3] = __ldg(g + ((int64_t)(1 + c2) * E + ne) * NP + nn);
-                    un[4] = __ldg(g + ((int64_t)4 * E + ne) * NP + nn);
-                }
-            } else {
-#pragma unroll
-                for (int v = 0; v < V; ++v) un[v] = uo[v];
-            }
-            if (side) riemann64(a.surface_flux, uo, un, Fs[1], k);
-            else riemann64(a.surface_flux, un, uo, Fs[0], k);
-        }
-
         // ---- split-form volume flux differencing along the line
         int idx[NN];
 #pragma unroll
@@ -454,6 +413,52 @@ __global__ void __launch_bounds__(NT, NEMO_FP64_MINB) k_stage_euler64(StageArgs 
                 t[m][v] = t[m][v] + smi * F[v];
             }
         }
+        // ---- surface fluxes at the two ends of the line (faces 2d, 2d+1 at (la,lb)), after the
+        //      volume pairs so that they are not live during the pair loop (fewer registers)
+        double Fs[2][V];
+#pragma unroll
+        for (int side = 0; side < 2; ++side) {
+            const int f = 2 * d + side;
+            const int own = line_node(d, la, lb, side ? NN - 1 : 0);
+            double uo[V], un[V];
+            uo[0] = su[(0 * EPC + el) * NP + own];
+            uo[1] = su[((1 + c0) * EPC + el) * NP + own];
+            uo[2] = su[((1 + c1) * EPC + el) * NP + own];
+            uo[3] = su[((1 + c2) * EPC + el) * NP + own];
+            uo[4] = su[(4 * EPC + el) * NP + own];
+            const int32_t ne = a.nbr[e * 6 + f];
+            if (ne <= -2) {  // 2:1 mortar face: flux row of the mortar kernel
+                const double* mf = a.mflux + (int64_t)(-2 - ne) * V * NF + ab;
+#pragma unroll
+                for (int v = 0; v < V; ++v) Fs[side][v] = mf[v * NF];
+                continue;
+            }
+            if (ne >= 0) {
+                const int nn = line_node(d, la, lb, side ? 0 : NN - 1);
+                const int64_t nl = (int64_t)ne - e0;
+                if (nl >= 0 && nl < nel) {
+                    const int nli = (int)nl;
+                    un[0] = su[(0 * EPC + nli) * NP + nn];
+                    un[1] = su[((1 + c0) * EPC + nli) * NP + nn];
+                    un[2] = su[((1 + c1) * EPC + nli) * NP + nn];
+                    un[3] = su[((1 + c2) * EPC + nli) * NP + nn];
+                    un[4] = su[(4 * EPC + nli) * NP + nn];
+                } else {
+                    const double* g = a.u_in;
+                    un[0] = __ldg(g + ((int64_t)0 * E + ne) * NP + nn);
+                    un[1] = __ldg(g + ((int64_t)(1 + c0) * E + ne) * NP + nn);
+                    un[2] = __ldg(g + ((int64_t)(1 + c1) * E + ne) * NP + nn);
+                    un[3] = __ldg(g + ((int64_t)(1 + c2) * E + ne) * NP + nn);
+                    un[4] = __ldg(g + ((int64_t)4 * E + ne) * NP + nn);
+                }
+            } else {
+#pragma unroll
+                for (int v = 0; v < V; ++v) un[v] = uo[v];
+            }
+            if (side) riemann64(a.surface_flux, uo, un, Fs[1], k);
+            else riemann64(a.surface_flux, un, uo, Fs[0], k);
+        }
+
         // ---- surface lift at the line ends
 #pragma unroll
         for (int v = 0; v < V; ++v) {
@@ -566,7 +571,7 @@ __global__ void __launch_bounds__(NT, NEMO_FP64_MINB) k_stage_euler64(StageArgs 
 #pragma unroll
         for (int v = 0; v < V; ++v) a.u_out[((int64_t)v * E + e0 + pel) * NP + n] = su[(v * EPC + pel) * NP + n];
     }
-    if (st == 4 && blockIdx.x == 0 && tid == 0) {
+    if (st == 4 && a.tick && blockIdx.x == 0 && tid == 0) {
         for (int g = 0; g < ctrl->ngroups; ++g) ctrl->t[g] = ctrl->t[g] + ctrl->dt[g];
         ctrl->steps += 1;
     }
@@ -606,7 +611,8 @@ __global__ void k_totals_sum64(const double* __restrict__ part, int64_t E, int n
 int stage_smem_bytes64() { return (V * EPC * NP + 6 * EPC * NP + 2 * V * EPC * NP) * (int)sizeof(double); }
 
 cudaError_t launch_stage_euler64(const StageArgs& a, bool blend, bool ind, bool rhs_only, cudaStream_t s) {
-    const int grid = (int)((a.E_own + EPC - 1) / EPC);
+    const int grid = (int)((a.E_own - a.E_begin + EPC - 1) / EPC);
+    if (grid <= 0) return cudaSuccess;
     const int smem = stage_smem_bytes64();
     (void)ind;
     if (rhs_only) {
@@ -697,7 +703,8 @@ cudaError_t launch_repair_states64(double* st, int64_t n, int nv, int mhd, int32
 }
 
 cudaError_t launch_stage_mhd64(const StageArgs& a, bool blend, bool rhs_only, cudaStream_t s) {
-    const int grid = (int)((a.E_own + mhd::EPC - 1) / mhd::EPC);
+    const int grid = (int)((a.E_own - a.E_begin + mhd::EPC - 1) / mhd::EPC);
+    if (grid <= 0) return cudaSuccess;
     const int smem = stage_smem_bytes_mhd64();
     if (rhs_only) {
         if (blend) k_stage_mhd<double, true, true><<<grid, mhd::NT, smem, s>>>(a);

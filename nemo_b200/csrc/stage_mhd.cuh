@@ -431,7 +431,7 @@ __global__ void __launch_bounds__(mhd::NT, sizeof(R) == 4 ? 3 : 1) k_stage_mhd(S
     if (!RHS_ONLY && !a.prep_only && ctrl->done) return;
     const int tid = threadIdx.x;
     const int64_t E = a.E;
-    const int64_t e0 = (int64_t)blockIdx.x * MEPC;
+    const int64_t e0 = a.E_begin + (int64_t)blockIdx.x * MEPC;
     const int nel = (int)min((int64_t)MEPC, a.E_own - e0);
     const R kap = (R)k.kappa, mu0 = (R)k.mu0;
     const R ch = (R)ctrl->glm_ch;
@@ -632,7 +632,7 @@ __global__ void __launch_bounds__(mhd::NT, sizeof(R) == 4 ? 3 : 1) k_stage_mhd(S
                 a.u_out[((int64_t)v * E + e) * NP + n] = su[(v * MEPC + el) * NP + n];
             }
     }
-    if (st == 4 && blockIdx.x == 0 && tid == 0) {
+    if (st == 4 && a.tick && blockIdx.x == 0 && tid == 0) {
         for (int g = 0; g < ctrl->ngroups; ++g) ctrl->t[g] = ctrl->t[g] + ctrl->dt[g];
         ctrl->steps += 1;
     }

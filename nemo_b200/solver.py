@@ -71,6 +71,27 @@ class Solver:
         aos = np.ascontiguousarray(u.transpose(1, 0, 2))
         call("nemo_gpu_upload_state", abi.ptr(aos), self.V * self.n ** 3 * 8)
 
+    def upload_async(self, aos, stride_bytes):
+        """Asynchronous upload from a pinned host buffer laid out like the reference's quad array
+        (nemo_gpu_upload_state_async): taken in stream order by the steps enqueued after it."""
+        call("nemo_gpu_upload_state_async", ctypes.c_void_p(aos), int(stride_bytes))
+
+    def run_async(self, nsteps):
+        """Enqueue nsteps device-dt steps without waiting (nemo_gpu_run_async)."""
+        call("nemo_gpu_run_async", int(nsteps))
+
+    def download_async(self, aos, stride_bytes):
+        """Start the device->host copy of the state after the enqueued steps (checkpoint staging)."""
+        call("nemo_gpu_checkpoint_begin", ctypes.c_void_p(aos), int(stride_bytes), None)
+        self._download_pending = True
+
+    def sync(self):
+        """Wait for everything enqueued (steps and copies); raise what the device reported."""
+        if getattr(self, "_download_pending", False):
+            call("nemo_gpu_checkpoint_wait", ctypes.byref(ctypes.c_double()), ctypes.byref(ctypes.c_int64()))
+            self._download_pending = False
+        call("nemo_gpu_sync")
+
     def upload_aos(self, aos, stride_bytes):
         """Upload from a host buffer laid out like the reference's quad array (per-element stride)."""
         call("nemo_gpu_upload_state", ctypes.c_void_p(aos), int(stride_bytes))

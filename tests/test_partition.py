@@ -27,12 +27,22 @@ def blast_state(m):
 def test_partition_invariants(nranks):
     m = band_forest()
     parts = partition.partition(m, nranks)
-    owned = np.concatenate([p.glob[: p.n_owned] for p in parts])
+    owned = np.concatenate([np.sort(p.glob[: p.n_owned]) for p in parts])
     assert np.array_equal(owned, np.arange(m.E))
     gnbr = m.neighbors()
     for p in parts:
         lnbr = p.mesh.neighbors()          # a valid local mesh (every face on one side)
         lm = p.mesh.mortars()
+        # interior elements come first and read no ghost: no ghost neighbour, no ghost mortar quad
+        assert 0 < p.n_interior < p.n_owned
+        inner = lnbr[: p.n_interior]
+        assert np.all(inner < p.n_owned)
+        for row in lm:
+            quads = row[[0, 2, 3, 4, 5]]
+            if np.any(quads < p.n_interior):
+                assert np.all(quads < p.n_owned)
+        # both owned blocks keep the element order
+        assert np.all(np.diff(p.glob[: p.n_interior]) > 0) and np.all(np.diff(p.glob[p.n_interior: p.n_owned]) > 0)
         for e in range(p.n_owned):
             for f in range(6):
                 if lnbr[e, f] >= 0:
@@ -95,7 +105,8 @@ def _worker(rank, world, port, out_dir, nsteps):
                 if st > 0:
                     partition.exchange(part, dist, get_rows, set_rows, make_buffer)
                 o.stage(ul, reg, st, float(dt.item()))
-        np.save(os.path.join(out_dir, f"rank{rank}.npy"), ul[:, :own])
+        order = np.argsort(part.glob[:own])   # owned elements in global order
+        np.save(os.path.join(out_dir, f"rank{rank}.npy"), ul[:, :own][:, order])
     finally:
         dist.destroy_process_group()
 
@@ -203,3 +214,117 @@ def test_face_exchange_gloo(tmp_path):
     import torch.multiprocessing as tmp
     tmp.spawn(_face_worker, args=(3, _free_port(), str(tmp_path)), nprocs=3, join=True)
     assert all(bool(np.load(tmp_path / f"ok{r}.npy")[0]) for r in range(3))
+
+
+def mhd_cfg():
+    c = abi.cfg_struct(eqn=abi.EQN_MHD, n_vars=9, volume_flux=abi.VOLFLUX_EC_MHD, surface_flux=abi.SURFFLUX_HLLD,
+                       kappa=5.0 / 3.0, mu0=1.0, indicator=abi.IND_MODAL, positivity=1)
+    return c
+
+
+def _mhd_worker(rank, world, port, out_dir, nsteps):
+    """GLM-MHD on gloo ranks: the oracle stage on the rank's share, Δt all-reduced (MIN), the wave and
+    velocity maxima all-reduced (MAX) into the cleaning speed of every rank, the ghost exchange
+    posted before and finished after the interior work of each stage (begin / end)."""
+    import torch
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        m = band_forest()
+        u = np.ascontiguousarray(setups.orszag_tang(m))
+        part = partition.partition(m, world)[rank]
+        cfg = mhd_cfg()
+        lm = part.mesh
+        o = orc.Oracle.for_mesh(cfg, lm, nthreads=1)
+        ul = np.ascontiguousarray(u[:, part.glob])
+        reg = np.zeros_like(ul)
+        V, own = ul.shape[0], part.n_owned
+
+        def get_rows(idx):
+            return torch.from_numpy(np.ascontiguousarray(ul[:, idx].transpose(1, 0, 2)).reshape(len(idx), -1))
+
+        def set_rows(idx, buf):
+            ul[:, idx] = buf.numpy().reshape(len(idx), V, 64).transpose(1, 0, 2)
+
+        def make_buffer(n):
+            return torch.empty((n, V * 64), dtype=torch.float64)
+
+        delta_own = np.ascontiguousarray(lm.delta[:own])
+        for _ in range(nsteps):
+            partition.exchange(part, dist, get_rows, set_rows, make_buffer)
+            lmx, vmx = orc.ctypes.c_double(), orc.ctypes.c_double()
+            dt_loc = orc.lib().or_timestep2(o._c(), own, orc._p(delta_own), orc._p(np.ascontiguousarray(ul[:, :own])),
+                                            orc.ctypes.byref(lmx), orc.ctypes.byref(vmx))
+            lmax, vmax = lmx.value, vmx.value
+            dt = torch.tensor([dt_loc], dtype=torch.float64)
+            dist.all_reduce(dt, op=dist.ReduceOp.MIN)
+            sp = torch.tensor([lmax, vmax], dtype=torch.float64)
+            dist.all_reduce(sp, op=dist.ReduceOp.MAX)
+            cfg.glm_ch = 2.0 * abs(float(sp[0]) - float(sp[1]))
+            cfg.glm_alpha = cfg.glm_ch / 0.18
+            for st in range(5):
+                if st > 0:
+                    h = partition.exchange_begin(part, dist, get_rows, make_buffer)
+                    partition.exchange_end(h, set_rows)
+                o.stage(ul, reg, st, float(dt.item()))
+        order = np.argsort(part.glob[:own])
+        np.save(os.path.join(out_dir, f"rank{rank}.npy"), ul[:, :own][:, order])
+    finally:
+        dist.destroy_process_group()
+
+
+def test_partitioned_mhd_oracle_run_matches_single_process(tmp_path):
+    import torch.multiprocessing as tmp
+    orc.build()
+    nsteps = 2
+    tmp.spawn(_mhd_worker, args=(2, _free_port(), str(tmp_path), nsteps), nprocs=2, join=True)
+    got = np.concatenate([np.load(tmp_path / f"rank{r}.npy") for r in range(2)], axis=1)
+    m = band_forest()
+    u = setups.orszag_tang(m)
+    ref, _, n, _ = orc.Oracle.for_mesh(mhd_cfg(), m).run(u, nsteps=nsteps)
+    assert n == nsteps
+    assert np.array_equal(got, ref)
+
+
+def _overlap_worker(rank, world, port, out_dir):
+    """exchange_begin posts the transfers; work between begin and end; exchange_end delivers the
+    same traces as a back-to-back exchange."""
+    import time
+    import torch
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        m = band_forest()
+        u = blast_state(m)
+        part = partition.partition(m, world)[rank]
+        V = u.shape[0]
+        ul = np.zeros((V, len(part.glob), 64))
+        ul[:, : part.n_owned] = u[:, part.glob[: part.n_owned]]
+
+        def get_rows(ent):
+            idx, fs = ent
+            return torch.from_numpy(np.array([ul[:, i][:, _face_nodes(f)].ravel() for i, f in zip(idx, fs)]))
+
+        def set_rows(ent, buf):
+            b = buf.numpy()
+            for k, (i, f) in enumerate(zip(*ent)):
+                ul[:, i, _face_nodes(f)] = b[k].reshape(V, 16)
+
+        h = partition.exchange_begin(part, dist, get_rows, lambda n: torch.empty((n, V * 16), dtype=torch.float64),
+                                     faces=True)
+        time.sleep(0.05 * (rank + 1))           # "interior work" of uneven length on the ranks
+        partition.exchange_end(h, set_rows)
+        ok = all(np.array_equal(ul[:, i, _face_nodes(f)], u[:, part.glob[i], _face_nodes(f)])
+                 for idx, fs in part.recv_f.values() for i, f in zip(idx, fs))
+        np.save(os.path.join(out_dir, f"ok{rank}.npy"), np.array([ok]))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_exchange_begin_end_with_work_between(world, tmp_path):
+    import torch.multiprocessing as tmp
+    tmp.spawn(_overlap_worker, args=(world, _free_port(), str(tmp_path)), nprocs=world, join=True)
+    assert all(bool(np.load(tmp_path / f"ok{r}.npy")[0]) for r in range(world))
