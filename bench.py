@@ -8,9 +8,10 @@ reduction); one DOF-update is one node with all 5 variables advanced through one
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload W]
 
-Multi-GPU (torchrun): every rank advances its own replica of the workload (independent runs; the
-element-partitioned halo exchange is not built), the timed region is bracketed by barriers and the
-max over ranks is reported; value is the whole-job DOF-updates/s.
+Multi-GPU (torchrun): one domain split over the ranks (element partition along the Morton order,
+ghost face traces exchanged over NCCL while each rank advances its interior elements; strong
+scaling); the timed region is bracketed by barriers, the max over ranks is reported, and value is
+the whole-job DOF-updates/s.
 """
 import argparse
 import json
@@ -204,6 +205,8 @@ FORMS = {
     "fp32_learned": (1, True),
 }
 GATE = 1e-6   # relative L1 density error of a form against the plain FP64 (oracle) run at t_end
+SCHEDULES = {0: "grid, 8 elements per CTA", 1: "persistent", 2: "grid, 4 elements per CTA",
+             3: "grid, 16 elements per CTA"}
 
 
 def accuracy_check(wl, m, u, abi, Solver, t_end=0.05, groups=None):  # noqa: C901
@@ -340,6 +343,102 @@ def roofline_of(bytes_per_launch, flops_per_launch, avg_s, hbm_gbs, peak_tflops,
     return out
 
 
+def run_partitioned(args, rank, world, local, dist, torch):
+    """N > 1: one domain split over the ranks (strong scaling).  Each rank advances its contiguous
+    Morton range of elements plus ghost copies of their face neighbours with the chosen form (FP32
+    bulk + modal indicator); per stage the partition-boundary traces go over NCCL while the rank's
+    interior elements advance, then the boundary elements follow (partition.PartitionedRun); Δt is an
+    all-reduce minimum.  Timed on the device, max over ranks."""
+    import ctypes
+    from nemo_b200 import abi, partition
+    m, u, groups = make_state(args.workload)
+    if groups is not None:
+        raise SystemExit("the partitioned bench runs single-group workloads")
+    V = nvars(args.workload)
+    part = partition.partition(m, world)[rank]
+    cfg = make_cfg(args.workload, abi.PREC_FP32)
+    run = partition.PartitionedRun(cfg, part, dist)
+    abi.call("nemo_gpu_set_schedule", 0, 0)
+    u_loc = np.ascontiguousarray(u[:, part.glob])
+    run.upload(u_loc)
+    run.run(args.warmup)
+    stream_ptr = ctypes.c_uint64()
+    abi.call("nemo_gpu_stream", ctypes.byref(stream_ptr))
+    stream = torch.cuda.ExternalStream(stream_ptr.value)
+
+    def timed(fn, steps):
+        dist.barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        dist.barrier()
+        t = torch.tensor([e0.elapsed_time(e1)], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    with ClockSampler(local) as clk:
+        ms = timed(run.step, args.steps)
+    dof_per_step = m.E * 64 * 5
+    value = dof_per_step * args.steps / (ms * 1e-3)
+    # end to end: every rank uploads its share, advances one step, downloads its owned elements
+    e2e_steps = max(3, min(args.steps, 10))
+    row = V * 64 * 8
+    host_in = torch.empty(u_loc.size, dtype=torch.float64, pin_memory=True)
+    host_in.numpy()[:] = np.ascontiguousarray(u_loc.transpose(1, 0, 2)).ravel()
+    host_out = torch.empty(u_loc.size, dtype=torch.float64, pin_memory=True)
+
+    def e2e_step():
+        run.s.upload_aos(host_in.data_ptr(), row)
+        run.step()
+        abi.call("nemo_gpu_download_state", ctypes.c_void_p(host_out.data_ptr()), row)
+
+    e2e_step()
+    e2e_ms = timed(e2e_step, e2e_steps)
+    loc_bytes = torch.tensor([float(u_loc.nbytes), float(part.n_owned * row)], device="cuda")
+    dist.all_reduce(loc_bytes)
+    bytes_per_launch = sum(m.E * 64 * V * 8 * (3 if st == 0 else 4) for st in range(5)) / 5.0
+    hbm, hbm_kind = load_peaks()
+    stage_s = ms * 1e-3 / (5 * args.steps)
+    achieved = bytes_per_launch / stage_s / 1e9 / world
+    nsend = sum(len(v[0]) for v in part.send_f.values())
+    # the library's kernels per step on this rank: 5 ghost refreshes (one pack per peer sent to, one
+    # unpack per peer received from), the CFL evaluation (control reset + prepare launch), and per
+    # stage the dt set, the interior and boundary stage launches and, on forests, two mortar launches
+    nm = len(part.mesh.mortars())
+    per_step = (5 * (len(part.send_f) + len(part.recv_f)) + 2
+                + 5 * (1 + (part.n_interior > 0) + (part.n_owned > part.n_interior) + 2 * (nm > 0)))
+    launches = torch.tensor([float(per_step * args.steps)], device="cuda")
+    dist.all_reduce(launches)
+    if rank == 0:
+        line = {
+            "metric": "DOF-updates/s per RK stage", "value": value, "unit": "DOF-updates/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "f32 flux bulk, f64 state/register/update",
+            "data": "synthetic", "config": workload_config(args.workload, m, u),
+            "form": "chosen: FP32 bulk + FP64 state/register/update/repair/reductions, modal indicator",
+            "parallelism": f"element partition over {world} GPUs (Morton ranges, NCCL face-trace exchange "
+                           "overlapped with the interior elements of each stage)",
+            "clocks": clk.summary(),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                         "traffic": None, "peak_source": hbm_kind, "kernel": "k_stage_euler32",
+                         "note": "per GPU, from the whole step time (exchange and all-reduce included)"},
+            "e2e": {"value": dof_per_step * e2e_steps / (e2e_ms * 1e-3), "unit": "DOF-updates/s",
+                    "h2d_bytes_per_step": float(loc_bytes[0]), "d2h_bytes_per_step": float(loc_bytes[1]),
+                    "note": "per step, all ranks: upload of each rank's share (owned + ghost elements) from "
+                            "pinned host memory, one partitioned step, download of each rank's elements"},
+            "gpu_launches": int(launches.item()),
+            "exchange": {"face_rows_sent_by_rank0_per_stage": nsend,
+                         "bytes_sent_by_rank0_per_stage": nsend * (V * 16 + 1) * 8,
+                         "interior_fraction_rank0": part.n_interior / part.n_owned},
+        }
+        print(json.dumps(line), flush=True)
+    run.s.finalize()
+
+
 def main():  # noqa: C901
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -372,6 +471,14 @@ def main():  # noqa: C901
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
+    if world > 1:
+        try:
+            run_partitioned(args, rank, world, local, dist, torch)
+        finally:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+
     from nemo_b200 import abi
     from nemo_b200.solver import Solver
     import ctypes
@@ -398,10 +505,11 @@ def main():  # noqa: C901
             if args.schedule == "auto":
                 mode, ctas, tms = s.autotune(nsteps=3)   # restores the state it times
             else:
-                mode, ctas, tms = (0, 0, [-1.0] * 5) if args.schedule == "grid" else (1, 4 * peaks["sms"], [-1.0] * 5)
+                mode, ctas, tms = (0, 0, [-1.0] * 8) if args.schedule == "grid" else (1, 4 * peaks["sms"], [-1.0] * 8)
                 s.set_schedule(mode, ctas)
-            sched = {"chosen": "persistent" if mode == 1 else "grid", "persistent_ctas": ctas,
-                     "autotune_ms_per_step": {"grid": tms[0], "persistent_1_per_sm": tms[1],
+            sched = {"chosen": SCHEDULES[mode], "persistent_ctas": ctas,
+                     "autotune_ms_per_step": {"grid_8_elements_per_cta": tms[0], "grid_4_elements_per_cta": tms[5],
+                                              "grid_16_elements_per_cta": tms[6], "persistent_1_per_sm": tms[1],
                                               "persistent_2_per_sm": tms[2], "persistent_3_per_sm": tms[3],
                                               "persistent_4_per_sm": tms[4]}}
         abi.call("nemo_gpu_stream", ctypes.byref(stream_ptr))

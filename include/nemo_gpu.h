@@ -210,8 +210,8 @@ int nemo_gpu_download_state(double* host, int64_t elem_stride_bytes);
    library's upload stream into one of two staging slots and returns at once; the library stream
    takes the new state in stream order (work enqueued before the call still sees the old state, work
    enqueued after it the new one, as a new run: time 0, register cleared).  So the copy of the next
-   state overlaps the stage work of the current one and, with nemo_gpu_checkpoint_begin as the
-   asynchronous download, the copy of its result.  host must be pinned (cudaHostAlloc or
+   state overlaps the stage work of the current one and, with nemo_gpu_download_state_async, the
+   copy of its result.  host must be pinned (cudaHostAlloc or
    cudaHostRegister) for the copy to be asynchronous, and must not be modified before
    nemo_gpu_upload_wait returns (or before the second-next call of this function, which reuses the
    slot).  Same layout and stride rules as nemo_gpu_upload_state.  No reference counterpart: the
@@ -221,6 +221,14 @@ int nemo_gpu_upload_state_async(const double* host, int64_t elem_stride_bytes);
 /* Wait until the host->device copies of every asynchronous upload have finished (their host
    buffers may then be reused). */
 int nemo_gpu_upload_wait(void);
+
+/* Asynchronous form of nemo_gpu_download_state: the state after all work enqueued so far is copied
+   in stream order into one of two staging slots and from there to host on the library's download
+   stream; the call returns at once (it waits only when the slot's copy of two calls ago is still
+   running).  host should be pinned and must not be read before nemo_gpu_sync returns.  With
+   nemo_gpu_upload_state_async and nemo_gpu_run_async the copies in both directions overlap the
+   steps of other states.  No reference counterpart. */
+int nemo_gpu_download_state_async(double* host, int64_t elem_stride_bytes);
 
 /* Checkpoint staging (the state that hook_checkpoint_fill writes, source/checkpoint/flash/
    checkpoint_mod.f90:319-364, and the restart that source/nemo_prog.f90:107-114 leaves as a TODO).
@@ -248,14 +256,14 @@ int nemo_gpu_stage(int32_t stage, double dt, double t_stage, int32_t* nbad_out);
 
 /* Enqueue nsteps full time steps with the device-side dt (as nemo_gpu_run without an end time) on
    the library stream and return without waiting: with nemo_gpu_upload_state_async before and
-   nemo_gpu_checkpoint_begin after it, a host streams states through the library with the copies of
-   one state overlapping the steps of another.  Errors the device reports while these steps run
+   nemo_gpu_download_state_async after it, a host streams states through the library with the
+   copies of one state overlapping the steps of another.  Errors the device reports while these steps run
    (bounded waits, a non-finite dt) come back from the next nemo_gpu_sync or nemo_gpu_run; repair
    failures are counted in nemo_gpu_status.  Not in timing mode.  No reference counterpart. */
 int nemo_gpu_run_async(int64_t nsteps);
 
-/* Wait for all work the library has enqueued (steps, asynchronous uploads and checkpoint copies)
-   and return the status the device reported for it. */
+/* Wait for all work the library has enqueued (steps, asynchronous uploads and downloads, checkpoint
+   copies) and return the status the device reported for it. */
 int nemo_gpu_sync(void);
 
 /* One full time step (5 stages) with the given dt, replayed from a captured CUDA graph. */
@@ -361,14 +369,16 @@ int nemo_gpu_last_error(char* buf, int32_t len);
 
 /* Stage schedule autotuner (no reference counterpart: the reference has one CPU loop).  For the
    FP32 Euler form it times nsteps full steps of each candidate from the current state -- one CTA per
-   tile of 8 elements plus the mortar kernel, and the persistent kernel with 1 to 4 CTAs per SM
-   (as many as fit) taking the mortar pairs and then the tiles from a device queue -- restores the
-   state, the register, the indicator and the control block after each, and keeps the fastest.
-   mode_out (0 grid, 1 persistent), ctas_out (persistent grid size) and ms_out[5] (ms per step of
-   each candidate, -1 if not run) may be NULL.  Other forms have one schedule (mode 0). */
+   tile of 8, 4 or 16 elements plus the mortar kernel, and the persistent kernel (tiles of 8) with 1
+   to 4 CTAs per SM (as many as fit) taking the mortar pairs and then the tiles from a device queue
+   -- restores the state, the register, the indicator and the control block after each, and keeps
+   the fastest.  mode_out (0 grid with 8 elements per CTA, 1 persistent, 2 grid with 4, 3 grid with
+   16), ctas_out (persistent grid size) and ms_out[8] (ms per step: [0] grid 8, [1..4] persistent at
+   1..4 CTAs per SM, [5] grid 4, [6] grid 16, [7] unused; -1 where not run) may be NULL.  Other forms
+   have one schedule (mode 0). */
 int nemo_gpu_autotune(int32_t nsteps, int32_t* mode_out, int32_t* ctas_out, double* ms_out);
 
-/* Set the FP32 Euler stage schedule directly (mode 0 grid, 1 persistent with ctas CTAs). */
+/* Set the FP32 Euler stage schedule directly (mode as nemo_gpu_autotune's; ctas for mode 1). */
 int nemo_gpu_set_schedule(int32_t mode, int32_t ctas);
 
 /* Timing mode: when on, nemo_gpu_run issues its kernels as plain launches with a CUDA event

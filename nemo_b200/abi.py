@@ -34,7 +34,7 @@ EXPORTS = [
     "nemo_gpu_pack_faces", "nemo_gpu_unpack_faces", "nemo_gpu_measure_peaks", "nemo_gpu_amr_operators",
     "nemo_gpu_repair_states", "nemo_gpu_upload_state_async", "nemo_gpu_upload_wait", "nemo_gpu_run_async",
     "nemo_gpu_sync", "nemo_gpu_set_interior", "nemo_gpu_stage_interior", "nemo_gpu_stage_boundary",
-    "nemo_gpu_glm_speeds", "nemo_gpu_set_glm",
+    "nemo_gpu_glm_speeds", "nemo_gpu_set_glm", "nemo_gpu_download_state_async",
 ]
 
 
@@ -106,6 +106,7 @@ def load(path=LIB_PATH):
         "nemo_gpu_stage_boundary": [i32, dbl, ctypes.POINTER(i32)],
         "nemo_gpu_glm_speeds": [ctypes.POINTER(dbl), ctypes.POINTER(dbl)],
         "nemo_gpu_set_glm": [dbl, dbl],
+        "nemo_gpu_download_state_async": [vp, i64],
         "nemo_gpu_totals_noalloc": [vp, vp, i64, i64, i32, vp, ctypes.c_uint64],
         "nemo_gpu_set_mlp": [vp, i32, vp, vp],
         "nemo_gpu_features": [vp, vp],

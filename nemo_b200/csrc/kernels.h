@@ -79,11 +79,12 @@ cudaError_t launch_repair_states64(double* st, int64_t n, int nv, int mhd, int32
 
 // FP32-bulk Euler path (stage_fp32.cu)
 cudaError_t setup_stage_euler32(const OpConsts& ops);
-cudaError_t launch_stage_euler32(const StageArgs& a, bool blend, bool rhs_only, cudaStream_t s);
+// epc: elements per CTA of the grid schedule, 4, 8 or 16
+cudaError_t launch_stage_euler32(const StageArgs& a, bool blend, bool rhs_only, cudaStream_t s, int epc = 8);
 // persistent FP32 stage with the mortar pairs as its first tasks (grid = CTAs, <= SMs x resident)
 cudaError_t launch_stage_euler32p(const StageArgs& a, const MortarArgs& ma, bool blend, int grid, cudaStream_t s);
 cudaError_t stage32p_max_ctas_per_sm(bool blend, int* n);
-int stage_smem_bytes32();
+int stage_smem_bytes32(int epc);
 
 // GLM-MHD stages (stage_mhd.cuh instantiated in stage_fp64.cu / stage_fp32.cu)
 cudaError_t setup_stage_mhd64();

@@ -242,6 +242,16 @@ struct Lib {
     bool in_used[2] = {false, false};
     int in_next = 0;
     Control* in_ctrl = nullptr;                    // pinned [2]
+
+    // asynchronous downloads (nemo_gpu_download_state_async): two AoS staging slots filled in stream
+    // order by the library stream, copied to the host on their own stream
+    cudaStream_t out_stream = nullptr;
+    double* out_stage[2] = {nullptr, nullptr};
+    int64_t out_bytes = 0;
+    cudaEvent_t out_ready[2] = {nullptr, nullptr};  // the slot holds the snapshot
+    cudaEvent_t out_done[2] = {nullptr, nullptr};   // its device->host copy finished
+    bool out_used[2] = {false, false};
+    int out_next = 0;
 };
 
 Lib g;
@@ -280,6 +290,16 @@ void release_checkpoint() {
     g.ckpt_bytes = 0;
 }
 
+void release_downloads() {
+    for (int i = 0; i < 2; ++i) {
+        if (g.out_used[i]) cudaEventSynchronize(g.out_done[i]);
+        g.out_used[i] = false;
+        free_dev(g.out_stage[i]);
+        g.out_stage[i] = nullptr;
+    }
+    g.out_bytes = 0;
+}
+
 void release_uploads() {
     for (int i = 0; i < 2; ++i) {
         if (g.in_used[i]) cudaEventSynchronize(g.in_free[i]);
@@ -293,6 +313,7 @@ void release_uploads() {
 void release_mesh() {
     release_checkpoint();
     release_uploads();
+    release_downloads();
     release_graphs();
     free_dev(g.u[0]); free_dev(g.u[1]); free_dev(g.reg); free_dev(g.stagebuf);
     free_dev(g.alpha[0]); free_dev(g.alpha[1]); free_dev(g.alpha_used);
@@ -396,7 +417,8 @@ cudaError_t launch_stage_any(const StageArgs& a, bool rhs_only, cudaStream_t s) 
         if (g.cfg.precision == NEMO_PREC_FP32) return launch_stage_mhd32(a, blended(), rhs_only, s);
         return launch_stage_mhd64(a, blended(), rhs_only, s);
     }
-    if (g.cfg.precision == NEMO_PREC_FP32) return launch_stage_euler32(a, blended(), rhs_only, s);
+    if (g.cfg.precision == NEMO_PREC_FP32)
+        return launch_stage_euler32(a, blended(), rhs_only, s, g.tune_mode == 2 ? 4 : (g.tune_mode == 3 ? 16 : 8));
     return launch_stage_euler64(a, blended(), blended(), rhs_only, s);
 }
 
@@ -1009,6 +1031,40 @@ int nemo_gpu_upload_state_async(const double* host, int64_t stride) {
     return NEMO_OK;
 }
 
+int nemo_gpu_download_state_async(double* host, int64_t stride) {
+    int st = ensure_ready();
+    if (st) return st;
+    if (!host) return fail(NEMO_ERR_ARG, "host is NULL");
+    const size_t row = sizeof(double) * (size_t)g.V * NP;
+    if (stride < (int64_t)row) return fail(NEMO_ERR_ARG, "element stride %lld < %zu bytes", (long long)stride, row);
+    if (!g.out_stream) CK(cudaStreamCreateWithFlags(&g.out_stream, cudaStreamNonBlocking));
+    for (int i = 0; i < 2; ++i) {
+        if (!g.out_ready[i]) CK(cudaEventCreateWithFlags(&g.out_ready[i], cudaEventDisableTiming));
+        if (!g.out_done[i]) CK(cudaEventCreateWithFlags(&g.out_done[i], cudaEventDisableTiming));
+    }
+    const int64_t bytes = (int64_t)row * g.E;
+    if (g.out_bytes != bytes) {
+        release_downloads();
+        for (int i = 0; i < 2; ++i) CK(cudaMalloc(&g.out_stage[i], (size_t)bytes));
+        g.out_bytes = bytes;
+    }
+    const int s = g.out_next;
+    // the slot's previous copy must have left the staging buffer (two downloads ago)
+    if (g.out_used[s]) CK(cudaEventSynchronize(g.out_done[s]));
+    CK(launch_soa_to_aos(g.u[g.cur], g.out_stage[s], g.E, g.V, g.stream));
+    CK(cudaEventRecord(g.out_ready[s], g.stream));
+    CK(cudaStreamWaitEvent(g.out_stream, g.out_ready[s], 0));
+    if (stride == (int64_t)row)
+        CK(cudaMemcpyAsync(host, g.out_stage[s], (size_t)bytes, cudaMemcpyDeviceToHost, g.out_stream));
+    else
+        CK(cudaMemcpy2DAsync(host, (size_t)stride, g.out_stage[s], row, row, (size_t)g.E, cudaMemcpyDeviceToHost,
+                             g.out_stream));
+    CK(cudaEventRecord(g.out_done[s], g.out_stream));
+    g.out_used[s] = true;
+    g.out_next = s ^ 1;
+    return NEMO_OK;
+}
+
 int nemo_gpu_upload_wait(void) {
     for (int i = 0; i < 2; ++i)
         if (g.in_used[i]) CK(cudaEventSynchronize(g.in_done[i]));
@@ -1245,6 +1301,7 @@ int nemo_gpu_run_async(int64_t nsteps) {
 int nemo_gpu_sync(void) {
     if (!g.inited) return fail(NEMO_ERR_STATE, "nemo_gpu_init has not been called");
     if (g.in_stream) CK(cudaStreamSynchronize(g.in_stream));
+    if (g.out_stream) CK(cudaStreamSynchronize(g.out_stream));
     if (g.copy_stream) CK(cudaStreamSynchronize(g.copy_stream));
     CK(cudaStreamSynchronize(g.stream));
     if (g.has_mesh) return check_ctrl_error();
@@ -1395,7 +1452,7 @@ int nemo_gpu_autotune(int32_t nsteps, int32_t* mode_out, int32_t* ctas_out, doub
     if (st) return st;
     if (nsteps < 1 || nsteps > 1000) return fail(NEMO_ERR_ARG, "nsteps must be in [1, 1000]");
     if (ms_out)
-        for (int i = 0; i < 5; ++i) ms_out[i] = -1.0;
+        for (int i = 0; i < 8; ++i) ms_out[i] = -1.0;
     const bool tunable = !is_mhd() && g.cfg.precision == NEMO_PREC_FP32;
     if (!tunable) {  // the other forms have a single schedule
         g.tune_mode = 0;
@@ -1459,13 +1516,22 @@ int nemo_gpu_autotune(int32_t nsteps, int32_t* mode_out, int32_t* ctas_out, doub
     if (e == cudaSuccess) e = save_or_restore(false, ctrial);
     double best = 1e300;
     int best_mode = 0, best_ctas = 0;
-    const int ncand = 1 + std::min(occ, 4);
+    // candidates (mode, CTAs, slot of ms_out): the grid schedule at 8, 4 and 16 elements per CTA, the
+    // persistent kernel at 1..4 CTAs per SM (as many as fit)
+    struct Cand { int mode, ctas, slot; };
+    Cand cand[8];
+    int ncand = 0;
+    cand[ncand++] = {0, 0, 0};
+    for (int c = 1; c <= std::min(occ, 4); ++c) cand[ncand++] = {1, nsm * c, c};
+    cand[ncand++] = {2, 0, 5};
+    cand[ncand++] = {3, 0, 6};
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     if (e == cudaSuccess) e = cudaEventCreate(&e0);
     if (e == cudaSuccess) e = cudaEventCreate(&e1);
-    for (int c = 0; c < ncand && e == cudaSuccess; ++c) {
-        g.tune_mode = c == 0 ? 0 : 1;
-        g.tune_ctas = c == 0 ? 0 : nsm * c;
+    for (int ci = 0; ci < ncand && e == cudaSuccess; ++ci) {
+        g.tune_mode = cand[ci].mode;
+        g.tune_ctas = cand[ci].ctas;
+        const int c = cand[ci].slot;
         // one untimed step (first-launch costs), then nsteps timed steps, from the same state
         for (int rep = 0; rep < 2 && e == cudaSuccess; ++rep) {
             const int n = rep == 0 ? 1 : nsteps;
@@ -1509,7 +1575,8 @@ int nemo_gpu_autotune(int32_t nsteps, int32_t* mode_out, int32_t* ctas_out, doub
 
 int nemo_gpu_set_schedule(int32_t mode, int32_t ctas) {
     if (!g.inited) return fail(NEMO_ERR_STATE, "nemo_gpu_init has not been called");
-    if (mode != 0 && mode != 1) return fail(NEMO_ERR_ARG, "mode must be 0 (grid) or 1 (persistent)");
+    if (mode < 0 || mode > 3)
+        return fail(NEMO_ERR_ARG, "mode must be 0 (grid, 8 elements per CTA), 1 (persistent), 2 (grid, 4) or 3 (grid, 16)");
     if (mode == 1) {
         int nsm = 0, dev = 0, occ = 0;
         CK(cudaGetDevice(&dev));
@@ -1740,6 +1807,14 @@ int nemo_gpu_finalize(void) {
     g.in_ctrl = nullptr;
     g.in_stream = nullptr;
     g.in_next = 0;
+    for (int i = 0; i < 2; ++i) {   // release_mesh released the staging slots
+        if (g.out_ready[i]) cudaEventDestroy(g.out_ready[i]);
+        if (g.out_done[i]) cudaEventDestroy(g.out_done[i]);
+        g.out_ready[i] = g.out_done[i] = nullptr;
+    }
+    if (g.out_stream) cudaStreamDestroy(g.out_stream);
+    g.out_stream = nullptr;
+    g.out_next = 0;
     g.ctrl = nullptr;
     g.tot = nullptr;
     g.mlp32 = nullptr;

@@ -23,9 +23,10 @@ __constant__ OpConsts c_ops32;
 
 namespace {
 
-constexpr int EPC = 8;          // elements per CTA
-constexpr int TPE = 16;         // threads per element, one per line position (a,b)
-constexpr int NT = EPC * TPE;   // 128 threads: a warp holds exactly two elements
+constexpr int EPC8 = 8;         // elements per CTA of the persistent kernel (the grid kernel takes 4, 8
+                                // or 16 as a template parameter; the autotuner picks)
+constexpr int TPE = 16;         // threads per element, one per line position (a,b): a warp holds
+                                // exactly two elements
 constexpr int V = 5;
 constexpr int NQ = 6;           // FP32 node data: rho, vx, vy, vz, p, beta
 // element stride of the FP32 shared-memory arrays (node data, rhs terms, epilogue scratch): the 6
@@ -55,6 +56,7 @@ __device__ __forceinline__ bool mbar_wait32(uint64_t* bar, unsigned phase) {
 // contiguous per variable), completing on the CTA's mbarrier (initialised once by mbar_init32; one
 // phase per tile).  The RK register does not pass through shared memory: the update reads and
 // writes it straight from global memory with coalesced accesses, after an L2 prefetch issued here.
+template <int EPC>
 __device__ __forceinline__ void tile_issue32(double* su, const double* __restrict__ u,
                                              const double* __restrict__ reg, int64_t E, int64_t e0, int nel,
                                              uint64_t* bar) {
@@ -89,6 +91,7 @@ __device__ __forceinline__ bool tile_wait32(uint64_t* bar, unsigned phase, Contr
 
 // Write the tile's new state back with 1D bulk copies from shared memory.  The calling thread waits
 // until the copies have read shared memory before the CTA may reuse or leave it.
+template <int EPC>
 __device__ __forceinline__ void tile_store32(const double* su, double* __restrict__ u_out, int64_t E, int64_t e0,
                                              int nel) {
     const unsigned bytes = (unsigned)(nel * NP * 8);
@@ -263,6 +266,7 @@ __device__ __forceinline__ float tsum16(float (&v)[16], int l) {
     return v[0];
 }
 
+template <int EPC>
 __device__ __forceinline__ void epilogue32(const StageArgs& a, const double* su, float* scratch, const float* sw,
                                            int el, int ab, int la, int lb, bool active, int64_t e,
                                            const OpConsts& k) {
@@ -529,7 +533,9 @@ struct Smem32 {
     const float* s_w;  // learned indicator, transposed layout (shared memory, or global through L1)
 };
 
+template <int EPC>
 __device__ __forceinline__ void load_mlp32(const StageArgs& a, float* s_w) {
+    constexpr int NT = EPC * TPE;
     if (a.mlp32t) {  // visible to the epilogue after the barriers of the stage
         const float4* src = reinterpret_cast<const float4*>(a.mlp32t);
         float4* dst = reinterpret_cast<float4*>(s_w);
@@ -537,6 +543,7 @@ __device__ __forceinline__ void load_mlp32(const StageArgs& a, float* s_w) {
     }
 }
 
+template <int EPC>
 __device__ __forceinline__ Smem32 smem32(double* smem, uint64_t* bar, float* s_alpha, int* s_bad, const float* s_w) {
     Smem32 S;
     S.su = smem;
@@ -571,7 +578,7 @@ __device__ __forceinline__ void mbar_init32(uint64_t* bar) {
 // One tile of EPC elements (tile index `tile`, TMA barrier parity `phase`): thread (a,b) of an
 // element owns the x-, y- and z-lines through (a,b) and processes them one direction after the
 // other, accumulating into one shared rhs array (x, then y, then z).  A warp holds two elements.
-template <bool BLEND, bool RHS_ONLY, bool PERSIST>
+template <int EPC, bool BLEND, bool RHS_ONLY, bool PERSIST>
 __device__ __forceinline__ void tile32(const StageArgs& a, const Smem32& S, int64_t tile, unsigned phase,
                                        uint32_t epoch) {
     const OpConsts& k = c_ops32;
@@ -606,7 +613,7 @@ __device__ __forceinline__ void tile32(const StageArgs& a, const Smem32& S, int6
         s_alpha[tid] = al;
     }
     const bool load_reg = !RHS_ONLY && !a.prep_only && a.stage > 0;
-    tile_issue32(su, a.u_in, load_reg ? a.reg : nullptr, E, e0, nel, S.bar);
+    tile_issue32<EPC>(su, a.u_in, load_reg ? a.reg : nullptr, E, e0, nel, S.bar);
     __syncthreads();   // s_alpha / s_bad visible
     if (!tile_wait32(S.bar, phase, ctrl)) return;
 
@@ -615,7 +622,7 @@ __device__ __forceinline__ void tile32(const StageArgs& a, const Smem32& S, int6
     const int64_t e = e0 + el;
     if (a.prep_only) {
         __syncthreads();
-        epilogue32(a, su, sq, s_w, el, ab, la, lb, active, e, k);
+        epilogue32<EPC>(a, su, sq, s_w, el, ab, la, lb, active, e, k);
         return;
     }
     auto SQ = [&](int q, int elx, int n) -> float& { return sq[(q * EPC + elx) * SP + n]; };
@@ -859,19 +866,19 @@ __device__ __forceinline__ void tile32(const StageArgs& a, const Smem32& S, int6
     // make the generic-proxy writes of su visible to the bulk copies, then store the tile
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncthreads();
-    if (tid == 0) tile_store32(su, a.u_out, E, e0, nel);
+    if (tid == 0) tile_store32<EPC>(su, a.u_out, E, e0, nel);
     if (st == 4 && a.tick && tile == 0 && tid == 0) {
         for (int g = 0; g < ctrl->ngroups; ++g) ctrl->t[g] = ctrl->t[g] + ctrl->dt[g];
         ctrl->steps += 1;
     }
 
-    epilogue32(a, su, sq, s_w, el, ab, la, lb, active, e, k);
+    epilogue32<EPC>(a, su, sq, s_w, el, ab, la, lb, active, e, k);
     if (tid == 0) tile_store_wait32();
 }
 
 
-template <bool BLEND, bool RHS_ONLY>
-__global__ void __launch_bounds__(NT, 4) k_stage_euler32(StageArgs a) {
+template <int EPC, bool BLEND, bool RHS_ONLY>
+__global__ void __launch_bounds__(EPC * TPE, 32 / EPC) k_stage_euler32(StageArgs a) {
     extern __shared__ __align__(128) double smem[];
     __shared__ uint64_t bar[1];
     __shared__ float s_alpha[EPC];
@@ -879,9 +886,9 @@ __global__ void __launch_bounds__(NT, 4) k_stage_euler32(StageArgs a) {
     if (!RHS_ONLY && !a.prep_only && a.ctrl->done) return;
     // the learned indicator's weights are read through L1 by the epilogue (a CTA handles one tile:
     // a shared-memory copy of the 6 KB per CTA would cost more L2 reads than it saves)
-    const Smem32 S = smem32(smem, bar, s_alpha, s_bad, a.mlp32t);
+    const Smem32 S = smem32<EPC>(smem, bar, s_alpha, s_bad, a.mlp32t);
     mbar_init32(bar);
-    tile32<BLEND, RHS_ONLY, false>(a, S, (int64_t)blockIdx.x, 0u, 0u);
+    tile32<EPC, BLEND, RHS_ONLY, false>(a, S, (int64_t)blockIdx.x, 0u, 0u);
 }
 
 // Persistent form: gridDim.x CTAs (a multiple of the SM count) take tasks from a device counter --
@@ -890,7 +897,8 @@ __global__ void __launch_bounds__(NT, 4) k_stage_euler32(StageArgs a) {
 // was taken before any tile task, by a running CTA that waits on nothing, so the waits end.  The
 // last CTA to finish resets the counter and advances the epoch for the next launch.
 template <bool BLEND>
-__global__ void __launch_bounds__(NT, 4) k_stage_euler32p(StageArgs a, MortarArgs ma) {
+__global__ void __launch_bounds__(EPC8 * TPE, 4) k_stage_euler32p(StageArgs a, MortarArgs ma) {
+    constexpr int EPC = EPC8;
     extern __shared__ __align__(128) double smem[];
     __shared__ uint64_t bar[1];
     __shared__ float s_alpha[EPC];
@@ -901,8 +909,8 @@ __global__ void __launch_bounds__(NT, 4) k_stage_euler32p(StageArgs a, MortarArg
     if (ctrl->done) return;
     const uint32_t epoch = ctrl->epoch;
     ma.epoch = epoch;
-    load_mlp32(a, s_w);
-    const Smem32 S = smem32(smem, bar, s_alpha, s_bad, s_w);
+    load_mlp32<EPC>(a, s_w);
+    const Smem32 S = smem32<EPC>(smem, bar, s_alpha, s_bad, s_w);
     mbar_init32(bar);
     const int64_t ntiles = (a.E_own - a.E_begin + EPC - 1) / EPC;
     const int64_t npairs = (ma.nm + mortar::MPB - 1) / mortar::MPB;
@@ -919,7 +927,7 @@ __global__ void __launch_bounds__(NT, 4) k_stage_euler32p(StageArgs a, MortarArg
         }
         const int64_t tile = task - npairs;
         if (tile >= ntiles) break;
-        tile32<BLEND, false, true>(a, S, tile, phase, epoch);
+        tile32<EPC, BLEND, false, true>(a, S, tile, phase, epoch);
         phase ^= 1u;
     }
     if (threadIdx.x == 0) {
@@ -934,22 +942,29 @@ __global__ void __launch_bounds__(NT, 4) k_stage_euler32p(StageArgs a, MortarArg
     }
 }
 
-int stage_smem_bytes32() {
-    return V * EPC * NP * (int)sizeof(double) + (NQ + V) * EPC * SP * (int)sizeof(float);
+int stage_smem_bytes32(int epc) {
+    return V * epc * NP * (int)sizeof(double) + (NQ + V) * epc * SP * (int)sizeof(float);
 }
 
-cudaError_t launch_stage_euler32(const StageArgs& a, bool blend, bool rhs_only, cudaStream_t s) {
+template <int EPC>
+static cudaError_t launch32(const StageArgs& a, bool blend, bool rhs_only, cudaStream_t s) {
     const int grid = (int)((a.E_own - a.E_begin + EPC - 1) / EPC);
     if (grid <= 0) return cudaSuccess;
-    const int smem = stage_smem_bytes32();
+    const int smem = stage_smem_bytes32(EPC), nt = EPC * TPE;
     if (rhs_only) {
-        if (blend) k_stage_euler32<true, true><<<grid, NT, smem, s>>>(a);
-        else k_stage_euler32<false, true><<<grid, NT, smem, s>>>(a);
+        if (blend) k_stage_euler32<EPC, true, true><<<grid, nt, smem, s>>>(a);
+        else k_stage_euler32<EPC, false, true><<<grid, nt, smem, s>>>(a);
     } else {
-        if (blend) k_stage_euler32<true, false><<<grid, NT, smem, s>>>(a);
-        else k_stage_euler32<false, false><<<grid, NT, smem, s>>>(a);
+        if (blend) k_stage_euler32<EPC, true, false><<<grid, nt, smem, s>>>(a);
+        else k_stage_euler32<EPC, false, false><<<grid, nt, smem, s>>>(a);
     }
     return cudaGetLastError();
+}
+
+cudaError_t launch_stage_euler32(const StageArgs& a, bool blend, bool rhs_only, cudaStream_t s, int epc) {
+    if (epc == 4) return launch32<4>(a, blend, rhs_only, s);
+    if (epc == 16) return launch32<16>(a, blend, rhs_only, s);
+    return launch32<8>(a, blend, rhs_only, s);
 }
 
 template <typename K>
@@ -960,30 +975,39 @@ static cudaError_t set_attrs32(K kernel, int smem) {
 }
 
 cudaError_t launch_stage_euler32p(const StageArgs& a, const MortarArgs& ma, bool blend, int grid, cudaStream_t s) {
-    const int smem = stage_smem_bytes32();
-    if (blend) k_stage_euler32p<true><<<grid, NT, smem, s>>>(a, ma);
-    else k_stage_euler32p<false><<<grid, NT, smem, s>>>(a, ma);
+    const int smem = stage_smem_bytes32(EPC8);
+    if (blend) k_stage_euler32p<true><<<grid, EPC8 * TPE, smem, s>>>(a, ma);
+    else k_stage_euler32p<false><<<grid, EPC8 * TPE, smem, s>>>(a, ma);
     return cudaGetLastError();
 }
 
 cudaError_t stage32p_max_ctas_per_sm(bool blend, int* n) {
-    const int smem = stage_smem_bytes32();
-    if (blend) return cudaOccupancyMaxActiveBlocksPerMultiprocessor(n, k_stage_euler32p<true>, NT, smem);
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(n, k_stage_euler32p<false>, NT, smem);
+    const int smem = stage_smem_bytes32(EPC8);
+    if (blend) return cudaOccupancyMaxActiveBlocksPerMultiprocessor(n, k_stage_euler32p<true>, EPC8 * TPE, smem);
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(n, k_stage_euler32p<false>, EPC8 * TPE, smem);
+}
+
+template <int EPC>
+static cudaError_t setup32() {
+    // the grid-schedule kernels leave the shared-memory carveout to the driver: it keeps 4 CTAs per
+    // SM (8 elements per CTA) and more L1 than the largest carveout would (1 % faster per stage on B200)
+    const auto dyn = cudaFuncAttributeMaxDynamicSharedMemorySize;
+    const int smem = stage_smem_bytes32(EPC);
+    cudaError_t err;
+    if ((err = cudaFuncSetAttribute(k_stage_euler32<EPC, true, true>, dyn, smem)) != cudaSuccess) return err;
+    if ((err = cudaFuncSetAttribute(k_stage_euler32<EPC, false, true>, dyn, smem)) != cudaSuccess) return err;
+    if ((err = cudaFuncSetAttribute(k_stage_euler32<EPC, true, false>, dyn, smem)) != cudaSuccess) return err;
+    return cudaFuncSetAttribute(k_stage_euler32<EPC, false, false>, dyn, smem);
 }
 
 cudaError_t setup_stage_euler32(const OpConsts& ops) {
-    const int smem = stage_smem_bytes32();
+    const int smem = stage_smem_bytes32(EPC8);
     cudaError_t err;
     if ((err = set_attrs32(k_stage_euler32p<true>, smem)) != cudaSuccess) return err;
     if ((err = set_attrs32(k_stage_euler32p<false>, smem)) != cudaSuccess) return err;
-    // the grid-schedule kernels leave the shared-memory carveout to the driver: it keeps 4 CTAs per
-    // SM and more L1 than the largest carveout would (1 % faster per stage on B200)
-    const auto dyn = cudaFuncAttributeMaxDynamicSharedMemorySize;
-    if ((err = cudaFuncSetAttribute(k_stage_euler32<true, true>, dyn, smem)) != cudaSuccess) return err;
-    if ((err = cudaFuncSetAttribute(k_stage_euler32<false, true>, dyn, smem)) != cudaSuccess) return err;
-    if ((err = cudaFuncSetAttribute(k_stage_euler32<true, false>, dyn, smem)) != cudaSuccess) return err;
-    if ((err = cudaFuncSetAttribute(k_stage_euler32<false, false>, dyn, smem)) != cudaSuccess) return err;
+    if ((err = setup32<4>()) != cudaSuccess) return err;
+    if ((err = setup32<8>()) != cudaSuccess) return err;
+    if ((err = setup32<16>()) != cudaSuccess) return err;
     return cudaMemcpyToSymbol(c_ops32, &ops, sizeof(OpConsts));
 }
 

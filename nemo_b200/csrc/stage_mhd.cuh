@@ -22,8 +22,16 @@
 namespace nemo {
 namespace mhd {
 
-constexpr int EPC = 8;
-constexpr int NT = 128;
+// Tile shape (compile-time knobs for tuning builds): elements per CTA (16 threads each) and, for the
+// plain FP64 form, the minimum number of resident CTAs per SM asked of the register allocator.
+#ifndef NEMO_MHD_EPC
+#define NEMO_MHD_EPC 8
+#endif
+#ifndef NEMO_MHD64_MINB
+#define NEMO_MHD64_MINB 1
+#endif
+constexpr int EPC = NEMO_MHD_EPC;
+constexpr int NT = 16 * EPC;
 constexpr int V = 9;
 // element stride of the rhs array: 6 words of padding move the two elements of a warp onto
 // different banks (as in the Euler FP32 stage; 0.7 % faster per FP32 stage at 64^3)
@@ -412,7 +420,7 @@ __device__ void epilogue_mhd(const StageArgs& a, const double* su, R* scr, unsig
 // pair fluxes cheaper but the stage 4 % slower, as the larger carveout left L1 too small for the
 // neighbour traces and register rows.
 template <typename R, bool BLEND, bool RHS_ONLY>
-__global__ void __launch_bounds__(mhd::NT, sizeof(R) == 4 ? 3 : 1) k_stage_mhd(StageArgs a) {
+__global__ void __launch_bounds__(mhd::NT, sizeof(R) == 4 ? 3 : NEMO_MHD64_MINB) k_stage_mhd(StageArgs a) {
     constexpr int MEPC = mhd::EPC, MV = mhd::V;
     using mhd::load_rot;
     using mhd::load_rot_global;

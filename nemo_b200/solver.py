@@ -81,15 +81,12 @@ class Solver:
         call("nemo_gpu_run_async", int(nsteps))
 
     def download_async(self, aos, stride_bytes):
-        """Start the device->host copy of the state after the enqueued steps (checkpoint staging)."""
-        call("nemo_gpu_checkpoint_begin", ctypes.c_void_p(aos), int(stride_bytes), None)
-        self._download_pending = True
+        """Start the device->host copy of the state after the enqueued steps into a pinned host buffer
+        laid out like the reference's quad array (nemo_gpu_download_state_async)."""
+        call("nemo_gpu_download_state_async", ctypes.c_void_p(aos), int(stride_bytes))
 
     def sync(self):
         """Wait for everything enqueued (steps and copies); raise what the device reported."""
-        if getattr(self, "_download_pending", False):
-            call("nemo_gpu_checkpoint_wait", ctypes.byref(ctypes.c_double()), ctypes.byref(ctypes.c_int64()))
-            self._download_pending = False
         call("nemo_gpu_sync")
 
     def upload_aos(self, aos, stride_bytes):
@@ -135,7 +132,7 @@ class Solver:
         """Pick the stage schedule by timing (FP32 Euler form); returns (mode, ctas, ms per step of
         each candidate)."""
         mode, ctas = ctypes.c_int32(), ctypes.c_int32()
-        ms = np.zeros(5)
+        ms = np.zeros(8)
         call("nemo_gpu_autotune", int(nsteps), ctypes.byref(mode), ctypes.byref(ctas), abi.ptr(ms))
         return mode.value, ctas.value, ms
 

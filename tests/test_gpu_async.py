@@ -1,5 +1,5 @@
 """GPU tests of the asynchronous path through the C-ABI: nemo_gpu_upload_state_async,
-nemo_gpu_run_async and the checkpoint staging as the asynchronous download.  States streamed through
+nemo_gpu_run_async and nemo_gpu_download_state_async (two staging slots each way).  States streamed through
 the library this way give, bit for bit, what the synchronous calls give, each download matching its
 own upload even when the uploads of later states are already in flight."""
 import ctypes

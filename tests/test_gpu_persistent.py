@@ -65,12 +65,23 @@ def test_autotune_keeps_state_and_picks_a_schedule():
     s = Solver(abi.default_cfg(precision=abi.PREC_FP32, indicator=abi.IND_MODAL), m)
     s.upload(u)
     mode, ctas, ms = s.autotune(nsteps=2)
-    assert mode in (0, 1) and (mode == 0 or ctas >= 148)
-    assert np.all(ms[:2] > 0)
+    assert mode in (0, 1, 2, 3) and (mode != 1 or ctas >= 148)
+    assert np.all(ms[:2] > 0) and ms[5] > 0 and ms[6] > 0 and ms[7] == -1.0
     assert np.array_equal(s.download(), u)
     assert s.status()[0] == 0.0
     t, n = s.run(nsteps=3)
     got = s.download()
     s.finalize()
     ref, tr = run_with(m, u, (0, 0), nsteps=3)
+    assert t == tr and np.array_equal(got, ref)
+
+
+@pytest.mark.parametrize("mode", [2, 3])
+def test_grid_tile_sizes_match_the_default_tile(mode):
+    """The grid schedule with 4 or 16 elements per CTA gives what 8 elements per CTA give (the
+    element arithmetic does not depend on the tile)."""
+    m = mesh.brick(8, lo=(-0.5,) * 3, hi=(0.5,) * 3)
+    u = setups.sedov(m, sigma=0.05)
+    ref, tr = run_with(m, u, (0, 0), nsteps=4)
+    got, t = run_with(m, u, (mode, 0), nsteps=4)
     assert t == tr and np.array_equal(got, ref)
