@@ -343,6 +343,44 @@ def roofline_of(bytes_per_launch, flops_per_launch, avg_s, hbm_gbs, peak_tflops,
     return out
 
 
+def measure_secondary(wl, args, peaks, torch, ctypes, abi):
+    """Device throughput of the chosen and the plain form on another workload (same steps and
+    warm-up as the main one, per-kernel CUDA events, schedule by the autotuner)."""
+    m, u, groups = make_state(wl)
+    V = nvars(wl)
+    mhd = bool(WORKLOADS[wl].get("mhd"))
+    dof_per_step = m.E * 64 * 5
+    bytes_per_launch = sum(m.E * 64 * V * 8 * (3 if st == 0 else 4) for st in range(5)) / 5.0
+    flops_dof = load_flops(wl)
+    hbm, _ = load_peaks()
+    out = {"workload": WORKLOADS[wl]["desc"], "elements": int(m.E), "nodes": int(m.E * 64)}
+    stream_ptr = ctypes.c_uint64()
+    for key in ("fp64_modal", "fp32_modal"):
+        prec, learned = FORMS[key]
+        s = make_solver(wl, m, prec, learned, groups)
+        s.upload(u)
+        sched = None
+        if prec == abi.PREC_FP32:
+            mode, _, _ = s.autotune(nsteps=2)
+            sched = SCHEDULES[mode]
+        abi.call("nemo_gpu_stream", ctypes.byref(stream_ptr))
+        stream = torch.cuda.ExternalStream(stream_ptr.value)
+        s.run(nsteps=args.warmup)
+        ms, st_ms, st_n, _, _, _, _ = timed_run(s, args.steps, stream, None, torch, ctypes, abi)
+        s.finalize()
+        avg_s = st_ms * 1e-3 / max(st_n, 1)
+        rf = roofline_of(bytes_per_launch, flops_dof * m.E * 64 if flops_dof else None, avg_s, hbm,
+                         peaks["fp32_tflops"] if prec == abi.PREC_FP32 else peaks["fp64_tflops"],
+                         "fp32" if prec == abi.PREC_FP32 else "fp64")
+        out[key] = {"value": dof_per_step * args.steps / (ms * 1e-3), "unit": "DOF-updates/s",
+                    "ms_per_step": ms / args.steps, "avg_stage_ms": avg_s * 1e3, "schedule": sched,
+                    "kernel": ("k_stage_mhd<float>" if mhd else "k_stage_euler32") if prec else
+                              ("k_stage_mhd<double>" if mhd else "k_stage_euler64"),
+                    "roofline": rf}
+    out["chosen_form_speedup"] = out["fp32_modal"]["value"] / out["fp64_modal"]["value"]
+    return out
+
+
 def run_partitioned(args, rank, world, local, dist, torch):
     """N > 1: one domain split over the ranks (strong scaling).  Each rank advances its contiguous
     Morton range of elements plus ghost copies of their face neighbours with the chosen form (FP32
@@ -450,6 +488,9 @@ def main():  # noqa: C901
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
     ap.add_argument("--no-accuracy", action="store_true", help="skip the run to t_end that checks the L1 error")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-indicator form (profiling runs)")
+    ap.add_argument("--secondary", default="batch,ot64",
+                    help="further workloads timed in the same run (chosen and plain form, device throughput "
+                         "only; comma-separated, empty for none)")
     ap.add_argument("--schedule", default="auto", choices=["auto", "grid", "persistent"],
                     help="FP32 stage schedule: autotuned (default) or fixed (profiling runs)")
     args = ap.parse_args()
@@ -610,6 +651,10 @@ def main():  # noqa: C901
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(args.workload, u, m)
 
+    secondary = {}
+    for wl2 in [w for w in args.secondary.split(",") if w and w != args.workload]:
+        secondary[wl2] = measure_secondary(wl2, args, peaks, torch, ctypes, abi)
+
     if rank == 0:
         rf = chosen["roofline"]
         line = {
@@ -660,6 +705,8 @@ def main():  # noqa: C901
         line["plain_fp64"] = forms.pop("fp64_modal")
         line["other_forms"] = forms
         line["accuracy"] = accuracy
+        if secondary:
+            line["secondary_workloads"] = secondary
         if cpu:
             line["cpu_baseline"] = cpu
         line["pid"] = {"chosen": 1e6 * world / value, "plain_fp64": 1e6 * world / line["plain_fp64"]["value"],
