@@ -704,25 +704,20 @@ __device__ __forceinline__ void tile32(const StageArgs& a, const Smem32& S, int6
                         qn.p = SQ(4, nli, nn);
                         qn.E = qn.p * ikm1 + 0.5f * qn.rho * (qn.vn * qn.vn + qn.vt1 * qn.vt1 + qn.vt2 * qn.vt2);
                     } else {
-                        // out-of-tile trace (L2 only, each node read once per CTA), its primitives
-                        // recovered exactly as the tile's own (same operations, x-y-z order), so the
-                        // result does not depend on which neighbours share the CTA's tile
-                        const double* g = a.u_in;
+                        const double* g = a.u_in;   // out-of-tile trace: L2 only, each node read once per CTA
                         const double r = __ldcg(g + ((int64_t)0 * E + ne) * NP + nn);
-                        const double mx = __ldcg(g + ((int64_t)1 * E + ne) * NP + nn);
-                        const double my = __ldcg(g + ((int64_t)2 * E + ne) * NP + nn);
-                        const double mz = __ldcg(g + ((int64_t)3 * E + ne) * NP + nn);
+                        const double m0 = __ldcg(g + ((int64_t)(1 + c0) * E + ne) * NP + nn);
+                        const double m1 = __ldcg(g + ((int64_t)(1 + c1) * E + ne) * NP + nn);
+                        const double m2 = __ldcg(g + ((int64_t)(1 + c2) * E + ne) * NP + nn);
                         const double en = __ldcg(g + ((int64_t)4 * E + ne) * NP + nn);
-                        const double ir = rcp64(r);
-                        const double vx = mx * ir, vy = my * ir, vz = mz * ir;
-                        const double pr = k.km1 * (en - 0.5 * (mx * vx + my * vy + mz * vz));
-                        const float vf[3] = {(float)vx, (float)vy, (float)vz};
+                        const double ir = 1.0 / r;
+                        const double v0 = m0 * ir, v1 = m1 * ir, v2 = m2 * ir;
                         qn.rho = (float)r;
-                        qn.vn = vf[c0];
-                        qn.vt1 = vf[c1];
-                        qn.vt2 = vf[c2];
-                        qn.p = (float)pr;
-                        qn.E = qn.p * ikm1 + 0.5f * qn.rho * (qn.vn * qn.vn + qn.vt1 * qn.vt1 + qn.vt2 * qn.vt2);
+                        qn.vn = (float)v0;
+                        qn.vt1 = (float)v1;
+                        qn.vt2 = (float)v2;
+                        qn.p = (float)(k.km1 * (en - 0.5 * (m0 * v0 + m1 * v1 + m2 * v2)));
+                        qn.E = (float)en;
                     }
                 }
                 if (side) riemann32(a.surface_flux, qo, qn, Fs[1], k);
