@@ -647,7 +647,16 @@ cudaError_t launch_totals64(const double* u, const double* delta, int64_t E, int
 }
 
 
-// ---- GLM-MHD stage (double flux arithmetic)
+// ---- GLM-MHD stage (double flux arithmetic).  Tile of the plain form: 4 elements (64 threads) with
+// at least 4 CTAs per SM at the full 255 registers (Orszag-Tang 64^3, B200: 12.81 ms per stage against
+// 13.21 ms for 8 elements x 1-2 CTAs/SM; 2 elements x 8 CTAs 12.81 ms; 4 x 5 at 168 registers
+// 15.89 ms; bit-identical results).  The FP32 form keeps its 8-element tile (stage_fp32.cu).
+#ifndef NEMO_MHD_EPC
+#define NEMO_MHD_EPC 4
+#endif
+#ifndef NEMO_MHD64_MINB
+#define NEMO_MHD64_MINB 4
+#endif
 #define NEMO_MHD_OPS c_ops64
 }  // namespace nemo
 #include "stage_mhd.cuh"
