@@ -594,6 +594,9 @@ __device__ __forceinline__ void tile32(const StageArgs& a, const Smem32& S, int6
     const int64_t e0 = a.E_begin + tile * EPC;
     const int nel = (int)min((int64_t)EPC, a.E_own - e0);
 
+    // the tile's bulk copy first, so that it is in flight while the blending coefficients are read
+    const bool load_reg = !RHS_ONLY && !a.prep_only && a.stage > 0;
+    tile_issue32<EPC>(su, a.u_in, load_reg ? a.reg : nullptr, E, e0, nel, S.bar);
     if (tid < EPC) {
         s_bad[tid] = 0;
         float al = 0.0f;
@@ -612,8 +615,6 @@ __device__ __forceinline__ void tile32(const StageArgs& a, const Smem32& S, int6
         }
         s_alpha[tid] = al;
     }
-    const bool load_reg = !RHS_ONLY && !a.prep_only && a.stage > 0;
-    tile_issue32<EPC>(su, a.u_in, load_reg ? a.reg : nullptr, E, e0, nel, S.bar);
     __syncthreads();   // s_alpha / s_bad visible
     if (!tile_wait32(S.bar, phase, ctrl)) return;
 
@@ -820,6 +821,16 @@ __device__ __forceinline__ void tile32(const StageArgs& a, const Smem32& S, int6
     const double A = rk_a(st);
     const double cdt = a.group ? (active ? rk_c(st) * ctrl->dt[a.group[e]] : 0.0) : rk_c(st) * ctrl->dt[0];
     if (active) {
+        // the thread's 20 register values are loaded before any is stored: interleaved with the
+        // stores (which the compiler cannot prove to be other addresses) each load would wait for
+        // the previous store, 20 L2 round trips in a row.  L2 only (prefetched there at the tile
+        // start): L1 stays for the neighbour traces.
+        double rg[4][V];
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+#pragma unroll
+            for (int v = 0; v < V; ++v)
+                rg[q][v] = (RHS_ONLY || st == 0) ? 0.0 : __ldcg(a.reg + ((int64_t)v * E + e) * NP + ab + 16 * q);
         bool ok = true;
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
@@ -833,8 +844,7 @@ __device__ __forceinline__ void tile32(const StageArgs& a, const Smem32& S, int6
                 if (RHS_ONLY) {
                     a.rhs_out[g] = rhs;
                 } else {
-                    // L2 only (prefetched there at the tile start): L1 stays for the neighbour traces
-                    const double r2 = st == 0 ? rhs : A * __ldcg(a.reg + g) + rhs;
+                    const double r2 = st == 0 ? rhs : A * rg[q][v] + rhs;
                     a.reg[g] = r2;
                     su[s] = su[s] + cdt * r2;
                 }

@@ -65,9 +65,10 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned phase) {
     return false;
 }
 
-// Stage the tile's state (V arrays of nel*64 doubles, contiguous per variable) into smem.
-__device__ __forceinline__ bool tile_load(double* su, const double* __restrict__ u, int64_t E, int64_t e0, int nel,
-                                          uint64_t* bar, Control* ctrl) {
+// Stage the tile's state (V arrays of nel*64 doubles, contiguous per variable) into smem: the issue
+// (barrier set-up, then thread 0 starts the bulk copies) and, after other work, the wait.
+__device__ __forceinline__ void tile_issue(double* su, const double* __restrict__ u, int64_t E, int64_t e0, int nel,
+                                          uint64_t* bar) {
     if (threadIdx.x == 0) {
         unsigned b = smem_u32(bar);
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(b) : "memory");
@@ -88,6 +89,9 @@ __device__ __forceinline__ bool tile_load(double* su, const double* __restrict__
                 : "memory");
         }
     }
+}
+
+__device__ __forceinline__ bool tile_wait(uint64_t* bar, Control* ctrl) {
     bool ok = mbar_wait(bar, 0);
     if (!ok) {
         atomicOr(&ctrl->error, 1);
@@ -310,6 +314,8 @@ __global__ void __launch_bounds__(NT, NEMO_FP64_MINB) k_stage_euler64(StageArgs 
     const int64_t e0 = a.E_begin + (int64_t)blockIdx.x * EPC;
     const int nel = (int)min((int64_t)EPC, a.E_own - e0);
 
+    // the tile's bulk copy first, so that it is in flight while the blending coefficients are read
+    tile_issue(su, a.u_in, E, e0, nel, &bar);
     if (tid < EPC) {
         s_bad[tid] = 0;
         s_lam[tid][0] = s_lam[tid][1] = s_lam[tid][2] = 0ull;
@@ -328,7 +334,8 @@ __global__ void __launch_bounds__(NT, NEMO_FP64_MINB) k_stage_euler64(StageArgs 
         }
         s_alpha[tid] = al;
     }
-    if (!tile_load(su, a.u_in, E, e0, nel, &bar, ctrl)) return;
+    __syncthreads();   // s_alpha, s_bad, s_lam visible
+    if (!tile_wait(&bar, ctrl)) return;
     if (a.prep_only) {
         epilogue64(a, su, smem + V * EPC * NP, s_lam, nel, e0, tid, k);
         return;
@@ -526,6 +533,11 @@ __global__ void __launch_bounds__(NT, NEMO_FP64_MINB) k_stage_euler64(StageArgs 
         const int64_t pe = e0 + pel;
         const double cdt = a.group ? rk_c(st) * ctrl->dt[a.group[pe]] : Cdt;
         bool ok = true;
+        // the node's register values are loaded before any is stored (interleaved, each load would
+        // wait for the previous store: the compiler cannot prove the addresses differ)
+        double rg[V];
+#pragma unroll
+        for (int v = 0; v < V; ++v) rg[v] = (RHS_ONLY || st == 0) ? 0.0 : a.reg[((int64_t)v * E + pe) * NP + n];
 #pragma unroll
         for (int v = 0; v < V; ++v) {
             const int s = (v * EPC + pel) * NP + n;
@@ -535,7 +547,7 @@ __global__ void __launch_bounds__(NT, NEMO_FP64_MINB) k_stage_euler64(StageArgs 
             if (RHS_ONLY) {
                 a.rhs_out[g] = rhs;
             } else {
-                const double rr = st == 0 ? rhs : A * a.reg[g] + rhs;
+                const double rr = st == 0 ? rhs : A * rg[v] + rhs;
                 a.reg[g] = rr;
                 su[s] = su[s] + cdt * rr;
             }

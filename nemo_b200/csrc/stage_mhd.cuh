@@ -53,8 +53,10 @@ __device__ __forceinline__ bool mbar_wait_m(uint64_t* bar, unsigned phase) {
     return false;
 }
 
-__device__ __forceinline__ bool tile_load_m(double* su, const double* __restrict__ u, int64_t E, int64_t e0, int nel,
-                                            uint64_t* bar, Control* ctrl) {
+// The tile's bulk copy: issue (barrier set-up, thread 0 starts the copies), then, after other work,
+// the wait.
+__device__ __forceinline__ void tile_issue_m(double* su, const double* __restrict__ u, int64_t E, int64_t e0, int nel,
+                                             uint64_t* bar) {
     if (threadIdx.x == 0) {
         const unsigned b = su32(bar);
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(b) : "memory");
@@ -73,6 +75,9 @@ __device__ __forceinline__ bool tile_load_m(double* su, const double* __restrict
                 "l"(u + ((int64_t)v * E + e0) * NP), "r"(bytes), "r"(b)
                 : "memory");
     }
+}
+
+__device__ __forceinline__ bool tile_wait_m(uint64_t* bar, Control* ctrl) {
     bool ok = mbar_wait_m(bar, 0);
     if (!ok) {
         atomicOr(&ctrl->error, 1);
@@ -444,6 +449,8 @@ __global__ void __launch_bounds__(mhd::NT, sizeof(R) == 4 ? 3 : NEMO_MHD64_MINB)
     const R kap = (R)k.kappa, mu0 = (R)k.mu0;
     const R ch = (R)ctrl->glm_ch;
 
+    // the tile's bulk copy first, so that it is in flight while the blending coefficients are read
+    mhd::tile_issue_m(su, a.u_in, E, e0, nel, &bar);
     if (tid < MEPC) {
         s_bad[tid] = 0;
         s_lam[tid][0] = s_lam[tid][1] = s_lam[tid][2] = 0ull;
@@ -462,7 +469,8 @@ __global__ void __launch_bounds__(mhd::NT, sizeof(R) == 4 ? 3 : NEMO_MHD64_MINB)
         s_alpha[tid] = al;
     }
     if (tid == 0) s_vmax = 0ull;
-    if (!mhd::tile_load_m(su, a.u_in, E, e0, nel, &bar, ctrl)) return;
+    __syncthreads();   // s_alpha, s_bad, s_lam, s_vmax visible
+    if (!mhd::tile_wait_m(&bar, ctrl)) return;
     if (a.prep_only) {
         mhd::epilogue_mhd<R>(a, su, sR, s_lam, &s_vmax, nel, e0, tid, k);
         return;
@@ -599,6 +607,15 @@ __global__ void __launch_bounds__(mhd::NT, sizeof(R) == 4 ? 3 : NEMO_MHD64_MINB)
         for (int i = 0; i < NN; ++i) {
             const int n = nidx(i, la, lb);
             double uu[MV];
+            // the node's register values are loaded before any is stored (interleaved, each load
+            // would wait for the previous store); the FP32 form reads them from L2 only (0.7 %
+            // faster; the FP64 form is not)
+            double rgv[MV];
+#pragma unroll
+            for (int v = 0; v < MV; ++v) {
+                const int64_t g = ((int64_t)v * E + e) * NP + n;
+                rgv[v] = (RHS_ONLY || st == 0) ? 0.0 : (sizeof(R) == 4 ? __ldcg(a.reg + g) : a.reg[g]);
+            }
 #pragma unroll
             for (int v = 0; v < MV; ++v) {
                 const int s = (v * MEPC + el) * NP + n;
@@ -608,8 +625,7 @@ __global__ void __launch_bounds__(mhd::NT, sizeof(R) == 4 ? 3 : NEMO_MHD64_MINB)
                 if (RHS_ONLY) {
                     a.rhs_out[g] = rhs;
                 } else {
-                    // FP32 form: the register row from L2 only (0.7 % faster; the FP64 form is not)
-                    const double rg = st == 0 ? 0.0 : (sizeof(R) == 4 ? __ldcg(a.reg + g) : a.reg[g]);
+                    const double rg = rgv[v];
                     const double r2 = st == 0 ? rhs : A * rg + rhs;
                     a.reg[g] = r2;
                     su[s] = su[s] + cdt * r2;
