@@ -491,8 +491,9 @@ def main():  # noqa: C901
     ap.add_argument("--secondary", default="batch,ot64",
                     help="further workloads timed in the same run (chosen and plain form, device throughput "
                          "only; comma-separated, empty for none)")
-    ap.add_argument("--schedule", default="auto", choices=["auto", "grid", "persistent"],
-                    help="FP32 stage schedule: autotuned (default) or fixed (profiling runs)")
+    ap.add_argument("--schedule", default="auto", choices=["auto", "grid", "grid4", "grid16", "persistent"],
+                    help="FP32 stage schedule: autotuned (default) or fixed (profiling runs): grid with 8, 4 or 16 "
+                         "elements per CTA, or persistent")
     args = ap.parse_args()
     assert args.warmup >= 3 or args.impl == "reference" or os.environ.get("NEMO_BENCH_ALLOW_SHORT")
 
@@ -546,7 +547,9 @@ def main():  # noqa: C901
             if args.schedule == "auto":
                 mode, ctas, tms = s.autotune(nsteps=3)   # restores the state it times
             else:
-                mode, ctas, tms = (0, 0, [-1.0] * 8) if args.schedule == "grid" else (1, 4 * peaks["sms"], [-1.0] * 8)
+                fixed = {"grid": (0, 0), "grid4": (2, 0), "grid16": (3, 0), "persistent": (1, 4 * peaks["sms"])}
+                mode, ctas = fixed[args.schedule]
+                tms = [-1.0] * 8
                 s.set_schedule(mode, ctas)
             sched = {"chosen": SCHEDULES[mode], "persistent_ctas": ctas,
                      "autotune_ms_per_step": {"grid_8_elements_per_cta": tms[0], "grid_4_elements_per_cta": tms[5],
