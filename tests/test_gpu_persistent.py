@@ -62,7 +62,7 @@ def test_persistent_forest_with_fused_mortars(ctas):
 def test_autotune_keeps_state_and_picks_a_schedule():
     m = mesh.brick(8)
     u = setups.smooth_random(m, seed=8)
-    s = Solver(abi.default_cfg(precision=abi.PREC_FP32, indicator=abi.IND_MODAL), m)
+    s = Solver(abi.default_cfg(precision=abi.PREC_FP32, indicator=abi.IND_MODAL, positivity=1), m)
     s.upload(u)
     mode, ctas, ms = s.autotune(nsteps=2)
     assert mode in (0, 1, 2, 3) and (mode != 1 or ctas >= 148)
@@ -72,7 +72,9 @@ def test_autotune_keeps_state_and_picks_a_schedule():
     t, n = s.run(nsteps=3)
     got = s.download()
     s.finalize()
-    ref, tr = run_with(m, u, (0, 0), nsteps=3)
+    # the same schedule set by hand from a fresh upload (FP32 results depend on the tile size, which
+    # decides which neighbour traces come from the tile and which from global memory)
+    ref, tr = run_with(m, u, (mode, ctas), nsteps=3)
     assert t == tr and np.array_equal(got, ref)
 
 
