@@ -6,6 +6,7 @@ host code with -ffp-contract=off; the FP32-bulk kernels keep FMA contraction.
 import os
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
@@ -45,7 +46,7 @@ def build(verbose=False, force=False, ptxas_info=False):
     os.makedirs(BUILD, exist_ok=True)
     headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))]
     headers.append(os.path.join(HERE, "..", "include", "nemo_gpu.h"))
-    objs = []
+    objs, jobs = [], []
     for src, extra in SOURCES.items():
         s = os.path.join(CSRC, src)
         o = os.path.join(BUILD, src.replace(".cu", ".o"))
@@ -54,7 +55,15 @@ def build(verbose=False, force=False, ptxas_info=False):
             cmd = [nvcc()] + ARCH + COMMON + extra + (["-Xptxas", "-v"] if ptxas_info else []) + ["-c", s, "-o", o]
             if verbose:
                 print(" ".join(cmd), file=sys.stderr)
-            r = subprocess.run(cmd, capture_output=True, text=True)
+            jobs.append((src, cmd))
+
+    # the translation units are independent: compile them concurrently (the stage kernels dominate)
+    def run(job):
+        src, cmd = job
+        return src, subprocess.run(cmd, capture_output=True, text=True)
+
+    with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as pool:
+        for src, r in pool.map(run, jobs):
             if r.returncode != 0:
                 raise RuntimeError(f"nvcc failed for {src}:\n{r.stderr}")
             if ptxas_info or verbose:

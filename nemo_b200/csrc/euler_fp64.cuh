@@ -51,11 +51,13 @@ __device__ __forceinline__ void hllc64(const double* UL, const double* UR, doubl
     double at = sqrt(k.km1 * (Ht - 0.5 * (vt * vt)));
     double SL = fmin(fmin(vt - at, VL - beta * cL), 0.0);
     double SR = fmax(fmax(vt + at, VR + beta * cR), 0.0);
-    if (SL >= 0.0) { xflux64(UL, pL, F); return; }
-    if (SR <= 0.0) { xflux64(UR, pR, F); return; }
+    // the supersonic cases (SL >= 0: the left flux, SR <= 0: the right flux) are selected at the
+    // end instead of returned early: the same values, and no branch between the Riemann fluxes
+    // of a line, which the compiler can then interleave (discarded values may be inf or NaN)
     double FL[5], FR[5];
     xflux64(UL, pL, FL);
     xflux64(UR, pR, FR);
+    const bool supL = SL >= 0.0, supR = SR <= 0.0;
     double smooth = sqrt(fabs(pL - pR) / (pL + pR));
     double SS = (pR - pL + UL[1] * (SL - VL) - UR[1] * (SR - VR)) / (UL[0] * (SL - VL) - UR[0] * (SR - VR));
     const bool left = (SL <= 0.0 && 0.0 <= SS);
@@ -76,7 +78,8 @@ __device__ __forceinline__ void hllc64(const double* UL, const double* UR, doubl
 #pragma unroll
     for (int v = 0; v < 5; ++v) {
         double FH = (SR * FL[v] - SL * FR[v] + SLSR * (UR[v] - UL[v])) / dS;
-        F[v] = smooth * FH + oms * (FU[v] + S * (Us[v] - U[v]));
+        const double Fm = smooth * FH + oms * (FU[v] + S * (Us[v] - U[v]));
+        F[v] = supL ? FL[v] : (supR ? FR[v] : Fm);
     }
 }
 
@@ -97,6 +100,14 @@ __device__ __forceinline__ void riemann64(int kind, const double* uL, const doub
                                           const OpConsts& k) {
     if (kind == 1) rusanov64(uL, uR, F, k);
     else hllc64(uL, uR, F, k);
+}
+
+// FAST: the flux kinds fixed at compile time (HLLC faces and subcells, Chandrashekar pairs); a
+// run-time switch inside the unrolled line loops is a branch around every flux
+template <bool FAST>
+__device__ __forceinline__ void riem64(int kind, const double* uL, const double* uR, double* F, const OpConsts& k) {
+    if (FAST) hllc64(uL, uR, F, k);
+    else riemann64(kind, uL, uR, F, k);
 }
 
 // logmean with the absolute switch, source/equations/euler/two_point/chandrashekar/

@@ -234,6 +234,13 @@ __device__ __forceinline__ void m_riemann_x(int kind, const R* uL, const R* uR, 
     else m_rusanov_x(uL, uR, F, kappa, mu0, ch);
 }
 
+// FAST: HLLD fixed at compile time (no run-time switch around every flux of the unrolled loops)
+template <bool FAST, typename R>
+__device__ __forceinline__ void m_riem(int kind, const R* uL, const R* uR, R* F, R kappa, R mu0, R ch) {
+    if (FAST) m_hlld_x(uL, uR, F, kappa, ch);
+    else m_riemann_x(kind, uL, uR, F, kappa, mu0, ch);
+}
+
 // LN_MEAN, source/equations/mhd/two_point/ec/two_point_flux_mod.f90:203-219 (relative switch)
 template <typename R>
 __device__ __forceinline__ R ln_mean_rel(R aL, R aR) {

@@ -1082,22 +1082,30 @@ int stage_smem_bytes_mhd32() { return mhd::V * mhd::EPC * (NP * (int)sizeof(doub
 cudaError_t setup_stage_mhd32() {
     const int smem = stage_smem_bytes_mhd32();
     cudaError_t err;
-    if ((err = cudaFuncSetAttribute(k_stage_mhd<float, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem))) return err;
-    if ((err = cudaFuncSetAttribute(k_stage_mhd<float, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem))) return err;
-    if ((err = cudaFuncSetAttribute(k_stage_mhd<float, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem))) return err;
-    return cudaFuncSetAttribute(k_stage_mhd<float, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    const auto dyn = cudaFuncAttributeMaxDynamicSharedMemorySize;
+    if ((err = cudaFuncSetAttribute(k_stage_mhd<float, true, true, false>, dyn, smem))) return err;
+    if ((err = cudaFuncSetAttribute(k_stage_mhd<float, false, true, false>, dyn, smem))) return err;
+    if ((err = cudaFuncSetAttribute(k_stage_mhd<float, true, false, false>, dyn, smem))) return err;
+    if ((err = cudaFuncSetAttribute(k_stage_mhd<float, false, false, false>, dyn, smem))) return err;
+    if ((err = cudaFuncSetAttribute(k_stage_mhd<float, true, false, true>, dyn, smem))) return err;
+    return cudaFuncSetAttribute(k_stage_mhd<float, false, false, true>, dyn, smem);
 }
 
 cudaError_t launch_stage_mhd32(const StageArgs& a, bool blend, bool rhs_only, cudaStream_t s) {
     const int grid = (int)((a.E_own - a.E_begin + mhd::EPC - 1) / mhd::EPC);
     if (grid <= 0) return cudaSuccess;
     const int smem = stage_smem_bytes_mhd32();
+    // the specialised kernel for HLLD faces and the EC pair flux, the general one for the rest
+    const bool fast = a.surface_flux == NEMO_SURFFLUX_HLLD && a.volume_flux == NEMO_VOLFLUX_EC_MHD;
     if (rhs_only) {
-        if (blend) k_stage_mhd<float, true, true><<<grid, mhd::NT, smem, s>>>(a);
-        else k_stage_mhd<float, false, true><<<grid, mhd::NT, smem, s>>>(a);
+        if (blend) k_stage_mhd<float, true, true, false><<<grid, mhd::NT, smem, s>>>(a);
+        else k_stage_mhd<float, false, true, false><<<grid, mhd::NT, smem, s>>>(a);
+    } else if (fast) {
+        if (blend) k_stage_mhd<float, true, false, true><<<grid, mhd::NT, smem, s>>>(a);
+        else k_stage_mhd<float, false, false, true><<<grid, mhd::NT, smem, s>>>(a);
     } else {
-        if (blend) k_stage_mhd<float, true, false><<<grid, mhd::NT, smem, s>>>(a);
-        else k_stage_mhd<float, false, false><<<grid, mhd::NT, smem, s>>>(a);
+        if (blend) k_stage_mhd<float, true, false, false><<<grid, mhd::NT, smem, s>>>(a);
+        else k_stage_mhd<float, false, false, false><<<grid, mhd::NT, smem, s>>>(a);
     }
     return cudaGetLastError();
 }

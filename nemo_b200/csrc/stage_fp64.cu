@@ -294,7 +294,7 @@ __device__ void epilogue64(const StageArgs& a, const double* su, double* sp, uns
 
 }  // namespace
 
-template <bool BLEND, bool IND, bool RHS_ONLY>
+template <bool BLEND, bool IND, bool RHS_ONLY, bool FAST>
 __global__ void __launch_bounds__(NT, NEMO_FP64_MINB) k_stage_euler64(StageArgs a) {
     extern __shared__ __align__(128) double smem[];
     double* su = smem;                    // [V][EPC][64] state, later the new state
@@ -386,7 +386,7 @@ __global__ void __launch_bounds__(NT, NEMO_FP64_MINB) k_stage_euler64(StageArgs 
         for (int pq = 0; pq < 6; ++pq) {
             const int i = PI_[pq], m = PM_[pq];
             double F[V];
-            if (a.volume_flux == NEMO_VOLFLUX_CENTRAL) {
+            if (!FAST && a.volume_flux == NEMO_VOLFLUX_CENTRAL) {
                 double ui[V], um[V];
                 ui[0] = su[(0 * EPC + el) * NP + idx[i]];
                 ui[1] = su[((1 + c0) * EPC + el) * NP + idx[i]];
@@ -462,8 +462,8 @@ __global__ void __launch_bounds__(NT, NEMO_FP64_MINB) k_stage_euler64(StageArgs 
 #pragma unroll
                 for (int v = 0; v < V; ++v) un[v] = uo[v];
             }
-            if (side) riemann64(a.surface_flux, uo, un, Fs[1], k);
-            else riemann64(a.surface_flux, un, uo, Fs[0], k);
+            if (side) riem64<FAST>(a.surface_flux, uo, un, Fs[1], k);
+            else riem64<FAST>(a.surface_flux, un, uo, Fs[0], k);
         }
 
         // ---- surface lift at the line ends
@@ -493,7 +493,7 @@ __global__ void __launch_bounds__(NT, NEMO_FP64_MINB) k_stage_euler64(StageArgs 
                         uR[2] = su[((1 + c1) * EPC + el) * NP + idx[i + 1]];
                         uR[3] = su[((1 + c2) * EPC + el) * NP + idx[i + 1]];
                         uR[4] = su[(4 * EPC + el) * NP + idx[i + 1]];
-                        riemann64(a.surface_flux, uL, uR, Fr, k);
+                        riem64<FAST>(a.surface_flux, uL, uR, Fr, k);
                     } else {
 #pragma unroll
                         for (int v = 0; v < V; ++v) Fr[v] = Fs[1][v];
@@ -627,12 +627,17 @@ cudaError_t launch_stage_euler64(const StageArgs& a, bool blend, bool ind, bool 
     if (grid <= 0) return cudaSuccess;
     const int smem = stage_smem_bytes64();
     (void)ind;
+    // the specialised kernel for HLLC faces and Chandrashekar pairs, the general one for the rest
+    const bool fast = a.surface_flux == NEMO_SURFFLUX_HLLC && a.volume_flux == NEMO_VOLFLUX_CHANDRASHEKAR;
     if (rhs_only) {
-        if (blend) k_stage_euler64<true, true, true><<<grid, NT, smem, s>>>(a);
-        else k_stage_euler64<false, false, true><<<grid, NT, smem, s>>>(a);
+        if (blend) k_stage_euler64<true, true, true, false><<<grid, NT, smem, s>>>(a);
+        else k_stage_euler64<false, false, true, false><<<grid, NT, smem, s>>>(a);
+    } else if (fast) {
+        if (blend) k_stage_euler64<true, true, false, true><<<grid, NT, smem, s>>>(a);
+        else k_stage_euler64<false, false, false, true><<<grid, NT, smem, s>>>(a);
     } else {
-        if (blend) k_stage_euler64<true, true, false><<<grid, NT, smem, s>>>(a);
-        else k_stage_euler64<false, false, false><<<grid, NT, smem, s>>>(a);
+        if (blend) k_stage_euler64<true, true, false, false><<<grid, NT, smem, s>>>(a);
+        else k_stage_euler64<false, false, false, false><<<grid, NT, smem, s>>>(a);
     }
     return cudaGetLastError();
 }
@@ -640,14 +645,13 @@ cudaError_t launch_stage_euler64(const StageArgs& a, bool blend, bool ind, bool 
 cudaError_t setup_stage_euler64(const OpConsts& ops) {
     const int smem = stage_smem_bytes64();
     cudaError_t err;
-    err = cudaFuncSetAttribute(k_stage_euler64<true, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    if (err != cudaSuccess) return err;
-    err = cudaFuncSetAttribute(k_stage_euler64<false, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    if (err != cudaSuccess) return err;
-    err = cudaFuncSetAttribute(k_stage_euler64<true, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    if (err != cudaSuccess) return err;
-    err = cudaFuncSetAttribute(k_stage_euler64<false, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    if (err != cudaSuccess) return err;
+    const auto dyn = cudaFuncAttributeMaxDynamicSharedMemorySize;
+    if ((err = cudaFuncSetAttribute(k_stage_euler64<true, true, true, false>, dyn, smem)) != cudaSuccess) return err;
+    if ((err = cudaFuncSetAttribute(k_stage_euler64<false, false, true, false>, dyn, smem)) != cudaSuccess) return err;
+    if ((err = cudaFuncSetAttribute(k_stage_euler64<true, true, false, false>, dyn, smem)) != cudaSuccess) return err;
+    if ((err = cudaFuncSetAttribute(k_stage_euler64<false, false, false, false>, dyn, smem)) != cudaSuccess) return err;
+    if ((err = cudaFuncSetAttribute(k_stage_euler64<true, true, false, true>, dyn, smem)) != cudaSuccess) return err;
+    if ((err = cudaFuncSetAttribute(k_stage_euler64<false, false, false, true>, dyn, smem)) != cudaSuccess) return err;
     return cudaMemcpyToSymbol(c_ops64, &ops, sizeof(OpConsts));
 }
 
@@ -680,10 +684,13 @@ int stage_smem_bytes_mhd64() { return mhd::V * mhd::EPC * (NP * (int)sizeof(doub
 cudaError_t setup_stage_mhd64() {
     const int smem = stage_smem_bytes_mhd64();
     cudaError_t err;
-    if ((err = cudaFuncSetAttribute(k_stage_mhd<double, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem))) return err;
-    if ((err = cudaFuncSetAttribute(k_stage_mhd<double, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem))) return err;
-    if ((err = cudaFuncSetAttribute(k_stage_mhd<double, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem))) return err;
-    return cudaFuncSetAttribute(k_stage_mhd<double, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    const auto dyn = cudaFuncAttributeMaxDynamicSharedMemorySize;
+    if ((err = cudaFuncSetAttribute(k_stage_mhd<double, true, true, false>, dyn, smem))) return err;
+    if ((err = cudaFuncSetAttribute(k_stage_mhd<double, false, true, false>, dyn, smem))) return err;
+    if ((err = cudaFuncSetAttribute(k_stage_mhd<double, true, false, false>, dyn, smem))) return err;
+    if ((err = cudaFuncSetAttribute(k_stage_mhd<double, false, false, false>, dyn, smem))) return err;
+    if ((err = cudaFuncSetAttribute(k_stage_mhd<double, true, false, true>, dyn, smem))) return err;
+    return cudaFuncSetAttribute(k_stage_mhd<double, false, false, true>, dyn, smem);
 }
 
 // Positivity repair of element states held outside the library (the per-quad kernel_repair of a
@@ -727,12 +734,17 @@ cudaError_t launch_stage_mhd64(const StageArgs& a, bool blend, bool rhs_only, cu
     const int grid = (int)((a.E_own - a.E_begin + mhd::EPC - 1) / mhd::EPC);
     if (grid <= 0) return cudaSuccess;
     const int smem = stage_smem_bytes_mhd64();
+    // the specialised kernel for HLLD faces and the EC pair flux, the general one for the rest
+    const bool fast = a.surface_flux == NEMO_SURFFLUX_HLLD && a.volume_flux == NEMO_VOLFLUX_EC_MHD;
     if (rhs_only) {
-        if (blend) k_stage_mhd<double, true, true><<<grid, mhd::NT, smem, s>>>(a);
-        else k_stage_mhd<double, false, true><<<grid, mhd::NT, smem, s>>>(a);
+        if (blend) k_stage_mhd<double, true, true, false><<<grid, mhd::NT, smem, s>>>(a);
+        else k_stage_mhd<double, false, true, false><<<grid, mhd::NT, smem, s>>>(a);
+    } else if (fast) {
+        if (blend) k_stage_mhd<double, true, false, true><<<grid, mhd::NT, smem, s>>>(a);
+        else k_stage_mhd<double, false, false, true><<<grid, mhd::NT, smem, s>>>(a);
     } else {
-        if (blend) k_stage_mhd<double, true, false><<<grid, mhd::NT, smem, s>>>(a);
-        else k_stage_mhd<double, false, false><<<grid, mhd::NT, smem, s>>>(a);
+        if (blend) k_stage_mhd<double, true, false, false><<<grid, mhd::NT, smem, s>>>(a);
+        else k_stage_mhd<double, false, false, false><<<grid, mhd::NT, smem, s>>>(a);
     }
     return cudaGetLastError();
 }

@@ -424,7 +424,7 @@ __device__ void epilogue_mhd(const StageArgs& a, const double* su, R* scr, unsig
 // from the FP64 tile: a shared-memory array of per-node FP32 primitives (20 KB more per CTA) made the
 // pair fluxes cheaper but the stage 4 % slower, as the larger carveout left L1 too small for the
 // neighbour traces and register rows.
-template <typename R, bool BLEND, bool RHS_ONLY>
+template <typename R, bool BLEND, bool RHS_ONLY, bool FAST>
 __global__ void __launch_bounds__(mhd::NT, sizeof(R) == 4 ? 3 : NEMO_MHD64_MINB) k_stage_mhd(StageArgs a) {
     constexpr int MEPC = mhd::EPC, MV = mhd::V;
     using mhd::load_rot;
@@ -508,10 +508,10 @@ __global__ void __launch_bounds__(mhd::NT, sizeof(R) == 4 ? 3 : NEMO_MHD64_MINB)
                     for (int v = 0; v < MV; ++v) un[v] = uo[v];
                 }
                 if (side) {
-                    m_riemann_x(a.surface_flux, uo, un, F, kap, mu0, ch);
+                    m_riem<FAST>(a.surface_flux, uo, un, F, kap, mu0, ch);
                     m_nc_x(uo, uo, un, G, mu0);
                 } else {
-                    m_riemann_x(a.surface_flux, un, uo, F, kap, mu0, ch);
+                    m_riem<FAST>(a.surface_flux, un, uo, F, kap, mu0, ch);
                     m_nc_x(uo, un, uo, G, mu0);
                 }
 #pragma unroll
@@ -530,7 +530,7 @@ __global__ void __launch_bounds__(mhd::NT, sizeof(R) == 4 ? 3 : NEMO_MHD64_MINB)
                     R ui[MV], um[MV], F[MV], Gi[MV], Gm[MV];
                     load_rot(su, el, idx[i], d, ui);
                     load_rot(su, el, idx[m], d, um);
-                    if (a.volume_flux == NEMO_VOLFLUX_CENTRAL) m_central_x(ui, um, F, kap, mu0, ch);
+                    if (!FAST && a.volume_flux == NEMO_VOLFLUX_CENTRAL) m_central_x(ui, um, F, kap, mu0, ch);
                     else m_ec_x(ui, um, F, kap, mu0, ch);
                     m_nc_x(ui, ui, um, Gi, mu0);
                     m_nc_x(um, ui, um, Gm, mu0);
@@ -569,7 +569,7 @@ __global__ void __launch_bounds__(mhd::NT, sizeof(R) == 4 ? 3 : NEMO_MHD64_MINB)
                         if (i < NN - 1) {
                             R ur[MV];
                             load_rot(su, el, idx[i + 1], d, ur);
-                            m_riemann_x(a.surface_flux, ui, ur, Fh, kap, mu0, ch);
+                            m_riem<FAST>(a.surface_flux, ui, ur, Fh, kap, mu0, ch);
                             m_nc_x(ui, ui, ur, G, mu0);
 #pragma unroll
                             for (int v = 0; v < MV; ++v) FR[v] = Fh[v] + G[v];
