@@ -491,11 +491,18 @@ def main():  # noqa: C901
     ap.add_argument("--secondary", default="batch,ot64",
                     help="further workloads timed in the same run (chosen and plain form, device throughput "
                          "only; comma-separated, empty for none)")
+    ap.add_argument("--nx", type=int, default=0,
+                    help="elements per direction of the workload's base mesh instead of its own size (a smaller "
+                         "sample for profiling runs; the config then says so)")
     ap.add_argument("--schedule", default="auto", choices=["auto", "grid", "grid4", "grid16", "persistent"],
                     help="FP32 stage schedule: autotuned (default) or fixed (profiling runs): grid with 8, 4 or 16 "
                          "elements per CTA, or persistent")
     args = ap.parse_args()
     assert args.warmup >= 3 or args.impl == "reference" or os.environ.get("NEMO_BENCH_ALLOW_SHORT")
+    if args.nx:
+        w = WORKLOADS[args.workload]
+        w["desc"] = f"{w['desc']} [sample: {args.nx} base elements per direction, set by --nx]"
+        w["nx"] = args.nx
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -588,7 +595,7 @@ def main():  # noqa: C901
     tpath = os.path.join(ROOT, "profiles", "stage_traffic.json")
     if os.path.exists(tpath):
         with open(tpath) as f:
-            traffic = json.load(f).get(args.workload)
+            traffic = None if args.nx else json.load(f).get(args.workload)
 
     e2e_val, e2e_steps, nbytes, e2e_serial = None, 0, u.nbytes, None
     if not args.no_e2e:

@@ -108,10 +108,11 @@ __device__ __forceinline__ void tile_store_wait32() {
     asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
 }
 
-// 1/x in FP64 from the FP32 reciprocal by two Newton steps (relative error ~1e-16 for the positive,
-// normal densities it is used on; the FP32 form needs no correctly rounded division here).
+// 1/x in FP64 from the approximate FP32 reciprocal (about 1 ulp of FP32) by two Newton steps
+// (relative error ~1e-16 for the positive, normal densities it is used on; the FP32 form needs no
+// correctly rounded division here).  The correctly rounded FP32 seed was 0.5-1 % slower per stage.
 __device__ __forceinline__ double rcp64(double x) {
-    double y = (double)__frcp_rn((float)x);
+    double y = (double)(1.0f / (float)x);   // the approximate FP32 reciprocal (fast-math) as the seed
     y = y * fma(-x, y, 2.0);
     return y * fma(-x, y, 2.0);
 }
@@ -631,7 +632,8 @@ __device__ __forceinline__ void tile32(const StageArgs& a, const Smem32& S, int6
         }
         s_alpha[tid] = al;
     }
-    __syncthreads();   // s_alpha / s_bad visible
+    // s_alpha and s_bad become visible at the barrier after the primitives: the coefficient loads
+    // overlap the bulk copy and the primitives instead of holding the whole CTA (1.5 % per stage)
     if (!tile_wait32(S.bar, phase, ctrl)) return;
 
     const int el = tid >> 4, ab = tid & 15, la = ab & 3, lb = ab >> 2;
@@ -664,7 +666,7 @@ __device__ __forceinline__ void tile32(const StageArgs& a, const Smem32& S, int6
             SQ(5, el, n) = 0.5f * rf / pf;
         }
     }
-    __syncthreads();
+    __syncthreads();   // the primitives of the tile, s_alpha and s_bad visible
 
     const float ikm1 = k.ikm1_32;
     const float c_enth = k.c_enth32;
