@@ -182,21 +182,28 @@ __device__ __forceinline__ void m_hlld_x(const R* uL, const R* uR, R* F, R kappa
         }
         const R sqL = sqrt(rs[0]), sqR = sqrt(rs[1]);
         const R SLs = SM - fabs(bn) / sqL, SRs = SM + fabs(bn) / sqR;
-        const int s = SM >= R(0.0) ? 0 : 1;
-        const R S = s ? SR : SL;
+        // side s of the contact (0: left, 1: right) picked by selects, not by indexing with a run-time
+        // index, which would put the two-sided arrays in local memory
+        const bool sr = !(SM >= R(0.0));
+        const R S = sr ? SR : SL;
+        const R rsS = sr ? rs[1] : rs[0], ws1S = sr ? ws1[1] : ws1[0], ws2S = sr ? ws2[1] : ws2[0];
+        const R cs1S = sr ? cs1[1] : cs1[0], cs2S = sr ? cs2[1] : cs2[0], esS = sr ? es[1] : es[0];
         R Us[8];
-        Us[0] = rs[s];
-        Us[1] = rs[s] * SM;
-        Us[2] = rs[s] * ws1[s];
-        Us[3] = rs[s] * ws2[s];
-        Us[4] = es[s];
+        Us[0] = rsS;
+        Us[1] = rsS * SM;
+        Us[2] = rsS * ws1S;
+        Us[3] = rsS * ws2S;
+        Us[4] = esS;
         Us[5] = bn;
-        Us[6] = cs1[s];
-        Us[7] = cs2[s];
-        const bool outer = s ? (SRs < R(0.0)) : (SLs >= R(0.0));
+        Us[6] = cs1S;
+        Us[7] = cs2S;
+        const bool outer = sr ? (SRs < R(0.0)) : (SLs >= R(0.0));
         if (outer) {
 #pragma unroll
-            for (int v = 0; v < 8; ++v) F[v] = Fk[s][v] + S * (Us[v] - Uk[s][v]);
+            for (int v = 0; v < 8; ++v) {
+                const R FkS = sr ? Fk[1][v] : Fk[0][v], UkS = sr ? Uk[1][v] : Uk[0][v];
+                F[v] = FkS + S * (Us[v] - UkS);
+            }
         } else {
             // double-star state of side s (Alfven waves); it equals the single-star state if B_n = 0
             R Uss[8];
@@ -209,18 +216,21 @@ __device__ __forceinline__ void m_hlld_x(const R* uL, const R* uR, R* F, R kappa
                 const R w2 = (sqL * ws2[0] + sqR * ws2[1] + sg * (cs2[1] - cs2[0])) * sden;
                 const R c1 = (sqL * cs1[1] + sqR * cs1[0] + sg * sqL * sqR * (ws1[1] - ws1[0])) * sden;
                 const R c2 = (sqL * cs2[1] + sqR * cs2[0] + sg * sqL * sqR * (ws2[1] - ws2[0])) * sden;
-                const R wcs = ws1[s] * cs1[s] + ws2[s] * cs2[s];
+                const R wcs = ws1S * cs1S + ws2S * cs2S;
                 const R wcss = w1 * c1 + w2 * c2;
-                const R sq = s ? sqR : sqL;
-                Uss[2] = rs[s] * w1;
-                Uss[3] = rs[s] * w2;
-                Uss[4] = s ? es[s] + sg * sq * (wcs - wcss) : es[s] - sg * sq * (wcs - wcss);
+                const R sq = sr ? sqR : sqL;
+                Uss[2] = rsS * w1;
+                Uss[3] = rsS * w2;
+                Uss[4] = sr ? esS + sg * sq * (wcs - wcss) : esS - sg * sq * (wcs - wcss);
                 Uss[6] = c1;
                 Uss[7] = c2;
             }
-            const R Ss = s ? SRs : SLs;
+            const R Ss = sr ? SRs : SLs;
 #pragma unroll
-            for (int v = 0; v < 8; ++v) F[v] = Fk[s][v] + Ss * Uss[v] - (Ss - S) * Us[v] - S * Uk[s][v];
+            for (int v = 0; v < 8; ++v) {
+                const R FkS = sr ? Fk[1][v] : Fk[0][v], UkS = sr ? Uk[1][v] : Uk[0][v];
+                F[v] = FkS + Ss * Uss[v] - (Ss - S) * Us[v] - S * UkS;
+            }
         }
     }
     F[4] = F[4] + ch * bn * psn;

@@ -334,9 +334,11 @@ __global__ void __launch_bounds__(NT, NEMO_FP64_MINB) k_stage_euler64(StageArgs 
         }
         s_alpha[tid] = al;
     }
-    __syncthreads();   // s_alpha, s_bad, s_lam visible
+    // s_alpha, s_bad and s_lam become visible at the barrier after the primitives: the coefficient
+    // loads overlap the bulk copy instead of holding the whole CTA
     if (!tile_wait(&bar, ctrl)) return;
     if (a.prep_only) {
+        __syncthreads();
         epilogue64(a, su, smem + V * EPC * NP, s_lam, nel, e0, tid, k);
         return;
     }

@@ -451,12 +451,15 @@ __global__ void __launch_bounds__(mhd::NT, sizeof(R) == 4 ? 3 : NEMO_MHD64_MINB)
 
     // the tile's bulk copy first, so that it is in flight while the blending coefficients are read
     mhd::tile_issue_m(su, a.u_in, E, e0, nel, &bar);
-    if (tid < MEPC) {
-        s_bad[tid] = 0;
-        s_lam[tid][0] = s_lam[tid][1] = s_lam[tid][2] = 0ull;
+    // the first thread of each element reads its blending coefficient; the element's 16 threads
+    // share a warp, so a warp sync makes it visible (no CTA barrier: the loads overlap the bulk copy)
+    if ((tid & 15) == 0) {
+        const int te = tid >> 4;
+        s_bad[te] = 0;
+        s_lam[te][0] = s_lam[te][1] = s_lam[te][2] = 0ull;
         R al = R(0.0);
-        if (BLEND && tid < nel) {
-            const int64_t e = e0 + tid;
+        if (BLEND && te < nel) {
+            const int64_t e = e0 + te;
             double ad = a.alpha_in[e];
             if (a.smooth)
                 for (int f = 0; f < 6; ++f) {
@@ -466,12 +469,13 @@ __global__ void __launch_bounds__(mhd::NT, sizeof(R) == 4 ? 3 : NEMO_MHD64_MINB)
             if (a.alpha_used) a.alpha_used[e] = ad;
             al = (R)ad;
         }
-        s_alpha[tid] = al;
+        s_alpha[te] = al;
     }
     if (tid == 0) s_vmax = 0ull;
-    __syncthreads();   // s_alpha, s_bad, s_lam, s_vmax visible
+    __syncwarp();   // s_alpha, s_bad of the warp's elements; s_lam and s_vmax are read after CTA barriers
     if (!mhd::tile_wait_m(&bar, ctrl)) return;
     if (a.prep_only) {
+        __syncthreads();
         mhd::epilogue_mhd<R>(a, su, sR, s_lam, &s_vmax, nel, e0, tid, k);
         return;
     }
