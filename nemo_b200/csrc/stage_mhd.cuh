@@ -2,9 +2,11 @@
 //
 // Included by stage_fp64.cu (R = double, -fmad=false: bit-identical to the oracle) and by
 // stage_fp32.cu (R = float, fast math; state, register, update, repair and reductions stay FP64).
-// One CTA = 8 elements, 16 threads per element; thread (a,b) owns the x-, y- and z-lines through
-// (a,b) and adds its direction terms into one shared rhs array (x, then y, then z), which keeps the
-// oracle's summation order.  Per line: surface flux (Rusanov) + the element's own-side
+// One CTA = EPC elements (8 for the FP32 form, 4 for the plain FP64 form), 16 threads per element;
+// thread (a,b) owns the x-, y- and z-lines through (a,b) and adds its direction terms into one
+// shared rhs array (x, then y, then z), which keeps the oracle's summation order.  Two kernels per
+// form: a general one (flux kinds chosen at run time) and one specialised to HLLD + EC.  Per line:
+// surface flux (HLLD or Rusanov) + the element's own-side
 // non-conservative Powell/GLM term at both ends, 6 node pairs of EC flux (Derigs) + non-conservative
 // term in flux-differencing form, the lift, and (alpha > 0) FV subcells with the same interface
 // terms; then the GLM damping -glm_alpha psi, the RK register/state update (FP64) and the
@@ -22,13 +24,16 @@
 namespace nemo {
 namespace mhd {
 
-// Tile shape (compile-time knobs for tuning builds): elements per CTA (16 threads each) and, for the
-// plain FP64 form, the minimum number of resident CTAs per SM asked of the register allocator.
+// Tile shape (compile-time knobs for tuning builds): elements per CTA (16 threads each) and, per
+// form, the minimum number of resident CTAs per SM asked of the register allocator.
 #ifndef NEMO_MHD_EPC
 #define NEMO_MHD_EPC 8
 #endif
 #ifndef NEMO_MHD64_MINB
 #define NEMO_MHD64_MINB 1
+#endif
+#ifndef NEMO_MHD32_MINB
+#define NEMO_MHD32_MINB 3
 #endif
 constexpr int EPC = NEMO_MHD_EPC;
 constexpr int NT = 16 * EPC;
@@ -425,7 +430,7 @@ __device__ void epilogue_mhd(const StageArgs& a, const double* su, R* scr, unsig
 // pair fluxes cheaper but the stage 4 % slower, as the larger carveout left L1 too small for the
 // neighbour traces and register rows.
 template <typename R, bool BLEND, bool RHS_ONLY, bool FAST>
-__global__ void __launch_bounds__(mhd::NT, sizeof(R) == 4 ? 3 : NEMO_MHD64_MINB) k_stage_mhd(StageArgs a) {
+__global__ void __launch_bounds__(mhd::NT, sizeof(R) == 4 ? NEMO_MHD32_MINB : NEMO_MHD64_MINB) k_stage_mhd(StageArgs a) {
     constexpr int MEPC = mhd::EPC, MV = mhd::V;
     using mhd::load_rot;
     using mhd::load_rot_global;
