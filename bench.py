@@ -710,10 +710,14 @@ def main():  # noqa: C901
             "e2e": None if e2e_val is None else {
                     "value": e2e_val, "unit": "DOF-updates/s", "h2d_bytes_per_step": nbytes,
                     "d2h_bytes_per_step": nbytes, "serial_value": e2e_serial,
+                    # host<->device bytes of both directions per second of the pipelined loop: the
+                    # copies bound it once they overlap the steps
+                    "copy_gbs": 2 * nbytes * e2e_val / (world * dof_per_step) / 1e9,
                     "note": "per step: upload of the full state from pinned host memory, one time step, "
                             "download of the full state, through the C-ABI; pipelined (asynchronous "
                             "upload of the next state and download of this one overlap the steps); "
-                            "serial_value: the same with synchronous calls"},
+                            "serial_value: the same with synchronous calls; copy_gbs: both copy "
+                            "directions together, bytes per second of the pipelined loop"},
             "gpu_launches": int(chosen["launches"]),
             "sim": {"t": chosen["t_sim"], "steps": chosen["steps"]},
         }
