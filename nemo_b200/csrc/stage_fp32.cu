@@ -1079,7 +1079,11 @@ cudaError_t setup_stage_euler32(const OpConsts& ops) {
 namespace nemo {
 #undef NEMO_MHD_OPS
 
-int stage_smem_bytes_mhd32() { return mhd::V * mhd::EPC * (NP * (int)sizeof(double) + mhd::SPM * (int)sizeof(float)); }
+// state, rhs rows and the subcell interface fluxes of each thread's line
+int stage_smem_bytes_mhd32() {
+    return mhd::V * mhd::EPC * (NP * (int)sizeof(double) + mhd::SPM * (int)sizeof(float)) +
+           (NN - 1) * mhd::V * mhd::NT * (int)sizeof(float);
+}
 
 cudaError_t setup_stage_mhd32() {
     const int smem = stage_smem_bytes_mhd32();

@@ -681,7 +681,11 @@ cudaError_t launch_totals64(const double* u, const double* delta, int64_t E, int
 namespace nemo {
 #undef NEMO_MHD_OPS
 
-int stage_smem_bytes_mhd64() { return mhd::V * mhd::EPC * (NP * (int)sizeof(double) + mhd::SPM * (int)sizeof(double)); }
+// state, rhs rows and the subcell interface fluxes of each thread's line
+int stage_smem_bytes_mhd64() {
+    return mhd::V * mhd::EPC * (NP * (int)sizeof(double) + mhd::SPM * (int)sizeof(double)) +
+           (NN - 1) * mhd::V * mhd::NT * (int)sizeof(double);
+}
 
 cudaError_t setup_stage_mhd64() {
     const int smem = stage_smem_bytes_mhd64();

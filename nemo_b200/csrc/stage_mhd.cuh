@@ -438,6 +438,7 @@ __global__ void __launch_bounds__(mhd::NT, sizeof(R) == 4 ? NEMO_MHD32_MINB : NE
     extern __shared__ __align__(128) double smem_m[];
     double* su = smem_m;                                    // [9][MEPC][64] FP64 state
     R* sR = reinterpret_cast<R*>(su + MV * MEPC * NP);        // [9][MEPC][64] rhs terms
+    R* sFh = sR + MV * MEPC * mhd::SPM;                        // [NN-1][9][NT] subcell interface fluxes
     __shared__ uint64_t bar;
     __shared__ R s_alpha[MEPC];
     __shared__ int s_bad[MEPC];
@@ -560,7 +561,17 @@ __global__ void __launch_bounds__(mhd::NT, sizeof(R) == 4 ? NEMO_MHD32_MINB : NE
             if (BLEND) {
                 const R al = s_alpha[el];
                 if (al > R(0.0)) {
-                    R Fh[MV];   // Riemann flux of the interface to the left of node i (i > 0)
+                    // the three interface Riemann fluxes in a rolled loop (one inlined solver instead of
+                    // three: less code), kept in the thread's shared-memory slots
+#pragma unroll 1
+                    for (int q = 0; q < NN - 1; ++q) {
+                        R uq[MV], ur[MV], Fq[MV];
+                        load_rot(su, el, line_node(d, la, lb, q), d, uq);
+                        load_rot(su, el, line_node(d, la, lb, q + 1), d, ur);
+                        m_riem<FAST>(a.surface_flux, uq, ur, Fq, kap, mu0, ch);
+#pragma unroll
+                        for (int v = 0; v < MV; ++v) sFh[(q * MV + v) * mhd::NT + tid] = Fq[v];
+                    }
 #pragma unroll
                     for (int i = 0; i < NN; ++i) {
                         R ui[MV], FR[MV], FL[MV], G[MV];
@@ -570,7 +581,7 @@ __global__ void __launch_bounds__(mhd::NT, sizeof(R) == 4 ? NEMO_MHD32_MINB : NE
                             load_rot(su, el, idx[i - 1], d, ul);
                             m_nc_x(ui, ul, ui, G, mu0);
 #pragma unroll
-                            for (int v = 0; v < MV; ++v) FL[v] = Fh[v] + G[v];
+                            for (int v = 0; v < MV; ++v) FL[v] = sFh[((i - 1) * MV + v) * mhd::NT + tid] + G[v];
                         } else {
 #pragma unroll
                             for (int v = 0; v < MV; ++v) FL[v] = Fs[0][v];
@@ -578,10 +589,9 @@ __global__ void __launch_bounds__(mhd::NT, sizeof(R) == 4 ? NEMO_MHD32_MINB : NE
                         if (i < NN - 1) {
                             R ur[MV];
                             load_rot(su, el, idx[i + 1], d, ur);
-                            m_riem<FAST>(a.surface_flux, ui, ur, Fh, kap, mu0, ch);
                             m_nc_x(ui, ui, ur, G, mu0);
 #pragma unroll
-                            for (int v = 0; v < MV; ++v) FR[v] = Fh[v] + G[v];
+                            for (int v = 0; v < MV; ++v) FR[v] = sFh[(i * MV + v) * mhd::NT + tid] + G[v];
                         } else {
 #pragma unroll
                             for (int v = 0; v < MV; ++v) FR[v] = Fs[1][v];
