@@ -13,10 +13,11 @@ nleaves blocks (checkpoint_utils_dataset_iterate, :134-203).  Here the parent bl
 projection of their children (the reference leaves them unwritten); "blnd" holds the element's
 blending coefficient at every node (the reference writes a per-node blend of its FV levels).
 
-Container: this image has no HDF5 library (neither libhdf5 nor h5py), so the datasets are written
-with FLASH's names, shapes and dtypes into an uncompressed numpy .npz archive (`<name>.f5.npz`,
-written as `.partial` and renamed, as the reference does); `to_hdf5` copies such an archive into an
-HDF5 file where h5py is present.  Restart is the part the reference leaves as a TODO
+Container: an HDF5 file named like the reference's (`<prefix><count:06d>.f5`), written as `.partial`
+and renamed, as the reference does.  This image has no HDF5 library (neither libhdf5 nor h5py), so
+`h5lite` writes the original-format HDF5 structures these datasets need (one root group of contiguous
+datasets, compound records for the scalar lists) from the file-format specification.  A path ending
+in `.npz` selects an uncompressed numpy archive of the same datasets instead.  Restart is the part the reference leaves as a TODO
 (source/nemo_prog.f90:107-114): `read` rebuilds the forest from the leaves' levels and coordinates,
 and `restart` uploads the state and restores the time and step counter.
 """
@@ -25,7 +26,7 @@ import os
 
 import numpy as np
 
-from . import abi
+from . import abi, h5lite
 from .mesh import forest_mesh
 
 FILE_FORMAT_VERSION = 9
@@ -171,37 +172,48 @@ def datasets(mesh, u, t, steps, cfg, dt=0.0, alpha=None, number=0, basename="chk
 
 
 def write(path, ds):
-    """Write the datasets to path (.npz archive) through a '.partial' file and a rename."""
+    """Write the datasets to path through a '.partial' file and a rename: an HDF5 file, or a numpy
+    archive if the path ends in '.npz'."""
     tmp = path + ".partial"
-    with open(tmp, "wb") as f:
-        np.savez(f, **ds)
+    if path.endswith(".npz"):
+        with open(tmp, "wb") as f:
+            np.savez(f, **ds)
+    else:
+        h5lite.write(tmp, ds)
     os.replace(tmp, path)
 
 
+def load_datasets(path):
+    """{name: array} of a checkpoint file, HDF5 (recognised by its signature) or numpy archive."""
+    with open(path, "rb") as f:
+        magic = f.read(8)
+    if magic == h5lite.SIG:
+        return h5lite.read(path)
+    with np.load(path) as z:
+        return {k: z[k] for k in z.files}
+
+
 def to_hdf5(npz_path, h5_path):
-    """Copy a checkpoint archive into an HDF5 file with h5py (where h5py is installed)."""
-    import h5py
-    with np.load(npz_path) as z, h5py.File(h5_path, "w") as f:
-        for k in z.files:
-            f.create_dataset(k, data=z[k])
+    """Copy a checkpoint archive (.npz) into an HDF5 file."""
+    write(h5_path, load_datasets(npz_path))
 
 
 def read(path):
-    """(mesh, u [V, E, 64], t, steps) from a checkpoint archive; the mesh is the forest of its leaves."""
-    with np.load(path) as z:
-        ip = {r["name"].decode(): int(r["value"]) for r in z["integer runtime parameters"]}
-        rp = {r["name"].decode(): float(r["value"]) for r in z["real runtime parameters"]}
-        iscal = {r["name"].decode(): int(r["value"]) for r in z["integer scalars"]}
-        rscal = {r["name"].decode(): float(r["value"]) for r in z["real scalars"]}
-        names = [n[0].decode() for n in z["unknown names"] if n[0].decode() != "blnd"]
-        leaf = z["node type"] == 1
-        lev = z["refine level"][leaf].astype(np.int64) - 1
-        lo = np.array([rp["xmin"], rp["ymin"], rp["zmin"]])
-        hi = np.array([rp["xmax"], rp["ymax"], rp["zmax"]])
-        nb, max_level = ip["nblockx"], ip["lrefine_max"] - 1
-        size = z["block size"][leaf]
-        crd = np.rint((z["coordinates"][leaf] - lo) / size - 0.5).astype(np.int64)
-        u = np.stack([z[n][leaf].reshape(-1, 64) for n in names])
+    """(mesh, u [V, E, 64], t, steps) from a checkpoint file; the mesh is the forest of its leaves."""
+    z = load_datasets(path)
+    ip = {r["name"].decode(): int(r["value"]) for r in z["integer runtime parameters"]}
+    rp = {r["name"].decode(): float(r["value"]) for r in z["real runtime parameters"]}
+    iscal = {r["name"].decode(): int(r["value"]) for r in z["integer scalars"]}
+    rscal = {r["name"].decode(): float(r["value"]) for r in z["real scalars"]}
+    names = [n[0].decode() for n in z["unknown names"] if n[0].decode() != "blnd"]
+    leaf = z["node type"] == 1
+    lev = z["refine level"][leaf].astype(np.int64) - 1
+    lo = np.array([rp["xmin"], rp["ymin"], rp["zmin"]])
+    hi = np.array([rp["xmax"], rp["ymax"], rp["zmax"]])
+    nb, max_level = ip["nblockx"], ip["lrefine_max"] - 1
+    size = z["block size"][leaf]
+    crd = np.rint((z["coordinates"][leaf] - lo) / size - 0.5).astype(np.int64)
+    u = np.stack([z[n][leaf].reshape(-1, 64) for n in names])
     mesh = forest_mesh(nb, max_level, lev, crd, lo, hi)
     # forest_mesh orders the leaves by Morton order; the file holds them in that order already
     order = np.lexsort((crd[:, 2], crd[:, 1], crd[:, 0], lev))
@@ -245,7 +257,7 @@ class Checkpointer:
         u = self.buf.numpy().reshape(s.E, s.V, s.n ** 3).transpose(1, 0, 2)
         if path is None:
             os.makedirs(self.directory, exist_ok=True)
-            path = os.path.join(self.directory, f"{self.basename}{self.count:06d}.f5.npz")
+            path = os.path.join(self.directory, f"{self.basename}{self.count:06d}.f5")
         write(path, datasets(s.mesh, u, t.value, st.value, s.cfg, alpha=self.abuf.numpy().copy(),
                              number=self.count, basename=self.basename))
         self.count += 1

@@ -54,9 +54,9 @@ def test_datasets_and_restriction():
     np.testing.assert_array_equal(ds["blnd"][nin:, 0, 0, 0], np.linspace(0, 0.5, m.E))
 
 
-def _round_trip(m, tmp_path):
+def _round_trip(m, tmp_path, name="chkpt_000000.f5"):
     u = setups.smooth_random(m, seed=9)
-    path = str(tmp_path / "chkpt_000000.f5.npz")
+    path = str(tmp_path / name)
     checkpoint.write(path, checkpoint.datasets(m, u, 0.125, 40, abi.default_cfg()))
     m2, u2, t, steps = checkpoint.read(path)
     assert t == 0.125 and steps == 40 and m2.E == m.E
@@ -80,16 +80,64 @@ def test_round_trip_brick(tmp_path):
     _round_trip(mesh.brick(4), tmp_path)
 
 
+def test_round_trip_numpy_archive(tmp_path):
+    _round_trip(band_forest(), tmp_path, "chkpt_000000.f5.npz")
+
+
+def test_hdf5_container_holds_every_dataset_unchanged(tmp_path):
+    """The HDF5 file (the reference's container) holds every FLASH dataset with its dtype, shape and
+    bytes -- the compound scalar and parameter records included -- and its structures are the
+    format's: the signature, a version-0 superblock whose end-of-file address is the file size,
+    the root group's B-tree, local heap and symbol-table nodes with the names in byte order."""
+    import struct
+    from nemo_b200 import h5lite
+    m = band_forest()
+    ds = checkpoint.datasets(m, setups.smooth_random(m, seed=3), 0.25, 12, abi.default_cfg(),
+                             alpha=np.linspace(0.0, 0.5, m.E))
+    path = str(tmp_path / "chkpt_000001.f5")
+    checkpoint.write(path, ds)
+    raw = open(path, "rb").read()
+    assert raw[:8] == b"\x89HDF\r\n\x1a\n" and raw[8] == 0
+    assert struct.unpack_from("<Q", raw, 40)[0] == len(raw)
+    btree, heap = struct.unpack_from("<QQ", raw, 80)
+    assert raw[btree:btree + 4] == b"TREE" and raw[heap:heap + 4] == b"HEAP"
+    back = h5lite.read(path)
+    assert sorted(back) == sorted(ds)
+    for k, v in ds.items():
+        v = np.asarray(v)
+        assert back[k].dtype == v.dtype and back[k].shape == v.shape and back[k].tobytes() == v.tobytes(), k
+    # the symbol-table nodes list the names in strcmp order
+    names, nsnod = [], struct.unpack_from("<H", raw, btree + 6)[0]
+    for i in range(nsnod):
+        child = struct.unpack_from("<Q", raw, btree + 32 + 16 * i)[0]
+        assert raw[child:child + 4] == b"SNOD"
+        seg = struct.unpack_from("<Q", raw, heap + 24)[0]
+        for j in range(struct.unpack_from("<H", raw, child + 6)[0]):
+            off = struct.unpack_from("<Q", raw, child + 8 + 40 * j)[0]
+            names.append(raw[seg + off:raw.index(b"\0", seg + off)])
+    assert names == sorted(names) and len(names) == len(ds)
+
+
+def test_numpy_archive_converts_to_hdf5(tmp_path):
+    m = mesh.brick(4)
+    ds = checkpoint.datasets(m, setups.smooth_random(m, seed=5), 0.5, 3, abi.default_cfg())
+    a, b = str(tmp_path / "c.f5.npz"), str(tmp_path / "c.f5")
+    checkpoint.write(a, ds)
+    checkpoint.to_hdf5(a, b)
+    r1, r2 = checkpoint.read(a), checkpoint.read(b)
+    assert np.array_equal(r1[1], r2[1]) and r1[2:] == r2[2:]
+
+
 def test_round_trip_mhd(tmp_path):
     """GLM-MHD state: the 9 FLASH variable names and a lossless round trip."""
     m = band_forest()
     u = setups.orszag_tang(m)
     c = abi.default_cfg(eqn=abi.EQN_MHD, n_vars=9, kappa=5 / 3)
-    path = str(tmp_path / "mhd.f5.npz")
+    path = str(tmp_path / "mhd.f5")
     checkpoint.write(path, checkpoint.datasets(m, u, 0.5, 7, c))
-    with np.load(path) as z:
-        assert [n[0] for n in z["unknown names"]] == [n.encode() for n in checkpoint.MHD_NAMES] + [b"blnd"]
-        g = {r["name"]: r["value"] for r in z["real runtime parameters"]}
-        assert abs(g[b"gamma"] - 5 / 3) < 1e-15
+    z = checkpoint.load_datasets(path)
+    assert [n[0] for n in z["unknown names"]] == [n.encode() for n in checkpoint.MHD_NAMES] + [b"blnd"]
+    g = {r["name"]: r["value"] for r in z["real runtime parameters"]}
+    assert abs(g[b"gamma"] - 5 / 3) < 1e-15
     m2, u2, t, steps = checkpoint.read(path)
     assert u2.shape == u.shape and np.array_equal(u2, u) and t == 0.5 and steps == 7
