@@ -7,8 +7,9 @@ published file-format specification (HDF5 File Format Specification, version 2.0
 version 0 with 8-byte offsets and lengths, version-1 object headers, the root group as a symbol
 table (a version-1 B-tree of group nodes over symbol-table nodes, names in a local heap), and per
 dataset the dataspace (version 1), datatype (version 1), fill-value (version 2) and data-layout
-(version 3, contiguous) messages.  The files open with any HDF5 reader that understands these
-original-format structures (all releases do); `read` parses exactly this subset back.
+(version 3, contiguous) messages: structures every HDF5 release reads.  No independent HDF5 reader
+is installed here to open the files with; `read` parses exactly this subset back, and the tests
+check the round trip byte for byte and the structures' signatures, ordering and addresses.
 """
 import struct
 
